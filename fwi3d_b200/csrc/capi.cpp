@@ -1,0 +1,338 @@
+// extern "C" entry points of libfwi3d_b200.so (declared in include/fwi3d_gpu.h).
+//
+// fwi_op mirrors one nl_we_op_{a,e,vti} object: it holds the per-shot
+// wavelet and geometry (we_op.hpp:59-79), a mutable copy of the parameters
+// that analyzeModel updates on every call (dt, courant, sub), and the device
+// state the forward pass leaves for the adjoint (the reference keeps it in
+// the mutable _zfp_wfld member, we_op.hpp:23).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/fwi3d_gpu.h"
+#include "engine.h"
+#include "host_ops.h"
+
+using namespace fwi;
+
+namespace {
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+template <class F>
+int guarded(F &&f)
+{
+    try {
+        f();
+        g_err.clear();
+        return FWI_OK;
+    } catch (const FwiError &e) {
+        return fail(e.code, e.what());
+    } catch (const std::bad_alloc &) {
+        return fail(FWI_ERR_OOM, "host allocation failed");
+    } catch (const std::invalid_argument &e) {
+        return fail(FWI_ERR_ARG, e.what());
+    } catch (const std::exception &e) {
+        return fail(FWI_ERR_CUDA, e.what());
+    }
+}
+
+bool finite_all(const float *p, int64_t n)
+{
+    for (int64_t i = 0; i < n; i++)
+        if (!std::isfinite(p[i])) return false;
+    return true;
+}
+}  // namespace
+
+struct fwi_op {
+    int device = 0;
+    fwi_grid grid{};
+    int nmodels = 3;
+    fwi_param par{};
+    int nt_data = 0;
+    float dt_data = 0.f;
+    int nscomp = 1, nrcomp = 1;
+    std::vector<float> wavelet;  // [nscomp][nt_data]
+    float sxyz[3] = {0, 0, 0};
+    int nr = 0;
+    std::vector<float> rxyz;     // [nr][5]
+    Problem pb{};
+    std::unique_ptr<Engine> eng;
+    std::vector<float> conv;     // converted model of the last call
+
+    int64_t nxyz() const { return (int64_t)grid.nx * grid.ny * grid.nz; }
+    int ncomp() const { return nmodels == 2 ? 1 : 3; }
+
+    // analyzeModel + convert_model on a copy of `model`, then make sure the
+    // engine matches the resulting time axis (we_op.cpp:874-878, 951-958).
+    void prepare(const float *model)
+    {
+        std::vector<float> m(model, model + nmodels * nxyz());
+        TimeAxis ta = analyze_model(m, nmodels, grid.nx, grid.ny, grid.nz, grid.dx, grid.dy, grid.dz, nt_data, dt_data,
+                                    par);
+        par.dt = ta.dt;
+        par.courant = ta.courant;
+        par.sub = ta.sub;
+        convert_model(m, nmodels, nxyz());
+        Problem p{};
+        p.nmodels = nmodels;
+        p.nx = grid.nx;
+        p.ny = grid.ny;
+        p.nz = grid.nz;
+        p.dx = grid.dx;
+        p.dy = grid.dy;
+        p.dz = grid.dz;
+        p.dt = ta.dt;
+        p.nt = ta.nt;
+        p.sub = ta.sub;
+        std::memcpy(p.bc, par.bc, sizeof(p.bc));
+        for (int f = 0; f < 6; f++) p.bc[f] = std::max(0, p.bc[f]);
+        std::memcpy(p.taper, par.taper, sizeof(p.taper));
+        p.taper_strength = par.taper_strength;
+        p.free_surface_stiffness = nmodels == 2 ? std::max(par.free_surface_stiffness, 1.0f) : par.free_surface_stiffness;
+        p.grad_fp64 = par.grad_fp64 != 0;
+        const bool same = eng && pb.nt == p.nt && pb.dt == p.dt && pb.sub == p.sub;
+        pb = p;
+        if (!same) eng.reset(new Engine(device, pb));
+        eng->set_model(m.data());
+        conv.swap(m);
+    }
+
+    std::vector<Loc> receivers() const
+    {
+        std::vector<Loc> l(nr);
+        for (int r = 0; r < nr; r++) l[r] = Loc{rxyz[5 * r], rxyz[5 * r + 1], rxyz[5 * r + 2]};
+        return l;
+    }
+};
+
+extern "C" {
+
+void fwi_param_default(fwi_param *p)
+{
+    std::memset(p, 0, sizeof(*p));
+    p->courant = 0.5f;
+    p->dt = -1.f;
+    p->sub = 0;
+    p->resampling_linear = 0;
+    p->sinc_half_length = 11;
+    p->mt = 0;
+    p->mxx = p->myy = p->mzz = p->mxy = p->mxz = p->myz = 1.f;
+    p->seismotype = 0;
+    p->gl = 0.f;
+    for (int f = 0; f < 6; f++) {
+        p->bc[f] = 1;
+        p->taper[f] = 0;
+    }
+    p->free_surface_stiffness = 1.05f;
+    p->taper_strength = 0.05f;
+    p->vpmin = 0.2f;
+    p->vpmax = 8.f;
+    p->vsmin = 0.1f;
+    p->vsmax = 5.f;
+    p->rhomin = 0.1f;
+    p->rhomax = 8.f;
+    p->deltamin = -0.5f;
+    p->deltamax = 1.f;
+    p->epsilonmin = 0.f;
+    p->epsilonmax = 1.f;
+    p->gammamin = 0.f;
+    p->gammamax = 1.f;
+    p->soft_clip = 0;
+    p->verbose = 0;
+    p->grad_fp64 = 1;
+}
+
+const char *fwi_last_error(void) { return g_err.c_str(); }
+
+const char *fwi_version(void) { return "fwi3d_b200 0.1 (sm_100a)"; }
+
+int fwi_op_create(fwi_op **out, int device, const fwi_grid *grid, int nmodels, const fwi_param *par,
+                  const float *wavelet, int wavelet_ncomp, int nt_data, float dt_data, const float *sxyz, int nr,
+                  const float *rxyz)
+{
+    if (!out || !grid || !par || !wavelet || !sxyz || (nr > 0 && !rxyz)) return fail(FWI_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (nmodels != 2 && nmodels != 3 && nmodels != 6)
+        return fail(FWI_ERR_ARG, "The model must contain 2, 3, or 6 parameters");
+    if (grid->nx < 12 || grid->ny < 12 || grid->nz < 12)
+        return fail(FWI_ERR_ARG, "each grid axis needs at least 12 points");
+    if (nt_data < 2 || !(dt_data > 0)) return fail(FWI_ERR_ARG, "the wavelet needs at least 2 samples and dt > 0");
+    if (nr < 1) return fail(FWI_ERR_ARG, "at least one receiver is required");
+    if (par->gl > 0) return fail(FWI_ERR_UNSUPPORTED, "DAS receivers (gl > 0) are not implemented on the GPU path");
+    return guarded([&] {
+        std::unique_ptr<fwi_op> op(new fwi_op());
+        op->device = device;
+        op->grid = *grid;
+        op->nmodels = nmodels;
+        op->par = *par;
+        if (nmodels == 2) op->par.mt = 0;
+        op->nt_data = nt_data;
+        op->dt_data = dt_data;
+        op->nscomp = nmodels == 2 ? 1 : (op->par.mt ? 6 : 3);
+        op->nrcomp = nmodels == 2 ? 1 : 3;
+        op->wavelet = expand_wavelet(wavelet, wavelet_ncomp, nt_data, nmodels, op->par);
+        std::memcpy(op->sxyz, sxyz, sizeof(op->sxyz));
+        op->nr = nr;
+        op->rxyz.assign(rxyz, rxyz + 5 * nr);
+        // source / receivers inside the model (analyzeGeometry, we_op.cpp:84-108)
+        const fwi_grid &g = *grid;
+        const float prec = std::min(g.dx, g.dz) * 1e-3f;
+        auto inside = [&](float x, float y, float z) {
+            return (x - g.ox >= -prec) && (-prec <= -x + g.ox + (g.nx - 1) * g.dx) && (y - g.oy >= -prec) &&
+                   (-prec <= -y + g.oy + (g.ny - 1) * g.dy) && (z - g.oz >= -prec) &&
+                   (-prec <= -z + g.oz + (g.nz - 1) * g.dz);
+        };
+        if (!inside(sxyz[0], sxyz[1], sxyz[2]))
+            throw FwiError(FWI_ERR_ARG, "Shot falls outside subsurface model boundaries");
+        for (int r = 0; r < nr; r++)
+            if (!inside(rxyz[5 * r], rxyz[5 * r + 1], rxyz[5 * r + 2]))
+                throw FwiError(FWI_ERR_ARG, "Receiver " + std::to_string(r) + " falls outside subsurface model boundaries");
+        *out = op.release();
+    });
+}
+
+int fwi_op_forward(fwi_op *op, int add, const float *model, float *data)
+{
+    if (!op || !model || !data) return fail(FWI_ERR_ARG, "null argument");
+    return guarded([&] {
+        if (!finite_all(model, op->nmodels * op->nxyz())) throw FwiError(FWI_ERR_NAN, "model contains non-finite values");
+        op->prepare(model);
+        const Problem &pb = op->pb;
+        const int nt = pb.nt;
+        const bool sinc = op->par.resampling_linear == 0;
+        // wavelet -> propagation sampling (we_op.cpp:907-911)
+        std::vector<float> src((size_t)op->nscomp * nt);
+        resample_forward(sinc, op->par.sinc_half_length, op->wavelet.data(), op->nt_data, op->dt_data, src.data(), nt,
+                         pb.dt, op->nscomp);
+        PointOp inj = make_delta(pb.nx, pb.ny, pb.nz, pb.dx, pb.dy, pb.dz, op->grid.ox, op->grid.oy, op->grid.oz,
+                                 {Loc{op->sxyz[0], op->sxyz[1], op->sxyz[2]}}, op->par.mt != 0);
+        PointOp ext = make_delta(pb.nx, pb.ny, pb.nz, pb.dx, pb.dy, pb.dz, op->grid.ox, op->grid.oy, op->grid.oz,
+                                 op->receivers(), false);
+        const InjTable it = injection_table(inj, pb.nx, pb.ny, pb.nz, op->ncomp());
+        const ExtTable et = extraction_table(ext, pb.nx, pb.ny, pb.nz);
+        const int ncr = op->ncomp();
+        const int ntr = ncr * op->nr;
+        std::vector<float> rcv((size_t)ntr * nt);
+        op->eng->forward(it, op->nscomp, src.data(), et, ncr, rcv.data(), pb.sub > 0);
+        if (!finite_all(rcv.data(), (int64_t)rcv.size())) throw FwiError(FWI_ERR_NAN, "non-finite values in the traces");
+        if (op->par.seismotype == 1) {
+            // particle velocity (we_op.cpp:932-938)
+            std::vector<float> v(rcv.size());
+            apply_dt(false, rcv.data(), v.data(), ntr, nt, pb.dt);
+            rcv.swap(v);
+        }
+        const float alpha = pb.dt / op->dt_data;
+        for (auto &v : rcv) v *= alpha;
+        if (!add) std::fill(data, data + (size_t)ntr * op->nt_data, 0.f);
+        resample_adjoint(sinc, op->par.sinc_half_length, data, op->nt_data, op->dt_data, rcv.data(), nt, pb.dt, ntr);
+    });
+}
+
+int fwi_op_jacobianT(fwi_op *op, int add, float *grad, const float *model0, const float *data)
+{
+    if (!op || !grad || !model0 || !data) return fail(FWI_ERR_ARG, "null argument");
+    return guarded([&] {
+        if (!op->eng || !op->eng->has_snapshots())
+            throw FwiError(FWI_ERR_STATE, "jacobianT needs a preceding forward on this operator with sub > 0");
+        if (!finite_all(model0, op->nmodels * op->nxyz())) throw FwiError(FWI_ERR_NAN, "model contains non-finite values");
+        const int64_t n = op->nxyz();
+        const int nm = std::min(3, op->nmodels);
+        // analyzeModel must reproduce the forward's time axis (same model in FWI)
+        const Problem before = op->pb;
+        {
+            std::vector<float> m(model0, model0 + op->nmodels * n);
+            TimeAxis ta = analyze_model(m, op->nmodels, op->grid.nx, op->grid.ny, op->grid.nz, op->grid.dx, op->grid.dy,
+                                        op->grid.dz, op->nt_data, op->dt_data, op->par);
+            if (ta.nt != before.nt || ta.dt != before.dt || ta.sub != before.sub)
+                throw FwiError(FWI_ERR_STATE, "the background model changes the time axis of the stored forward pass");
+            op->par.dt = ta.dt;
+            op->par.courant = ta.courant;
+            op->par.sub = ta.sub;
+            convert_model(m, op->nmodels, n);
+            op->eng->set_model(m.data());
+            op->conv.swap(m);
+        }
+        const Problem &pb = op->pb;
+        const int nt = pb.nt;
+        const int ncr = op->ncomp();
+        const int ntr = ncr * op->nr;
+        const bool sinc = op->par.resampling_linear == 0;
+        std::vector<float> temp;
+        if (add) temp.assign(grad, grad + nm * n);
+        else std::fill(grad, grad + nm * n, 0.f);
+        // data -> propagation sampling, Ht^-1, time reversal, -alpha (we_op.cpp:994-1003)
+        std::vector<float> rcv((size_t)ntr * nt);
+        resample_forward(sinc, op->par.sinc_half_length, data, op->nt_data, op->dt_data, rcv.data(), nt, pb.dt, ntr);
+        apply_ht(true, rcv.data(), rcv.data(), ntr, nt, pb.dt);
+        for (int tr = 0; tr < ntr; tr++) std::reverse(rcv.begin() + (size_t)tr * nt, rcv.begin() + (size_t)(tr + 1) * nt);
+        const float alpha = pb.dt / op->dt_data;
+        for (auto &v : rcv) v *= -alpha;
+        if (op->par.seismotype == 1) {
+            std::vector<float> v(rcv.size());
+            apply_dt(true, rcv.data(), v.data(), ntr, nt, pb.dt);
+            rcv.swap(v);
+        }
+        PointOp inj = make_delta(pb.nx, pb.ny, pb.nz, pb.dx, pb.dy, pb.dz, op->grid.ox, op->grid.oy, op->grid.oz,
+                                 op->receivers(), false);
+        const InjTable it = injection_table(inj, pb.nx, pb.ny, pb.nz, ncr);
+        std::vector<float> g((size_t)nm * n);
+        op->eng->adjoint(it, ntr, rcv.data(), g.data());
+        // The reference accumulates the imaging sums into pmod itself, so with
+        // add the previous content also goes through H and the chain rule
+        // before `temp` is added back (we_op.cpp:968-972, 1027-1075).
+        for (int64_t i = 0; i < nm * n; i++) grad[i] += g[i];
+        for (int p = 0; p < nm; p++) apply_h3(grad + p * n, pb.nx, pb.ny, pb.nz, pb.dx, pb.dy, pb.dz);
+        gradient_to_velocity(grad, op->conv.data(), op->nmodels, n);
+        if (add)
+            for (int64_t i = 0; i < nm * n; i++) grad[i] += temp[i];
+        if (!finite_all(grad, nm * n)) throw FwiError(FWI_ERR_NAN, "non-finite values in the gradient");
+    });
+}
+
+int fwi_op_get_info(const fwi_op *op, fwi_op_info *info)
+{
+    if (!op || !info) return fail(FWI_ERR_ARG, "null argument");
+    info->dt = op->pb.dt;
+    info->nt = op->pb.nt;
+    info->sub = op->pb.sub;
+    info->nscomp = op->nscomp;
+    info->nrcomp = op->nrcomp;
+    info->nr = op->nr;
+    info->device_bytes = op->eng ? op->eng->device_bytes() : 0;
+    return FWI_OK;
+}
+
+void fwi_op_destroy(fwi_op *op) { delete op; }
+
+int fwi_forward_batch(int device, const fwi_grid *grid, int nmodels, const fwi_param *par, const float *model,
+                      const float *wavelet, int wavelet_ncomp, int nt_data, float dt_data, int nshots,
+                      const float *sxyz, int nr, const float *rxyz, float *data)
+{
+    if (!grid || !par || !model || !wavelet || !sxyz || !rxyz || !data || nshots < 1)
+        return fail(FWI_ERR_ARG, "null argument or no shots");
+    const int nrcomp = nmodels == 2 ? 1 : 3;
+    for (int s = 0; s < nshots; s++) {
+        fwi_op *op = nullptr;
+        int rc = fwi_op_create(&op, device, grid, nmodels, par, wavelet, wavelet_ncomp, nt_data, dt_data, sxyz + 3 * s,
+                               nr, rxyz + (size_t)5 * nr * s);
+        if (rc != FWI_OK) return rc;
+        fwi_param p = *par;
+        (void)p;
+        rc = fwi_op_forward(op, 0, model, data + (size_t)s * nrcomp * nr * nt_data);
+        fwi_op_destroy(op);
+        if (rc != FWI_OK) return rc;
+    }
+    return FWI_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,519 @@
+// CUDA kernels of one propagation time step and the host time loops.
+//
+// One time step of the reference (we_op.cpp:623-836 elastic, :1274-1497 VTI,
+// :1640-1796 acoustic) becomes, per step and per shot:
+//   extract   receivers from curr (forward only)           k_extract
+//   aux       first-derivative scratch (elastic/VTI)        k_elastic_aux
+//   step      D2var + D1 terms + SAT + update + scale + taper, fused   k_*_step
+//   inject    sources (receivers' residual in the adjoint)  k_inject
+// and, every `sub` steps of the adjoint, the imaging condition k_*_image.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+
+#include "engine.h"
+#include "imaging.cuh"
+#include "physics.cuh"
+
+namespace fwi {
+
+#define CK(x)                                                                                               \
+    do {                                                                                                    \
+        cudaError_t e_ = (x);                                                                               \
+        if (e_ != cudaSuccess)                                                                              \
+            throw FwiError(e_ == cudaErrorMemoryAllocation ? FWI_ERR_OOM : FWI_ERR_CUDA,                   \
+                           std::string(#x) + ": " + cudaGetErrorString(e_));                                \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Device buffers
+// ---------------------------------------------------------------------------
+DevBuf::DevBuf(size_t n) { alloc(n); }
+DevBuf::~DevBuf()
+{
+    if (p) cudaFree(p);
+}
+DevBuf &DevBuf::operator=(DevBuf &&o) noexcept
+{
+    if (this != &o) {
+        if (p) cudaFree(p);
+        p = o.p;
+        bytes = o.bytes;
+        o.p = nullptr;
+        o.bytes = 0;
+    }
+    return *this;
+}
+void DevBuf::alloc(size_t n)
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    if (n == 0) return;
+    CK(cudaMalloc(&p, n));
+    bytes = n;
+}
+void DevBuf::zero(void *stream)
+{
+    if (p) CK(cudaMemsetAsync(p, 0, bytes, (cudaStream_t)stream));
+}
+
+// ---------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int BZ = 32, BX = 4, BY = 2;
+
+__device__ __forceinline__ bool point_of(const Dims &g, int &ix, int &iy, int &iz)
+{
+    iz = blockIdx.x * BZ + threadIdx.x;
+    ix = blockIdx.y * BX + threadIdx.y;
+    iy = blockIdx.z * BY + threadIdx.z;
+    return iz < g.nz && ix < g.nx && iy < g.ny;
+}
+
+dim3 grid_of(const Dims &g) { return dim3((g.nz + BZ - 1) / BZ, (g.nx + BX - 1) / BX, (g.ny + BY - 1) / BY); }
+
+__global__ void k_acoustic_step(StepArgs a)
+{
+    int ix, iy, iz;
+    if (!point_of(a.g, ix, iy, iz)) return;
+    a.next[0][a.g.idx(ix, iy, iz)] = acoustic_point(a, ix, iy, iz);
+}
+
+template <int PH>
+__global__ void k_elastic_aux(AuxArgs a)
+{
+    int ix, iy, iz;
+    if (!point_of(a.g, ix, iy, iz)) return;
+    elastic_aux_point<PH>(a, ix, iy, iz);
+}
+
+template <int PH>
+__global__ void k_elastic_step(StepArgs a)
+{
+    int ix, iy, iz;
+    if (!point_of(a.g, ix, iy, iz)) return;
+    const int64_t i = a.g.idx(ix, iy, iz);
+    const float v0 = elastic_point<PH>(a, 0, ix, iy, iz);
+    const float v1 = elastic_point<PH>(a, 1, ix, iy, iz);
+    const float v2 = elastic_point<PH>(a, 2, ix, iy, iz);
+    a.next[0][i] = v0;
+    a.next[1][i] = v1;
+    a.next[2][i] = v2;
+}
+
+// Post-injection: next += taper(scale(dt^2 (w s)/rho)) (elastic) or dt^2 (w s) K (acoustic).
+// Equivalent to the reference's injection into the operator sum before the
+// update (we_op.cpp:691-693) because update, scaling and taper are linear in it.
+__global__ void k_inject(StepArgs a, int c, const int64_t *gidx, const int *trace, const float *w, int n,
+                         const float *src, int nt, int it)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int64_t i = gidx[k];
+    const float s = w[k] * src[(int64_t)trace[k] * nt + it];
+    const int iz = (int)(i % a.g.nz);
+    const int ix = (int)((i / a.g.nz) % a.g.nx);
+    const int iy = (int)(i / ((int64_t)a.g.nz * a.g.nx));
+    const float dt2 = a.dt * a.dt;
+    float v = a.m[2] ? dt2 * s / a.m[2][i] : dt2 * s * a.m[0][i];
+    v = boundary_scale(a, v, c, ix, iy, iz);
+    v = taper(a, v, ix, iy, iz);
+    atomicAdd(&a.next[c][i], v);
+}
+
+// Initial condition prev = inject(src[:,0]) then scaled (we_op.cpp:611-619, 1635-1636).
+__global__ void k_inject0(float *prev, const int64_t *gidx, const int *trace, const float *w, int n, const float *src,
+                          int nt)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    atomicAdd(&prev[gidx[k]], w[k] * src[(int64_t)trace[k] * nt]);
+}
+
+__global__ void k_scale0(float *prev, const float *coef, int64_t n, float dt, int acoustic)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float p = prev[i];
+    if (p == 0.f) return;
+    if (acoustic) prev[i] = (float)((double)p * (0.5 * (double)coef[i] * dt * dt));
+    else prev[i] = (float)((double)p * (0.5 * dt * dt / (double)coef[i]));
+}
+
+// Receivers: rcv[c][r][it] = sum_k w_k u_c(g_k) (injector.cpp:118-140).
+__global__ void k_extract(const float *u, const int64_t *gidx, const float *w, int nrec, float *rcv, int nt, int it)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrec) return;
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < 27; k++) acc += w[27 * r + k] * u[gidx[27 * r + k]];
+    rcv[(int64_t)r * nt + it] = acc;
+}
+
+__global__ void k_acoustic_image(ImageArgs a)
+{
+    int ix, iy, iz;
+    if (!point_of(a.g, ix, iy, iz)) return;
+    acoustic_image_point(a, ix, iy, iz);
+}
+
+template <int PH>
+__global__ void k_elastic_image(ImageArgs a)
+{
+    int ix, iy, iz;
+    if (!point_of(a.g, ix, iy, iz)) return;
+    elastic_image_point<PH>(a, ix, iy, iz);
+}
+
+__global__ void k_d2f(const double *in, float *out, int64_t n)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (float)in[i];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Engine
+// ---------------------------------------------------------------------------
+Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
+{
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw FwiError(FWI_ERR_NOGPU, "no CUDA device");
+    if (device < 0 || device >= ndev) throw FwiError(FWI_ERR_ARG, "device index out of range");
+    CK(cudaSetDevice(device));
+    if (pb.nx < 12 || pb.ny < 12 || pb.nz < 12)
+        throw FwiError(FWI_ERR_ARG, "each grid axis needs at least 12 points (two 6-row SBP closures)");
+    init_sbp_tables();
+    CK(cudaMemcpyToSymbol(c_sbp, &g_sbp_host, sizeof(SbpTables)));
+    cudaStream_t s;
+    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    stream_ = s;
+    const int64_t n = pb.nxyz();
+    const int nc = pb.ncomp();
+    fields_.alloc(sizeof(float) * 3 * nc * n);
+    if (pb.nmodels != 2) aux_.alloc(sizeof(float) * (pb.nmodels == 6 ? 9 : 7) * n);
+}
+
+Engine::~Engine()
+{
+    if (stream_) {
+        cudaStreamSynchronize((cudaStream_t)stream_);
+        cudaStreamDestroy((cudaStream_t)stream_);
+    }
+}
+
+void Engine::sync() { CK(cudaStreamSynchronize((cudaStream_t)stream_)); }
+
+int64_t Engine::device_bytes() const
+{
+    return model_.bytes + fields_.bytes + aux_.bytes + snaps_.bytes + grad_.bytes + sdiv_.bytes + taper_.bytes +
+           src_dev_.bytes + rcv_dev_.bytes;
+}
+
+void Engine::set_model(const float *conv)
+{
+    CK(cudaSetDevice(device_));
+    const int64_t n = pb_.nxyz();
+    model_.alloc(sizeof(float) * pb_.nmodels * n);
+    CK(cudaMemcpyAsync(model_.p, conv, model_.bytes, cudaMemcpyHostToDevice, (cudaStream_t)stream_));
+
+    ScaleTables st = boundary_divisors(conv, pb_.nmodels, pb_.nx, pb_.ny, pb_.nz, pb_.dx, pb_.dy, pb_.dz, pb_.dt, pb_.bc);
+    scale_ = 0;
+    for (int f = 0; f < 6; f++) scale_ |= (pb_.bc[f] == BC_ABSORB);
+    size_t tot = 0;
+    const int nc = pb_.ncomp();
+    for (int f = 0; f < 6; f++)
+        for (int c = 0; c < nc; c++) tot += st.f[f][c].size();
+    std::vector<float> packed(tot);
+    size_t off[6][3] = {};
+    size_t o = 0;
+    for (int f = 0; f < 6; f++)
+        for (int c = 0; c < nc; c++) {
+            off[f][c] = o;
+            std::memcpy(packed.data() + o, st.f[f][c].data(), sizeof(float) * st.f[f][c].size());
+            o += st.f[f][c].size();
+        }
+    sdiv_.alloc(sizeof(float) * tot);
+    CK(cudaMemcpy(sdiv_.p, packed.data(), sdiv_.bytes, cudaMemcpyHostToDevice));
+    for (int f = 0; f < 6; f++)
+        for (int c = 0; c < 3; c++) sdiv_ptr_[f][c] = sdiv_.as<float>() + off[f][c < nc ? c : 0];
+
+    TaperTables tt = taper_tables(pb_.nx, pb_.ny, pb_.nz, pb_.taper, pb_.taper_strength);
+    size_t ttot = 0;
+    for (int k = 0; k < 6; k++) ttot += tt.t[k].size();
+    std::vector<float> tp(ttot);
+    size_t toff[6];
+    o = 0;
+    for (int k = 0; k < 6; k++) {
+        toff[k] = o;
+        std::memcpy(tp.data() + o, tt.t[k].data(), sizeof(float) * tt.t[k].size());
+        o += tt.t[k].size();
+    }
+    taper_.alloc(sizeof(float) * ttot);
+    CK(cudaMemcpy(taper_.p, tp.data(), taper_.bytes, cudaMemcpyHostToDevice));
+    for (int k = 0; k < 6; k++) taper_ptr_[k] = taper_.as<float>() + toff[k];
+    sync();
+}
+
+void Engine::upload_inj(const InjTable &t, int ntrace, DevInj &d)
+{
+    d.ntrace = ntrace;
+    for (int c = 0; c < 3; c++) {
+        d.n[c] = (int)t.gidx[c].size();
+        d.gidx[c].alloc(sizeof(int64_t) * d.n[c]);
+        d.trace[c].alloc(sizeof(int) * d.n[c]);
+        d.w[c].alloc(sizeof(float) * d.n[c]);
+        if (d.n[c]) {
+            CK(cudaMemcpy(d.gidx[c].p, t.gidx[c].data(), d.gidx[c].bytes, cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(d.trace[c].p, t.trace[c].data(), d.trace[c].bytes, cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(d.w[c].p, t.w[c].data(), d.w[c].bytes, cudaMemcpyHostToDevice));
+        }
+    }
+}
+
+namespace {
+StepArgs make_step_args(const Problem &pb, const float *m, const float *const sdiv[6][3], const float *const tap[6],
+                        int scale)
+{
+    StepArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.g = Dims{pb.nx, pb.ny, pb.nz};
+    a.dx = pb.dx;
+    a.dy = pb.dy;
+    a.dz = pb.dz;
+    a.dt = pb.dt;
+    const int64_t n = pb.nxyz();
+    for (int k = 0; k < pb.nmodels; k++) a.m[k] = m + k * n;
+    for (int f = 0; f < 6; f++) {
+        a.bc[f] = pb.bc[f];
+        a.tap[f] = tap[f];
+        for (int c = 0; c < 3; c++) a.sdiv[f][c] = sdiv[f][c];
+    }
+    a.scale = scale;
+    a.alpha_fs = (float)(0.2508560249 / pb.free_surface_stiffness);
+    return a;
+}
+}  // namespace
+
+void Engine::init_prev(const DevInj &inj, const float *src_dev, float *prev[3])
+{
+    cudaStream_t s = (cudaStream_t)stream_;
+    const int64_t n = pb_.nxyz();
+    const int nc = pb_.ncomp();
+    for (int c = 0; c < nc; c++) {
+        if (inj.n[c] == 0) continue;
+        k_inject0<<<(inj.n[c] + 255) / 256, 256, 0, s>>>(prev[c], inj.gidx[c].as<int64_t>(), inj.trace[c].as<int>(),
+                                                          inj.w[c].as<float>(), inj.n[c], src_dev, pb_.nt);
+        const float *coef = model_.as<float>() + (pb_.nmodels == 2 ? 0 : 2 * n);
+        k_scale0<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(prev[c], coef, n, pb_.dt, pb_.nmodels == 2);
+    }
+    CK(cudaGetLastError());
+}
+
+void Engine::step(int it, float *prev[3], float *curr[3], float *next[3], bool taper_prev)
+{
+    (void)it;
+    cudaStream_t s = (cudaStream_t)stream_;
+    const Dims g{pb_.nx, pb_.ny, pb_.nz};
+    const int64_t n = pb_.nxyz();
+    StepArgs a = make_step_args(pb_, model_.as<float>(), sdiv_ptr_, taper_ptr_, scale_);
+    const int nc = pb_.ncomp();
+    for (int c = 0; c < nc; c++) {
+        a.curr[c] = curr[c];
+        a.prev[c] = prev[c];
+        a.next[c] = next[c];
+    }
+    a.taper_prev = taper_prev ? 1 : 0;
+    const dim3 blk(BZ, BX, BY), grd = grid_of(g);
+    if (pb_.nmodels == 2) {
+        k_acoustic_step<<<grd, blk, 0, s>>>(a);
+    } else {
+        AuxArgs x;
+        std::memset(&x, 0, sizeof(x));
+        x.g = g;
+        x.dx = pb_.dx;
+        x.dy = pb_.dy;
+        x.dz = pb_.dz;
+        for (int k = 0; k < pb_.nmodels; k++) x.m[k] = a.m[k];
+        for (int c = 0; c < 3; c++) x.curr[c] = curr[c];
+        float *ab = aux_.as<float>();
+        if (pb_.nmodels == 3) {
+            // one shared divergence array in slots 0..2, then the six derivatives
+            x.aux[AUX_T0] = x.aux[AUX_T1] = x.aux[AUX_T2] = ab;
+            for (int k = 3; k < 9; k++) x.aux[k] = ab + (k - 2) * n;
+        } else {
+            for (int k = 0; k < 9; k++) x.aux[k] = ab + k * n;
+        }
+        for (int k = 0; k < 9; k++) a.aux[k] = x.aux[k];
+        if (pb_.nmodels == 3) {
+            k_elastic_aux<ELASTIC><<<grd, blk, 0, s>>>(x);
+            k_elastic_step<ELASTIC><<<grd, blk, 0, s>>>(a);
+        } else {
+            k_elastic_aux<VTI><<<grd, blk, 0, s>>>(x);
+            k_elastic_step<VTI><<<grd, blk, 0, s>>>(a);
+        }
+    }
+    CK(cudaGetLastError());
+}
+
+void Engine::inject(const DevInj &inj, const float *src_dev, int it, float *next[3])
+{
+    cudaStream_t s = (cudaStream_t)stream_;
+    StepArgs a = make_step_args(pb_, model_.as<float>(), sdiv_ptr_, taper_ptr_, scale_);
+    const int nc = pb_.ncomp();
+    for (int c = 0; c < nc; c++) a.next[c] = next[c];
+    for (int c = 0; c < nc; c++) {
+        if (inj.n[c] == 0) continue;
+        k_inject<<<(inj.n[c] + 127) / 128, 128, 0, s>>>(a, c, inj.gidx[c].as<int64_t>(), inj.trace[c].as<int>(),
+                                                         inj.w[c].as<float>(), inj.n[c], src_dev, pb_.nt, it);
+    }
+    CK(cudaGetLastError());
+}
+
+void Engine::extract(const DevExt &ext, float *curr[3], float *rcv_dev, int nrcomp, int it)
+{
+    cudaStream_t s = (cudaStream_t)stream_;
+    for (int c = 0; c < nrcomp; c++)
+        k_extract<<<(ext.nrec + 127) / 128, 128, 0, s>>>(curr[c], ext.gidx.as<int64_t>(), ext.w.as<float>(), ext.nrec,
+                                                          rcv_dev + (int64_t)c * ext.nrec * pb_.nt, pb_.nt, it);
+    CK(cudaGetLastError());
+}
+
+void Engine::forward(const InjTable &inj, int ntrace, const float *src, const ExtTable &ext, int nrcomp, float *rcv,
+                     bool store)
+{
+    CK(cudaSetDevice(device_));
+    cudaStream_t s = (cudaStream_t)stream_;
+    const int64_t n = pb_.nxyz();
+    const int nc = pb_.ncomp();
+    upload_inj(inj, ntrace, inj_);
+    src_dev_.alloc(sizeof(float) * ntrace * pb_.nt);
+    CK(cudaMemcpyAsync(src_dev_.p, src, src_dev_.bytes, cudaMemcpyHostToDevice, s));
+    ext_.nrec = ext.nrec;
+    ext_.gidx.alloc(sizeof(int64_t) * ext.gidx.size());
+    ext_.w.alloc(sizeof(float) * ext.w.size());
+    if (ext.nrec) {
+        CK(cudaMemcpyAsync(ext_.gidx.p, ext.gidx.data(), ext_.gidx.bytes, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(ext_.w.p, ext.w.data(), ext_.w.bytes, cudaMemcpyHostToDevice, s));
+    }
+    rcv_dev_.alloc(sizeof(float) * (size_t)nrcomp * ext.nrec * pb_.nt);
+    rcv_dev_.zero(s);
+
+    snaps_valid_ = false;
+    const bool keep = store && pb_.sub > 0;
+    if (keep) {
+        nsnap_ = 1 + pb_.nt / pb_.sub;
+        snaps_.alloc(sizeof(float) * (size_t)nsnap_ * nc * n);
+        snaps_.zero(s);
+    }
+
+    fields_.zero(s);
+    float *base = fields_.as<float>();
+    float *lv[3][3];
+    for (int l = 0; l < 3; l++)
+        for (int c = 0; c < 3; c++) lv[l][c] = base + ((int64_t)l * nc + (c < nc ? c : 0)) * n;
+    float **prev = lv[0], **curr = lv[1], **next = lv[2];
+    init_prev(inj_, src_dev_.as<float>(), prev);
+
+    auto snap = [&](int k, float **u) {
+        if (k > nsnap_ - 1) return;
+        CK(cudaMemcpyAsync(snaps_.as<float>() + (int64_t)k * nc * n, u[0], sizeof(float) * nc * n,
+                           cudaMemcpyDeviceToDevice, s));
+    };
+    for (int it = 0; it < pb_.nt - 1; it++) {
+        if (keep && it % pb_.sub == 0) snap(it / pb_.sub, curr);
+        extract(ext_, curr, rcv_dev_.as<float>(), nrcomp, it);
+        step(it, prev, curr, next, it > 0);
+        inject(inj_, src_dev_.as<float>(), it, next);
+        float **t = prev;
+        prev = curr;
+        curr = next;
+        next = t;
+    }
+    if (keep && (pb_.nt - 1) % pb_.sub == 0) snap((pb_.nt - 1) / pb_.sub, curr);
+    extract(ext_, curr, rcv_dev_.as<float>(), nrcomp, pb_.nt - 1);
+    CK(cudaMemcpyAsync(rcv, rcv_dev_.p, rcv_dev_.bytes, cudaMemcpyDeviceToHost, s));
+    sync();
+    snaps_valid_ = keep;
+}
+
+void Engine::image(int itl, float *curr[3], float *prevs[3])
+{
+    cudaStream_t s = (cudaStream_t)stream_;
+    const int64_t n = pb_.nxyz();
+    const int nc = pb_.ncomp();
+    ImageArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.g = Dims{pb_.nx, pb_.ny, pb_.nz};
+    a.dx = pb_.dx;
+    a.dy = pb_.dy;
+    a.dz = pb_.dz;
+    a.dtimg = pb_.sub * pb_.dt;
+    a.itl = itl;
+    a.last = pb_.nt / pb_.sub;
+    for (int k = 0; k < pb_.nmodels; k++) a.m[k] = model_.as<float>() + k * n;
+    for (int l = 0; l < 3; l++) {
+        const int k = itl - 1 + l;
+        const int kk = std::min(std::max(k, 0), nsnap_ - 1);
+        for (int c = 0; c < 3; c++) a.fwd[l][c] = snaps_.as<float>() + ((int64_t)kk * nc + (c < nc ? c : 0)) * n;
+    }
+    for (int c = 0; c < 3; c++) {
+        a.adj[c] = curr[c];
+        a.lag[c] = prevs[c];
+        a.grad[c] = grad_.as<double>() + (int64_t)(c < (pb_.nmodels == 2 ? 2 : 3) ? c : 0) * n;
+    }
+    const dim3 blk(BZ, BX, BY), grd = grid_of(a.g);
+    if (pb_.nmodels == 2) k_acoustic_image<<<grd, blk, 0, s>>>(a);
+    else if (pb_.nmodels == 3) k_elastic_image<ELASTIC><<<grd, blk, 0, s>>>(a);
+    else k_elastic_image<VTI><<<grd, blk, 0, s>>>(a);
+    CK(cudaGetLastError());
+}
+
+void Engine::adjoint(const InjTable &inj, int ntrace, const float *adj_src, float *grad)
+{
+    CK(cudaSetDevice(device_));
+    if (!snaps_valid_) throw FwiError(FWI_ERR_STATE, "adjoint needs the snapshots of a preceding forward with sub > 0");
+    cudaStream_t s = (cudaStream_t)stream_;
+    const int64_t n = pb_.nxyz();
+    const int nc = pb_.ncomp();
+    const int nm = std::min(3, pb_.nmodels);
+    DevInj dinj;
+    upload_inj(inj, ntrace, dinj);
+    DevBuf asrc(sizeof(float) * ntrace * pb_.nt);
+    CK(cudaMemcpyAsync(asrc.p, adj_src, asrc.bytes, cudaMemcpyHostToDevice, s));
+    grad_.alloc(sizeof(double) * nm * n);
+    grad_.zero(s);
+
+    fields_.zero(s);
+    float *base = fields_.as<float>();
+    float *lv[3][3];
+    for (int l = 0; l < 3; l++)
+        for (int c = 0; c < 3; c++) lv[l][c] = base + ((int64_t)l * nc + (c < nc ? c : 0)) * n;
+    float **prev = lv[0], **curr = lv[1], **next = lv[2];
+    init_prev(dinj, asrc.as<float>(), prev);
+    const int sub = pb_.sub;
+    for (int it = 0; it < pb_.nt - 1; it++) {
+        if ((pb_.nt - 1 - it) % sub == 0 && it != 0) image((pb_.nt - 1 - it) / sub, curr, prev);
+        step(it, prev, curr, next, it > 0);
+        inject(dinj, asrc.as<float>(), it, next);
+        float **t = prev;
+        prev = curr;
+        curr = next;
+        next = t;
+    }
+    image(0, curr, prev);
+    DevBuf gf(sizeof(float) * nm * n);
+    k_d2f<<<(unsigned)((nm * n + 255) / 256), 256, 0, s>>>(grad_.as<double>(), gf.as<float>(), nm * n);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(grad, gf.p, gf.bytes, cudaMemcpyDeviceToHost, s));
+    sync();
+}
+
+}  // namespace fwi

@@ -1,0 +1,124 @@
+/*
+ * fwi3d_gpu.h -- C ABI of the B200 wave-propagation engine (libfwi3d_b200.so).
+ *
+ * Drop-in for the time-stepping hot path of nmbader/fwi3d: the acoustic
+ * variable-density, elastic isotropic and elastic VTI propagators and their
+ * adjoint-state gradients.  Entry points replace, one for one, the reference
+ * operator calls a caller makes:
+ *
+ *   fwi_op_create     <- nl_we_op_{a,e,vti}(domain, allsrc, s, par)
+ *                        src/include/we_op.hpp:59-79 (elastic), :106 (VTI), :139-151 (acoustic)
+ *   fwi_op_forward    <- nl_we_op_e::apply_forward(add, pmod, pdat)
+ *                        we_op.hpp:50, src/cpp/we_op.cpp:872-946
+ *   fwi_op_jacobianT  <- nl_we_op_e::apply_jacobianT(add, pmod, pmod0, pdat)
+ *                        we_op.hpp:51, src/cpp/we_op.cpp:948-1078
+ *   fwi_op_destroy    <- delete op   (src/main/we_modeling.cpp:98, src/cpp/optimization.cpp:183)
+ *   fwi_forward_batch <- the rank-strided shot loop of WE_MODELING_3D
+ *                        (src/main/we_modeling.cpp:72-109) for shots sharing one model
+ *
+ * Errors: the reference aborts through successCheck -> exit(123)
+ * (src/include/misc.hpp:4-12).  Here every call returns FWI_OK (0) or a negative
+ * status and leaves a message for fwi_last_error().
+ *
+ * Conventions (the reference's): units km, km/s, g/cc, s; model layout
+ * [nmodels][ny][nx][nz] (z fastest) holding vp,rho (nmodels=2), vp,vs,rho (3) or
+ * vp,vs,rho,delta,epsilon,gamma (6); data layout [nrcomp][nr][nt_data]; wavelet
+ * [ncomp][nt_data] or a single trace duplicated as analyzeWavelet does
+ * (we_op.cpp:138-232).  Host buffers are owned by the caller; the operator owns
+ * its device model, wavefields, snapshots and traces.
+ */
+#ifndef FWI3D_GPU_H
+#define FWI3D_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FWI_OK 0
+#define FWI_ERR_ARG (-1)         /* bad shape / argument (reference: successCheck) */
+#define FWI_ERR_OOM (-2)         /* device memory exhausted */
+#define FWI_ERR_CUDA (-3)        /* CUDA runtime or launch failure */
+#define FWI_ERR_NAN (-4)         /* non-finite value in model or wavefield */
+#define FWI_ERR_STATE (-5)       /* adjoint requested without stored forward state */
+#define FWI_ERR_UNSUPPORTED (-6) /* option the GPU path does not implement */
+#define FWI_ERR_NOGPU (-7)       /* no CUDA device */
+
+/* Computational grid: model axes Z (fast), X, Y (src/cpp/we_op.cpp:28-30). */
+typedef struct fwi_grid {
+    int nx, ny, nz;
+    float ox, oy, oz;
+    float dx, dy, dz;
+} fwi_grid;
+
+/* Propagation knobs; field meaning and defaults as in `struct param`
+ * (src/include/param.hpp:8-71).  fwi_param_default() fills the defaults. */
+typedef struct fwi_param {
+    float courant, dt;        /* dt <= 0: CFL-derived (analyzeModel, we_op.cpp:405-425) */
+    int sub;                  /* snapshot/imaging sub-sampling; <0: derived; 0: none */
+    int resampling_linear;    /* 0 sinc (default), 1 linear */
+    int sinc_half_length;
+    int mt;                   /* moment-tensor source (6 components) */
+    float fangle, fazimuth;   /* vector-force direction */
+    float mxx, myy, mzz, mxy, mxz, myz;
+    int seismotype;           /* 0 displacement/pressure, 1 velocity (time derivative) */
+    float gl;                 /* DAS gauge length; > 0 unsupported on the GPU path */
+    int bc[6];                /* top, bottom, left, right, front, back: 0 none, 1 free, 2 absorbing, 3 rigid */
+    int taper[6];
+    float free_surface_stiffness, taper_strength;
+    float vpmin, vpmax, vsmin, vsmax, rhomin, rhomax;
+    float deltamin, deltamax, epsilonmin, epsilonmax, gammamin, gammamax;
+    int soft_clip;
+    int verbose;
+    /* GPU-specific */
+    int grad_fp64;            /* accumulate imaging sums in FP64 (default 1) */
+} fwi_param;
+
+void fwi_param_default(fwi_param *p);
+
+typedef struct fwi_op fwi_op;
+
+typedef struct fwi_op_info {
+    float dt;       /* propagation time step */
+    int nt;         /* propagation samples */
+    int sub;        /* snapshot interval */
+    int nscomp;     /* source components (1, 3 or 6) */
+    int nrcomp;     /* receiver components (1 or 3) */
+    int nr;         /* receivers */
+    int64_t device_bytes;
+} fwi_op_info;
+
+/* One shot on one device.  `rxyz` is [nr][5] (x, y, z, dip, azimuth), as the
+ * reference's par.rxyz[s]; `sxyz` is [3]. */
+int fwi_op_create(fwi_op **op, int device, const fwi_grid *grid, int nmodels, const fwi_param *par,
+                  const float *wavelet, int wavelet_ncomp, int nt_data, float dt_data, const float *sxyz, int nr,
+                  const float *rxyz);
+
+/* data (+)= F(model); keeps the forward snapshots for a following jacobianT when sub > 0. */
+int fwi_op_forward(fwi_op *op, int add, const float *model, float *data);
+
+/* grad (+)= J^T data at model0 (needs the preceding forward of the same op with sub > 0). */
+int fwi_op_jacobianT(fwi_op *op, int add, float *grad, const float *model0, const float *data);
+
+int fwi_op_get_info(const fwi_op *op, fwi_op_info *info);
+void fwi_op_destroy(fwi_op *op);
+
+/* Modeling of nshots shots that share one model, batched on the device.
+ * sxyz: [nshots][3]; nr: receivers per shot (same for all shots);
+ * rxyz: [nshots][nr][5]; data: [nshots][nrcomp][nr][nt_data]. */
+int fwi_forward_batch(int device, const fwi_grid *grid, int nmodels, const fwi_param *par, const float *model,
+                      const float *wavelet, int wavelet_ncomp, int nt_data, float dt_data, int nshots,
+                      const float *sxyz, int nr, const float *rxyz, float *data);
+
+/* Message of the last failing call on this thread. */
+const char *fwi_last_error(void);
+
+/* Library version string. */
+const char *fwi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FWI3D_GPU_H */
