@@ -1,0 +1,319 @@
+#!/usr/bin/env python
+"""Benchmark of the wave-propagation hot path on B200 GPUs.
+
+Workload (N=1): elastic isotropic modeling on a 256^3 grid (8 m spacing,
+dt 0.6 ms), 8 shots with explosive moment-tensor sources batched on the shared
+model, 128x128 three-component velocity receivers, free-surface top and
+absorbing sides with 20-point tapers -- seeded synthetic layered model (the
+reference publishes no dataset).  One bench step = one time step of the
+8-shot batch = 8 * 256^3 grid-point updates.
+
+Our arm: K time steps timed with CUDA events on the engine's stream after W
+warm-up steps; all state resident in HBM (the working set, ~9 GB, is far
+larger than L2, so no flush is needed between steps).  e2e: the public C-ABI
+batch call (fwi_forward_batch) with host buffers on a 300-step time axis,
+host<->device copies and host-side preparation inside the timed region.
+
+Reference arm (--impl reference): the reference's own CPU code (built from
+its sources into oracle/_ref) on the host cores, one shot of the same
+workload over a bounded time window.
+
+Multi-GPU (torchrun): shots are independent -- every rank runs its own 8-shot
+batch (weak scaling), no collective on the data path; the timing is the max
+over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_UPDATE = 48  # algorithmic FP32 traffic of one elastic point update (lambda, mu, rho, prev x3, curr x3, next x3)
+
+
+_CACHE = {}
+
+
+def workload(n=256, nshots=8, nsteps=3000):
+    """The seeded survey; the model is generated once per grid size and the
+    wavelet cut to ``nsteps`` + 1 samples."""
+    from fwi3d_b200 import synth
+
+    if n not in _CACHE:
+        _CACHE[n] = synth.elastic_layered(n=n, nsteps=4000, nshots=8)
+    base = _CACHE[n]
+    sv = base.shot(0) if nshots == 1 else base
+    sv = synth.Survey(sv.name, sv.nmodels, sv.nx, sv.ny, sv.nz, sv.dx, sv.dy, sv.dz, sv.model,
+                      np.ascontiguousarray(base.wavelet[:nsteps + 1]), sv.dt_data, sv.par.copy())
+    if nshots != 1:
+        sv.par.sxyz = sv.par.sxyz[:nshots]
+        sv.par.rxyz = sv.par.rxyz[:nshots]
+        sv.par.ns = nshots
+    return sv
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_per_update():
+    """DRAM bytes per grid-point update of the step kernels, from the committed
+    ncu summary (profiles/ncu_traffic.txt: key=value lines)."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    try:
+        vals = {}
+        with open(path) as f:
+            for line in f:
+                if "=" in line and not line.startswith("#"):
+                    k, v = line.strip().split("=", 1)
+                    vals[k.strip()] = v.strip()
+        return float(vals["dram_bytes_per_update"]), vals.get("kernel", "")
+    except Exception:
+        return None, ""
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 7:
+                    continue
+                try:
+                    sm.append(float(parts[0]))
+                    smax = float(parts[1])
+                except ValueError:
+                    continue
+                for name, v in zip(names, parts[3:7]):
+                    if v.lower() == "active":
+                        reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference(n_steps, threads, n=256):
+    """Reference CPU code (oracle/_ref, built from the reference sources): one
+    shot of the workload over an n_steps window; returns pt-updates/s."""
+    from oracle import refpy
+
+    sv = workload(n=n, nshots=1, nsteps=n_steps)
+    t0 = time.perf_counter()
+    refpy.modeling(sv, shot=0, precision="fp32", nthreads=threads)
+    dt = time.perf_counter() - t0
+    return sv.nxyz * n_steps / dt, dt
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    k = min(args.steps, args.ref_cap)
+    if args.warmup > 0:
+        cpu_reference(min(args.warmup, 3), threads)
+    value, secs = cpu_reference(k, threads)
+    sample = (f"1 shot of the 256^3 elastic workload, {k}-step window, whole apply_forward call "
+              f"(model analysis and setup included), OMP threads={threads}")
+    line = {
+        "impl": "reference", "metric": "grid-pt updates/s", "value": value, "unit": "pt/s", "n_gpus": args.gpus,
+        "steps": k, "warmup": args.warmup, "ms_per_step": secs * 1e3 / k, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "elastic iso modeling 256^3, 8 shots (CPU: 1-shot bounded window)",
+                   "grid": [256, 256, 256], "shots": 8, "parallelism": "cpu"},
+        "cpu_baseline": {"value": value, "unit": "pt/s", "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "pt/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, world, local):
+    import ctypes as C
+
+    import torch
+
+    from fwi3d_b200 import _lib, ops
+
+    torch.cuda.set_device(local)
+    lib = _lib.load()
+    sv = workload(n=args.n, nshots=args.shots, nsteps=max(args.steps + args.warmup + 1, 301))
+    ns = len(sv.par.sxyz)
+    dom = ops.Domain(sv.nx, sv.ny, sv.nz, sv.dx, sv.dy, sv.dz, 3)
+    nr = len(sv.par.rxyz[0])
+    w = np.ascontiguousarray(sv.wavelet, dtype=np.float32)
+    sx = np.ascontiguousarray(np.asarray(sv.par.sxyz, dtype=np.float32))
+    rx = np.ascontiguousarray(np.asarray(sv.par.rxyz, dtype=np.float32))
+    model = np.ascontiguousarray(sv.model, dtype=np.float32)
+    cp = ops.to_cparam(sv.par)
+
+    h = C.c_void_p()
+    _lib.check(lib.fwi_batch_create(C.byref(h), local, C.byref(dom.grid()), 3, C.byref(cp), _lib.fptr(model),
+                                    _lib.fptr(w), 1, w.shape[-1], sv.dt_data, ns, _lib.fptr(sx), nr, _lib.fptr(rx)))
+    sp = C.c_void_p()
+    _lib.check(lib.fwi_batch_stream(h, C.byref(sp)))
+    stream = torch.cuda.ExternalStream(sp.value)
+    info = _lib.OpInfo()
+    lps = C.c_int()
+    _lib.check(lib.fwi_batch_get_info(h, C.byref(info), C.byref(lps)))
+    _lib.check(lib.fwi_batch_reset(h))
+    _lib.check(lib.fwi_batch_run(h, args.warmup))
+    _lib.check(lib.fwi_batch_sync(h))
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    _lib.check(lib.fwi_batch_run(h, args.steps))
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+        torch.distributed.barrier()
+    lib.fwi_batch_destroy(h)
+
+    units_per_step = ns * sv.nxyz  # per rank
+    value = world * units_per_step * args.steps / (ms / 1e3)
+    ms_step = ms / args.steps
+    peak, peak_kind = peaks()
+    achieved = BYTES_PER_UPDATE * units_per_step / (ms_step / 1e3) / 1e9
+    tpu, tkernel = traffic_per_update()
+
+    # e2e through the public C-ABI call, host buffers, 300-step time axis
+    e2e = None
+    if not args.no_e2e:
+        sv_e = workload(n=args.n, nshots=args.shots, nsteps=300)
+        we = np.ascontiguousarray(sv_e.wavelet, dtype=np.float32)
+        out = np.zeros((ns, 3, nr, we.shape[-1]), dtype=np.float32)
+        if world > 1:
+            torch.distributed.barrier()
+        t0 = time.perf_counter()
+        _lib.check(lib.fwi_forward_batch(local, C.byref(dom.grid()), 3, C.byref(cp), _lib.fptr(model), _lib.fptr(we),
+                                         1, we.shape[-1], sv_e.dt_data, ns, _lib.fptr(sx), nr, _lib.fptr(rx),
+                                         _lib.fptr(out)))
+        te = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([te], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            te = float(t.item())
+        nsteps_e = we.shape[-1] - 1
+        h2d = model.nbytes + we.nbytes + sx.nbytes + rx.nbytes
+        e2e = {"value": world * units_per_step * nsteps_e / te, "unit": "pt/s",
+               "h2d_bytes_per_step": h2d / nsteps_e, "d2h_bytes_per_step": out.nbytes / nsteps_e,
+               "steps": nsteps_e, "seconds": te}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        v, secs = cpu_reference(args.cpu_steps, threads)
+        cpu = {"value": v, "unit": "pt/s", "cores": threads, "kind": "reference",
+               "sample": f"reference CPU build, 1 shot of the 256^3 elastic workload, {args.cpu_steps}-step window "
+                         f"({secs:.1f} s, setup included), OMP threads={threads}"}
+
+    if rank == 0:
+        line = {
+            "metric": "grid-pt updates/s", "value": value, "unit": "pt/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered model, Ricker sources)",
+            "config": {"workload": f"elastic iso modeling {args.n}^3, 8 m, dt 0.6 ms, {ns} moment-tensor shots "
+                                   f"batched on the shared model, {nr} 3-C receivers per shot",
+                       "grid": [args.n] * 3, "shots_per_gpu": ns, "receivers_per_shot": nr,
+                       "parallelism": f"shots x{world} (weak)", "l2": "working set >> L2 (no flush needed)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": (tpu * units_per_step if tpu else None),
+                         "algorithmic_bytes_per_update": BYTES_PER_UPDATE,
+                         "note": "per time step of the batch (all kernels of the step)" + (
+                             f"; traffic from ncu: {tkernel}" if tkernel else "")},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(lps.value) * args.steps, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=16)
+    ap.add_argument("--ref-cap", type=int, default=40, help="max time steps of the CPU reference window")
+    ap.add_argument("--n", type=int, default=256, help="grid points per axis (profiling runs use smaller grids)")
+    ap.add_argument("--shots", type=int, default=8)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        return run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch
+
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -25,7 +25,9 @@ FWI_ERR_NOGPU = -7
 # Every entry point declared in include/fwi3d_gpu.h.
 EXPORTS = [
     "fwi_param_default", "fwi_op_create", "fwi_op_forward", "fwi_op_jacobianT", "fwi_op_get_info",
-    "fwi_op_destroy", "fwi_forward_batch", "fwi_last_error", "fwi_version",
+    "fwi_op_destroy", "fwi_forward_batch", "fwi_batch_create", "fwi_batch_reset", "fwi_batch_run",
+    "fwi_batch_sync", "fwi_batch_stream", "fwi_batch_traces", "fwi_batch_get_info", "fwi_batch_destroy",
+    "fwi_last_error", "fwi_version",
 ]
 
 
@@ -55,7 +57,7 @@ class CParam(C.Structure):
         ("rhomin", C.c_float), ("rhomax", C.c_float),
         ("deltamin", C.c_float), ("deltamax", C.c_float), ("epsilonmin", C.c_float),
         ("epsilonmax", C.c_float), ("gammamin", C.c_float), ("gammamax", C.c_float),
-        ("soft_clip", C.c_int), ("verbose", C.c_int), ("grad_fp64", C.c_int),
+        ("soft_clip", C.c_int), ("verbose", C.c_int),
     ]
 
 
@@ -92,6 +94,22 @@ def load() -> C.CDLL:
     lib.fwi_forward_batch.argtypes = [C.c_int, C.POINTER(Grid), C.c_int, C.POINTER(CParam), fp, fp, C.c_int, C.c_int,
                                       C.c_float, C.c_int, fp, C.c_int, fp, fp]
     lib.fwi_forward_batch.restype = C.c_int
+    lib.fwi_batch_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(Grid), C.c_int, C.POINTER(CParam), fp, fp,
+                                     C.c_int, C.c_int, C.c_float, C.c_int, fp, C.c_int, fp]
+    lib.fwi_batch_create.restype = C.c_int
+    for name in ("fwi_batch_reset", "fwi_batch_sync"):
+        getattr(lib, name).argtypes = [vp]
+        getattr(lib, name).restype = C.c_int
+    lib.fwi_batch_run.argtypes = [vp, C.c_int]
+    lib.fwi_batch_run.restype = C.c_int
+    lib.fwi_batch_stream.argtypes = [vp, C.POINTER(vp)]
+    lib.fwi_batch_stream.restype = C.c_int
+    lib.fwi_batch_traces.argtypes = [vp, fp]
+    lib.fwi_batch_traces.restype = C.c_int
+    lib.fwi_batch_get_info.argtypes = [vp, C.POINTER(OpInfo), C.POINTER(C.c_int)]
+    lib.fwi_batch_get_info.restype = C.c_int
+    lib.fwi_batch_destroy.argtypes = [vp]
+    lib.fwi_batch_destroy.restype = None
     lib.fwi_last_error.restype = C.c_char_p
     lib.fwi_version.restype = C.c_char_p
     _lib = lib

@@ -99,7 +99,6 @@ struct fwi_op {
         std::memcpy(p.taper, par.taper, sizeof(p.taper));
         p.taper_strength = par.taper_strength;
         p.free_surface_stiffness = nmodels == 2 ? std::max(par.free_surface_stiffness, 1.0f) : par.free_surface_stiffness;
-        p.grad_fp64 = par.grad_fp64 != 0;
         const bool same = eng && pb.nt == p.nt && pb.dt == p.dt && pb.sub == p.sub;
         pb = p;
         if (!same) eng.reset(new Engine(device, pb));
@@ -113,6 +112,19 @@ struct fwi_op {
         for (int r = 0; r < nr; r++) l[r] = Loc{rxyz[5 * r], rxyz[5 * r + 1], rxyz[5 * r + 2]};
         return l;
     }
+};
+
+struct fwi_batch {
+    int device = 0;
+    fwi_grid grid{};
+    int nmodels = 3;
+    fwi_param par{};
+    int nt_data = 0;
+    float dt_data = 0.f;
+    int nshots = 1, nr = 0, nscomp = 1, nrcomp = 1;
+    int it = 0;  // time steps run since reset
+    Problem pb{};
+    std::unique_ptr<Engine> eng;
 };
 
 extern "C" {
@@ -149,7 +161,6 @@ void fwi_param_default(fwi_param *p)
     p->gammamax = 1.f;
     p->soft_clip = 0;
     p->verbose = 0;
-    p->grad_fp64 = 1;
 }
 
 const char *fwi_last_error(void) { return g_err.c_str(); }
@@ -223,7 +234,7 @@ int fwi_op_forward(fwi_op *op, int add, const float *model, float *data)
         const int ncr = op->ncomp();
         const int ntr = ncr * op->nr;
         std::vector<float> rcv((size_t)ntr * nt);
-        op->eng->forward(it, op->nscomp, src.data(), et, ncr, rcv.data(), pb.sub > 0);
+        op->eng->forward(it, op->nscomp, src.data(), et, rcv.data(), pb.sub > 0);
         if (!finite_all(rcv.data(), (int64_t)rcv.size())) throw FwiError(FWI_ERR_NAN, "non-finite values in the traces");
         if (op->par.seismotype == 1) {
             // particle velocity (we_op.cpp:932-938)
@@ -314,25 +325,179 @@ int fwi_op_get_info(const fwi_op *op, fwi_op_info *info)
 
 void fwi_op_destroy(fwi_op *op) { delete op; }
 
+int fwi_batch_create(fwi_batch **out, int device, const fwi_grid *grid, int nmodels, const fwi_param *par,
+                     const float *model, const float *wavelet, int wavelet_ncomp, int nt_data, float dt_data,
+                     int nshots, const float *sxyz, int nr, const float *rxyz)
+{
+    if (!out || !grid || !par || !model || !wavelet || !sxyz || !rxyz || nshots < 1 || nr < 1)
+        return fail(FWI_ERR_ARG, "null argument, no shot or no receiver");
+    *out = nullptr;
+    if (nmodels != 2 && nmodels != 3 && nmodels != 6)
+        return fail(FWI_ERR_ARG, "The model must contain 2, 3, or 6 parameters");
+    if (par->gl > 0) return fail(FWI_ERR_UNSUPPORTED, "DAS receivers (gl > 0) are not implemented on the GPU path");
+    return guarded([&] {
+        std::unique_ptr<fwi_batch> b(new fwi_batch());
+        b->device = device;
+        b->grid = *grid;
+        b->nmodels = nmodels;
+        b->par = *par;
+        if (nmodels == 2) b->par.mt = 0;
+        b->nt_data = nt_data;
+        b->dt_data = dt_data;
+        b->nshots = nshots;
+        b->nr = nr;
+        b->nscomp = nmodels == 2 ? 1 : (b->par.mt ? 6 : 3);
+        b->nrcomp = nmodels == 2 ? 1 : 3;
+        const int64_t n = (int64_t)grid->nx * grid->ny * grid->nz;
+        if (!finite_all(model, nmodels * n)) throw FwiError(FWI_ERR_NAN, "model contains non-finite values");
+        std::vector<float> m(model, model + nmodels * n);
+        TimeAxis ta = analyze_model(m, nmodels, grid->nx, grid->ny, grid->nz, grid->dx, grid->dy, grid->dz, nt_data,
+                                    dt_data, b->par);
+        convert_model(m, nmodels, n);
+        Problem &p = b->pb;
+        p.nmodels = nmodels;
+        p.nx = grid->nx;
+        p.ny = grid->ny;
+        p.nz = grid->nz;
+        p.dx = grid->dx;
+        p.dy = grid->dy;
+        p.dz = grid->dz;
+        p.dt = ta.dt;
+        p.nt = ta.nt;
+        p.sub = 0;
+        for (int f = 0; f < 6; f++) p.bc[f] = std::max(0, b->par.bc[f]);
+        std::memcpy(p.taper, b->par.taper, sizeof(p.taper));
+        p.taper_strength = b->par.taper_strength;
+        p.free_surface_stiffness =
+            nmodels == 2 ? std::max(b->par.free_surface_stiffness, 1.0f) : b->par.free_surface_stiffness;
+        p.nshots = nshots;
+        b->eng.reset(new Engine(device, p));
+        b->eng->set_model(m.data());
+        // sources: the same wavelet for every shot, resampled once
+        std::vector<float> w = expand_wavelet(wavelet, wavelet_ncomp, nt_data, nmodels, b->par);
+        std::vector<float> w1((size_t)b->nscomp * p.nt);
+        const bool sinc = b->par.resampling_linear == 0;
+        resample_forward(sinc, b->par.sinc_half_length, w.data(), nt_data, dt_data, w1.data(), p.nt, p.dt, b->nscomp);
+        std::vector<float> src((size_t)nshots * b->nscomp * p.nt);
+        for (int s = 0; s < nshots; s++) std::memcpy(src.data() + (size_t)s * w1.size(), w1.data(), sizeof(float) * w1.size());
+        const int nc = p.ncomp();
+        InjTable all;
+        ExtTable ext;
+        ext.nrec = nshots * nr;
+        for (int s = 0; s < nshots; s++) {
+            PointOp inj = make_delta(p.nx, p.ny, p.nz, p.dx, p.dy, p.dz, grid->ox, grid->oy, grid->oz,
+                                     {Loc{sxyz[3 * s], sxyz[3 * s + 1], sxyz[3 * s + 2]}}, b->par.mt != 0);
+            InjTable t = injection_table(inj, p.nx, p.ny, p.nz, nc);
+            for (int c = 0; c < nc; c++)
+                for (size_t k = 0; k < t.gidx[c].size(); k++) {
+                    all.gidx[c].push_back(t.gidx[c][k] + s * n);
+                    all.trace[c].push_back(t.trace[c][k] + s * b->nscomp);
+                    all.w[c].push_back(t.w[c][k]);
+                }
+            std::vector<Loc> rl(nr);
+            const float *rs = rxyz + (size_t)5 * nr * s;
+            for (int r = 0; r < nr; r++) rl[r] = Loc{rs[5 * r], rs[5 * r + 1], rs[5 * r + 2]};
+            PointOp rop = make_delta(p.nx, p.ny, p.nz, p.dx, p.dy, p.dz, grid->ox, grid->oy, grid->oz, rl, false);
+            ExtTable e = extraction_table(rop, p.nx, p.ny, p.nz);
+            for (auto g : e.gidx) ext.gidx.push_back(g + s * n);
+            ext.w.insert(ext.w.end(), e.w.begin(), e.w.end());
+        }
+        b->eng->set_sources(all, nshots * b->nscomp, src.data());
+        b->eng->set_receivers(ext, nr);
+        b->eng->sync();
+        *out = b.release();
+    });
+}
+
+int fwi_batch_reset(fwi_batch *b)
+{
+    if (!b) return fail(FWI_ERR_ARG, "null batch");
+    return guarded([&] {
+        b->eng->reset();
+        b->it = 0;
+    });
+}
+
+int fwi_batch_run(fwi_batch *b, int nsteps)
+{
+    if (!b || nsteps < 0) return fail(FWI_ERR_ARG, "bad argument");
+    return guarded([&] {
+        const int k = std::min(nsteps, b->pb.nt - 1 - b->it);
+        b->eng->run(b->it, k);
+        b->it += k;
+    });
+}
+
+int fwi_batch_sync(fwi_batch *b)
+{
+    if (!b) return fail(FWI_ERR_ARG, "null batch");
+    return guarded([&] { b->eng->sync(); });
+}
+
+int fwi_batch_stream(fwi_batch *b, void **stream)
+{
+    if (!b || !stream) return fail(FWI_ERR_ARG, "null argument");
+    *stream = b->eng->stream();
+    return FWI_OK;
+}
+
+int fwi_batch_traces(fwi_batch *b, float *data)
+{
+    if (!b || !data) return fail(FWI_ERR_ARG, "null argument");
+    return guarded([&] {
+        if (b->it != b->pb.nt - 1) throw FwiError(FWI_ERR_STATE, "the time axis has not been run to the end");
+        b->eng->extract_last();
+        const int nt = b->pb.nt;
+        const int ntr = b->nrcomp * b->nr;
+        std::vector<float> rcv((size_t)b->nshots * ntr * nt);
+        b->eng->copy_traces(rcv.data());
+        const bool sinc = b->par.resampling_linear == 0;
+        const float alpha = b->pb.dt / b->dt_data;
+        for (int s = 0; s < b->nshots; s++) {
+            float *r = rcv.data() + (size_t)s * ntr * nt;
+            std::vector<float> v;
+            if (b->par.seismotype == 1) {
+                v.resize((size_t)ntr * nt);
+                apply_dt(false, r, v.data(), ntr, nt, b->pb.dt);
+                r = v.data();
+            }
+            for (size_t i = 0; i < (size_t)ntr * nt; i++) r[i] *= alpha;
+            float *d = data + (size_t)s * ntr * b->nt_data;
+            std::fill(d, d + (size_t)ntr * b->nt_data, 0.f);
+            resample_adjoint(sinc, b->par.sinc_half_length, d, b->nt_data, b->dt_data, r, nt, b->pb.dt, ntr);
+        }
+    });
+}
+
+int fwi_batch_get_info(const fwi_batch *b, fwi_op_info *info, int *launches)
+{
+    if (!b || !info) return fail(FWI_ERR_ARG, "null argument");
+    info->dt = b->pb.dt;
+    info->nt = b->pb.nt;
+    info->sub = 0;
+    info->nscomp = b->nscomp;
+    info->nrcomp = b->nrcomp;
+    info->nr = b->nr;
+    info->device_bytes = b->eng->device_bytes();
+    if (launches) *launches = b->eng->launches_per_step();
+    return FWI_OK;
+}
+
+void fwi_batch_destroy(fwi_batch *b) { delete b; }
+
 int fwi_forward_batch(int device, const fwi_grid *grid, int nmodels, const fwi_param *par, const float *model,
                       const float *wavelet, int wavelet_ncomp, int nt_data, float dt_data, int nshots,
                       const float *sxyz, int nr, const float *rxyz, float *data)
 {
-    if (!grid || !par || !model || !wavelet || !sxyz || !rxyz || !data || nshots < 1)
-        return fail(FWI_ERR_ARG, "null argument or no shots");
-    const int nrcomp = nmodels == 2 ? 1 : 3;
-    for (int s = 0; s < nshots; s++) {
-        fwi_op *op = nullptr;
-        int rc = fwi_op_create(&op, device, grid, nmodels, par, wavelet, wavelet_ncomp, nt_data, dt_data, sxyz + 3 * s,
-                               nr, rxyz + (size_t)5 * nr * s);
-        if (rc != FWI_OK) return rc;
-        fwi_param p = *par;
-        (void)p;
-        rc = fwi_op_forward(op, 0, model, data + (size_t)s * nrcomp * nr * nt_data);
-        fwi_op_destroy(op);
-        if (rc != FWI_OK) return rc;
-    }
-    return FWI_OK;
+    fwi_batch *b = nullptr;
+    int rc = fwi_batch_create(&b, device, grid, nmodels, par, model, wavelet, wavelet_ncomp, nt_data, dt_data, nshots,
+                              sxyz, nr, rxyz);
+    if (rc != FWI_OK) return rc;
+    rc = fwi_batch_reset(b);
+    if (rc == FWI_OK) rc = fwi_batch_run(b, b->pb.nt - 1);
+    if (rc == FWI_OK) rc = fwi_batch_traces(b, data);
+    fwi_batch_destroy(b);
+    return rc;
 }
 
 }  // extern "C"

@@ -61,113 +61,132 @@ void DevBuf::zero(void *stream)
 }
 
 // ---------------------------------------------------------------------------
-// Kernels
+// Kernels (one thread per grid point; launch grid z covers y-blocks x shots)
 // ---------------------------------------------------------------------------
 namespace {
 
 constexpr int BZ = 32, BX = 4, BY = 2;
 
-__device__ __forceinline__ bool point_of(const Dims &g, int &ix, int &iy, int &iz)
+__device__ __forceinline__ bool point_of(const Dims &g, int nyb, int &ix, int &iy, int &iz, int &s)
 {
     iz = blockIdx.x * BZ + threadIdx.x;
     ix = blockIdx.y * BX + threadIdx.y;
-    iy = blockIdx.z * BY + threadIdx.z;
+    s = blockIdx.z / nyb;
+    iy = (blockIdx.z % nyb) * BY + threadIdx.z;
     return iz < g.nz && ix < g.nx && iy < g.ny;
 }
 
-dim3 grid_of(const Dims &g) { return dim3((g.nz + BZ - 1) / BZ, (g.nx + BX - 1) / BX, (g.ny + BY - 1) / BY); }
+int yblocks(const Dims &g) { return (g.ny + BY - 1) / BY; }
+dim3 grid_of(const Dims &g, int nshots)
+{
+    return dim3((g.nz + BZ - 1) / BZ, (g.nx + BX - 1) / BX, yblocks(g) * nshots);
+}
 
 __global__ void k_acoustic_step(StepArgs a)
 {
-    int ix, iy, iz;
-    if (!point_of(a.g, ix, iy, iz)) return;
-    a.next[0][a.g.idx(ix, iy, iz)] = acoustic_point(a, ix, iy, iz);
+    int ix, iy, iz, s;
+    if (!point_of(a.g, a.nyb, ix, iy, iz, s)) return;
+    const StepArgs b = shot_args(a, s);
+    b.next[0][b.g.idx(ix, iy, iz)] = acoustic_point(b, ix, iy, iz);
 }
 
 template <int PH>
 __global__ void k_elastic_aux(AuxArgs a)
 {
-    int ix, iy, iz;
-    if (!point_of(a.g, ix, iy, iz)) return;
-    elastic_aux_point<PH>(a, ix, iy, iz);
+    int ix, iy, iz, s;
+    if (!point_of(a.g, a.nyb, ix, iy, iz, s)) return;
+    elastic_aux_point<PH>(shot_args(a, s), ix, iy, iz);
 }
 
 template <int PH>
 __global__ void k_elastic_step(StepArgs a)
 {
-    int ix, iy, iz;
-    if (!point_of(a.g, ix, iy, iz)) return;
-    const int64_t i = a.g.idx(ix, iy, iz);
-    const float v0 = elastic_point<PH>(a, 0, ix, iy, iz);
-    const float v1 = elastic_point<PH>(a, 1, ix, iy, iz);
-    const float v2 = elastic_point<PH>(a, 2, ix, iy, iz);
-    a.next[0][i] = v0;
-    a.next[1][i] = v1;
-    a.next[2][i] = v2;
+    int ix, iy, iz, s;
+    if (!point_of(a.g, a.nyb, ix, iy, iz, s)) return;
+    const StepArgs b = shot_args(a, s);
+    const int64_t i = b.g.idx(ix, iy, iz);
+    const float v0 = elastic_point<PH>(b, 0, ix, iy, iz);
+    const float v1 = elastic_point<PH>(b, 1, ix, iy, iz);
+    const float v2 = elastic_point<PH>(b, 2, ix, iy, iz);
+    b.next[0][i] = v0;
+    b.next[1][i] = v1;
+    b.next[2][i] = v2;
 }
 
-// Post-injection: next += taper(scale(dt^2 (w s)/rho)) (elastic) or dt^2 (w s) K (acoustic).
-// Equivalent to the reference's injection into the operator sum before the
-// update (we_op.cpp:691-693) because update, scaling and taper are linear in it.
+// Post-injection: next += taper(scale(dt^2 (w s)/rho)) (elastic) or dt^2 (w s) K
+// (acoustic).  Equivalent to the reference's injection into the operator sum
+// before the update (we_op.cpp:691-693): update, scaling and taper are linear in it.
 __global__ void k_inject(StepArgs a, int c, const int64_t *gidx, const int *trace, const float *w, int n,
                          const float *src, int nt, int it)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    const int64_t i = gidx[k];
-    const float s = w[k] * src[(int64_t)trace[k] * nt + it];
+    const int64_t nxyz = a.g.nxyz();
+    const int64_t gi = gidx[k];
+    const int64_t sh = gi / nxyz;
+    const int64_t i = gi - sh * nxyz;
+    const float sv = w[k] * src[(int64_t)trace[k] * nt + it];
     const int iz = (int)(i % a.g.nz);
     const int ix = (int)((i / a.g.nz) % a.g.nx);
     const int iy = (int)(i / ((int64_t)a.g.nz * a.g.nx));
     const float dt2 = a.dt * a.dt;
-    float v = a.m[2] ? dt2 * s / a.m[2][i] : dt2 * s * a.m[0][i];
+    float v = a.m[2] ? dt2 * sv / a.m[2][i] : dt2 * sv * a.m[0][i];
     v = boundary_scale(a, v, c, ix, iy, iz);
     v = taper(a, v, ix, iy, iz);
-    atomicAdd(&a.next[c][i], v);
+    atomicAdd(&a.next[c][sh * a.sst + i], v);
 }
 
 // Initial condition prev = inject(src[:,0]) then scaled (we_op.cpp:611-619, 1635-1636).
-__global__ void k_inject0(float *prev, const int64_t *gidx, const int *trace, const float *w, int n, const float *src,
-                          int nt)
+__global__ void k_inject0(float *prev, int64_t sst, int64_t nxyz, const int64_t *gidx, const int *trace,
+                          const float *w, int n, const float *src, int nt)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    atomicAdd(&prev[gidx[k]], w[k] * src[(int64_t)trace[k] * nt]);
+    const int64_t gi = gidx[k];
+    const int64_t sh = gi / nxyz;
+    atomicAdd(&prev[sh * sst + (gi - sh * nxyz)], w[k] * src[(int64_t)trace[k] * nt]);
 }
 
-__global__ void k_scale0(float *prev, const float *coef, int64_t n, float dt, int acoustic)
+__global__ void k_scale0(float *prev, int64_t sst, const float *coef, int64_t n, int nshots, float dt, int acoustic)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float p = prev[i];
-    if (p == 0.f) return;
-    if (acoustic) prev[i] = (float)((double)p * (0.5 * (double)coef[i] * dt * dt));
-    else prev[i] = (float)((double)p * (0.5 * dt * dt / (double)coef[i]));
+    for (int s = 0; s < nshots; s++) {
+        float *p = prev + s * sst + i;
+        const float v = *p;
+        if (v == 0.f) continue;
+        if (acoustic) *p = (float)((double)v * (0.5 * (double)coef[i] * dt * dt));
+        else *p = (float)((double)v * (0.5 * dt * dt / (double)coef[i]));
+    }
 }
 
-// Receivers: rcv[c][r][it] = sum_k w_k u_c(g_k) (injector.cpp:118-140).
-__global__ void k_extract(const float *u, const int64_t *gidx, const float *w, int nrec, float *rcv, int nt, int it)
+// Receivers: rcv[s][c][r][it] = sum_k w_k u_c(g_k) (injector.cpp:118-140).
+__global__ void k_extract(const float *u, int64_t sst, int64_t nxyz, int ncomp, const int64_t *gidx, const float *w,
+                          int nrec, int nr, float *rcv, int nt, int it)
 {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= nrec) return;
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.y;
+    if (row >= nrec) return;
+    const int sh = row / nr, r = row - sh * nr;
+    const float *uc = u + sh * sst + c * nxyz;
     float acc = 0.f;
 #pragma unroll
-    for (int k = 0; k < 27; k++) acc += w[27 * r + k] * u[gidx[27 * r + k]];
-    rcv[(int64_t)r * nt + it] = acc;
+    for (int k = 0; k < 27; k++) acc += w[27 * row + k] * uc[gidx[27 * row + k] - (int64_t)sh * nxyz];
+    rcv[(((int64_t)sh * ncomp + c) * nr + r) * nt + it] = acc;
 }
 
 __global__ void k_acoustic_image(ImageArgs a)
 {
-    int ix, iy, iz;
-    if (!point_of(a.g, ix, iy, iz)) return;
+    int ix, iy, iz, s;
+    if (!point_of(a.g, (a.g.ny + BY - 1) / BY, ix, iy, iz, s)) return;
     acoustic_image_point(a, ix, iy, iz);
 }
 
 template <int PH>
 __global__ void k_elastic_image(ImageArgs a)
 {
-    int ix, iy, iz;
-    if (!point_of(a.g, ix, iy, iz)) return;
+    int ix, iy, iz, s;
+    if (!point_of(a.g, (a.g.ny + BY - 1) / BY, ix, iy, iz, s)) return;
     elastic_image_point<PH>(a, ix, iy, iz);
 }
 
@@ -190,6 +209,7 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     CK(cudaSetDevice(device));
     if (pb.nx < 12 || pb.ny < 12 || pb.nz < 12)
         throw FwiError(FWI_ERR_ARG, "each grid axis needs at least 12 points (two 6-row SBP closures)");
+    if (pb.nshots < 1) throw FwiError(FWI_ERR_ARG, "at least one shot");
     init_sbp_tables();
     CK(cudaMemcpyToSymbol(c_sbp, &g_sbp_host, sizeof(SbpTables)));
     cudaStream_t s;
@@ -197,8 +217,8 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     stream_ = s;
     const int64_t n = pb.nxyz();
     const int nc = pb.ncomp();
-    fields_.alloc(sizeof(float) * 3 * nc * n);
-    if (pb.nmodels != 2) aux_.alloc(sizeof(float) * (pb.nmodels == 6 ? 9 : 7) * n);
+    fields_.alloc(sizeof(float) * 3 * (size_t)pb.nshots * nc * n);
+    if (pb.nmodels != 2) aux_.alloc(sizeof(float) * (size_t)pb.nshots * (pb.nmodels == 6 ? 9 : 7) * n);
 }
 
 Engine::~Engine()
@@ -215,6 +235,12 @@ int64_t Engine::device_bytes() const
 {
     return model_.bytes + fields_.bytes + aux_.bytes + snaps_.bytes + grad_.bytes + sdiv_.bytes + taper_.bytes +
            src_dev_.bytes + rcv_dev_.bytes;
+}
+
+float *Engine::level(int l) const
+{
+    const int64_t lv = (int64_t)pb_.nshots * pb_.ncomp() * pb_.nxyz();
+    return fields_.as<float>() + ((rot_ + l) % 3) * lv;
 }
 
 void Engine::set_model(const float *conv)
@@ -298,40 +324,45 @@ StepArgs make_step_args(const Problem &pb, const float *m, const float *const sd
     }
     a.scale = scale;
     a.alpha_fs = (float)(0.2508560249 / pb.free_surface_stiffness);
+    a.nyb = yblocks(a.g);
+    a.sst = (int64_t)pb.ncomp() * n;
+    a.ast = (int64_t)(pb.nmodels == 6 ? 9 : 7) * n;
     return a;
 }
 }  // namespace
 
-void Engine::init_prev(const DevInj &inj, const float *src_dev, float *prev[3])
+void Engine::init_prev(const DevInj &inj, const float *src_dev, float *prev)
 {
     cudaStream_t s = (cudaStream_t)stream_;
     const int64_t n = pb_.nxyz();
     const int nc = pb_.ncomp();
+    const int64_t sst = (int64_t)nc * n;
     for (int c = 0; c < nc; c++) {
         if (inj.n[c] == 0) continue;
-        k_inject0<<<(inj.n[c] + 255) / 256, 256, 0, s>>>(prev[c], inj.gidx[c].as<int64_t>(), inj.trace[c].as<int>(),
-                                                          inj.w[c].as<float>(), inj.n[c], src_dev, pb_.nt);
+        k_inject0<<<(inj.n[c] + 255) / 256, 256, 0, s>>>(prev + c * n, sst, n, inj.gidx[c].as<int64_t>(),
+                                                          inj.trace[c].as<int>(), inj.w[c].as<float>(), inj.n[c],
+                                                          src_dev, pb_.nt);
         const float *coef = model_.as<float>() + (pb_.nmodels == 2 ? 0 : 2 * n);
-        k_scale0<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(prev[c], coef, n, pb_.dt, pb_.nmodels == 2);
+        k_scale0<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(prev + c * n, sst, coef, n, pb_.nshots, pb_.dt,
+                                                               pb_.nmodels == 2);
     }
     CK(cudaGetLastError());
 }
 
-void Engine::step(int it, float *prev[3], float *curr[3], float *next[3], bool taper_prev)
+void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
 {
-    (void)it;
     cudaStream_t s = (cudaStream_t)stream_;
     const Dims g{pb_.nx, pb_.ny, pb_.nz};
     const int64_t n = pb_.nxyz();
     StepArgs a = make_step_args(pb_, model_.as<float>(), sdiv_ptr_, taper_ptr_, scale_);
     const int nc = pb_.ncomp();
     for (int c = 0; c < nc; c++) {
-        a.curr[c] = curr[c];
-        a.prev[c] = prev[c];
-        a.next[c] = next[c];
+        a.curr[c] = curr + c * n;
+        a.prev[c] = prev + c * n;
+        a.next[c] = next + c * n;
     }
     a.taper_prev = taper_prev ? 1 : 0;
-    const dim3 blk(BZ, BX, BY), grd = grid_of(g);
+    const dim3 blk(BZ, BX, BY), grd = grid_of(g, pb_.nshots);
     if (pb_.nmodels == 2) {
         k_acoustic_step<<<grd, blk, 0, s>>>(a);
     } else {
@@ -341,8 +372,11 @@ void Engine::step(int it, float *prev[3], float *curr[3], float *next[3], bool t
         x.dx = pb_.dx;
         x.dy = pb_.dy;
         x.dz = pb_.dz;
+        x.nyb = a.nyb;
+        x.sst = a.sst;
+        x.ast = a.ast;
         for (int k = 0; k < pb_.nmodels; k++) x.m[k] = a.m[k];
-        for (int c = 0; c < 3; c++) x.curr[c] = curr[c];
+        for (int c = 0; c < 3; c++) x.curr[c] = curr + c * n;
         float *ab = aux_.as<float>();
         if (pb_.nmodels == 3) {
             // one shared divergence array in slots 0..2, then the six derivatives
@@ -363,12 +397,13 @@ void Engine::step(int it, float *prev[3], float *curr[3], float *next[3], bool t
     CK(cudaGetLastError());
 }
 
-void Engine::inject(const DevInj &inj, const float *src_dev, int it, float *next[3])
+void Engine::inject(const DevInj &inj, const float *src_dev, int it, float *next)
 {
     cudaStream_t s = (cudaStream_t)stream_;
     StepArgs a = make_step_args(pb_, model_.as<float>(), sdiv_ptr_, taper_ptr_, scale_);
     const int nc = pb_.ncomp();
-    for (int c = 0; c < nc; c++) a.next[c] = next[c];
+    const int64_t n = pb_.nxyz();
+    for (int c = 0; c < nc; c++) a.next[c] = next + c * n;
     for (int c = 0; c < nc; c++) {
         if (inj.n[c] == 0) continue;
         k_inject<<<(inj.n[c] + 127) / 128, 128, 0, s>>>(a, c, inj.gidx[c].as<int64_t>(), inj.trace[c].as<int>(),
@@ -377,35 +412,87 @@ void Engine::inject(const DevInj &inj, const float *src_dev, int it, float *next
     CK(cudaGetLastError());
 }
 
-void Engine::extract(const DevExt &ext, float *curr[3], float *rcv_dev, int nrcomp, int it)
+void Engine::extract(const DevExt &ext, const float *curr, float *rcv_dev, int it)
 {
+    if (ext.nrec == 0) return;
     cudaStream_t s = (cudaStream_t)stream_;
-    for (int c = 0; c < nrcomp; c++)
-        k_extract<<<(ext.nrec + 127) / 128, 128, 0, s>>>(curr[c], ext.gidx.as<int64_t>(), ext.w.as<float>(), ext.nrec,
-                                                          rcv_dev + (int64_t)c * ext.nrec * pb_.nt, pb_.nt, it);
+    const int nc = pb_.ncomp();
+    const int64_t n = pb_.nxyz();
+    const dim3 grd((ext.nrec + 127) / 128, nc);
+    k_extract<<<grd, 128, 0, s>>>(curr, (int64_t)nc * n, n, nc, ext.gidx.as<int64_t>(), ext.w.as<float>(), ext.nrec,
+                                  ext.nr, rcv_dev, pb_.nt, it);
     CK(cudaGetLastError());
 }
 
-void Engine::forward(const InjTable &inj, int ntrace, const float *src, const ExtTable &ext, int nrcomp, float *rcv,
-                     bool store)
+int Engine::launches_per_step() const
+{
+    int k = (pb_.nmodels == 2 ? 1 : 2);  // step (+ derivative pass)
+    if (ext_.nrec) k += 1;
+    for (int c = 0; c < 3; c++) k += inj_.n[c] ? 1 : 0;
+    return k;
+}
+
+void Engine::set_sources(const InjTable &inj, int ntrace, const float *src)
+{
+    CK(cudaSetDevice(device_));
+    upload_inj(inj, ntrace, inj_);
+    src_dev_.alloc(sizeof(float) * (size_t)ntrace * pb_.nt);
+    CK(cudaMemcpyAsync(src_dev_.p, src, src_dev_.bytes, cudaMemcpyHostToDevice, (cudaStream_t)stream_));
+}
+
+void Engine::set_receivers(const ExtTable &ext, int nr)
 {
     CK(cudaSetDevice(device_));
     cudaStream_t s = (cudaStream_t)stream_;
-    const int64_t n = pb_.nxyz();
-    const int nc = pb_.ncomp();
-    upload_inj(inj, ntrace, inj_);
-    src_dev_.alloc(sizeof(float) * ntrace * pb_.nt);
-    CK(cudaMemcpyAsync(src_dev_.p, src, src_dev_.bytes, cudaMemcpyHostToDevice, s));
     ext_.nrec = ext.nrec;
+    ext_.nr = nr;
     ext_.gidx.alloc(sizeof(int64_t) * ext.gidx.size());
     ext_.w.alloc(sizeof(float) * ext.w.size());
     if (ext.nrec) {
         CK(cudaMemcpyAsync(ext_.gidx.p, ext.gidx.data(), ext_.gidx.bytes, cudaMemcpyHostToDevice, s));
         CK(cudaMemcpyAsync(ext_.w.p, ext.w.data(), ext_.w.bytes, cudaMemcpyHostToDevice, s));
     }
-    rcv_dev_.alloc(sizeof(float) * (size_t)nrcomp * ext.nrec * pb_.nt);
+    rcv_dev_.alloc(sizeof(float) * (size_t)pb_.ncomp() * ext.nrec * pb_.nt);
     rcv_dev_.zero(s);
+}
 
+void Engine::reset()
+{
+    CK(cudaSetDevice(device_));
+    cudaStream_t s = (cudaStream_t)stream_;
+    rot_ = 0;
+    fields_.zero(s);
+    if (rcv_dev_.p) rcv_dev_.zero(s);
+    init_prev(inj_, src_dev_.as<float>(), level(0));
+}
+
+void Engine::run(int it0, int nsteps)
+{
+    for (int it = it0; it < it0 + nsteps && it < pb_.nt - 1; it++) {
+        extract(ext_, level(1), rcv_dev_.as<float>(), it);
+        step(level(0), level(1), level(2), it > 0);
+        inject(inj_, src_dev_.as<float>(), it, level(2));
+        rot_ = (rot_ + 1) % 3;
+    }
+}
+
+void Engine::extract_last() { extract(ext_, level(1), rcv_dev_.as<float>(), pb_.nt - 1); }
+
+void Engine::copy_traces(float *rcv)
+{
+    CK(cudaMemcpyAsync(rcv, rcv_dev_.p, rcv_dev_.bytes, cudaMemcpyDeviceToHost, (cudaStream_t)stream_));
+    sync();
+}
+
+void Engine::forward(const InjTable &inj, int ntrace, const float *src, const ExtTable &ext, float *rcv, bool store)
+{
+    CK(cudaSetDevice(device_));
+    cudaStream_t s = (cudaStream_t)stream_;
+    const int64_t n = pb_.nxyz();
+    const int nc = pb_.ncomp();
+    if (pb_.nshots != 1) throw FwiError(FWI_ERR_ARG, "the operator path runs one shot");
+    set_sources(inj, ntrace, src);
+    set_receivers(ext, ext.nrec);
     snaps_valid_ = false;
     const bool keep = store && pb_.sub > 0;
     if (keep) {
@@ -413,38 +500,23 @@ void Engine::forward(const InjTable &inj, int ntrace, const float *src, const Ex
         snaps_.alloc(sizeof(float) * (size_t)nsnap_ * nc * n);
         snaps_.zero(s);
     }
-
-    fields_.zero(s);
-    float *base = fields_.as<float>();
-    float *lv[3][3];
-    for (int l = 0; l < 3; l++)
-        for (int c = 0; c < 3; c++) lv[l][c] = base + ((int64_t)l * nc + (c < nc ? c : 0)) * n;
-    float **prev = lv[0], **curr = lv[1], **next = lv[2];
-    init_prev(inj_, src_dev_.as<float>(), prev);
-
-    auto snap = [&](int k, float **u) {
+    reset();
+    auto snap = [&](int k) {
         if (k > nsnap_ - 1) return;
-        CK(cudaMemcpyAsync(snaps_.as<float>() + (int64_t)k * nc * n, u[0], sizeof(float) * nc * n,
+        CK(cudaMemcpyAsync(snaps_.as<float>() + (int64_t)k * nc * n, level(1), sizeof(float) * nc * n,
                            cudaMemcpyDeviceToDevice, s));
     };
     for (int it = 0; it < pb_.nt - 1; it++) {
-        if (keep && it % pb_.sub == 0) snap(it / pb_.sub, curr);
-        extract(ext_, curr, rcv_dev_.as<float>(), nrcomp, it);
-        step(it, prev, curr, next, it > 0);
-        inject(inj_, src_dev_.as<float>(), it, next);
-        float **t = prev;
-        prev = curr;
-        curr = next;
-        next = t;
+        if (keep && it % pb_.sub == 0) snap(it / pb_.sub);
+        run(it, 1);
     }
-    if (keep && (pb_.nt - 1) % pb_.sub == 0) snap((pb_.nt - 1) / pb_.sub, curr);
-    extract(ext_, curr, rcv_dev_.as<float>(), nrcomp, pb_.nt - 1);
-    CK(cudaMemcpyAsync(rcv, rcv_dev_.p, rcv_dev_.bytes, cudaMemcpyDeviceToHost, s));
-    sync();
+    if (keep && (pb_.nt - 1) % pb_.sub == 0) snap((pb_.nt - 1) / pb_.sub);
+    extract_last();
+    copy_traces(rcv);
     snaps_valid_ = keep;
 }
 
-void Engine::image(int itl, float *curr[3], float *prevs[3])
+void Engine::image(int itl, const float *curr, const float *prevl)
 {
     cudaStream_t s = (cudaStream_t)stream_;
     const int64_t n = pb_.nxyz();
@@ -465,11 +537,12 @@ void Engine::image(int itl, float *curr[3], float *prevs[3])
         for (int c = 0; c < 3; c++) a.fwd[l][c] = snaps_.as<float>() + ((int64_t)kk * nc + (c < nc ? c : 0)) * n;
     }
     for (int c = 0; c < 3; c++) {
-        a.adj[c] = curr[c];
-        a.lag[c] = prevs[c];
+        const int cc = c < nc ? c : 0;
+        a.adj[c] = curr + cc * n;
+        a.lag[c] = prevl + cc * n;
         a.grad[c] = grad_.as<double>() + (int64_t)(c < (pb_.nmodels == 2 ? 2 : 3) ? c : 0) * n;
     }
-    const dim3 blk(BZ, BX, BY), grd = grid_of(a.g);
+    const dim3 blk(BZ, BX, BY), grd = grid_of(a.g, 1);
     if (pb_.nmodels == 2) k_acoustic_image<<<grd, blk, 0, s>>>(a);
     else if (pb_.nmodels == 3) k_elastic_image<ELASTIC><<<grd, blk, 0, s>>>(a);
     else k_elastic_image<VTI><<<grd, blk, 0, s>>>(a);
@@ -482,33 +555,24 @@ void Engine::adjoint(const InjTable &inj, int ntrace, const float *adj_src, floa
     if (!snaps_valid_) throw FwiError(FWI_ERR_STATE, "adjoint needs the snapshots of a preceding forward with sub > 0");
     cudaStream_t s = (cudaStream_t)stream_;
     const int64_t n = pb_.nxyz();
-    const int nc = pb_.ncomp();
     const int nm = std::min(3, pb_.nmodels);
     DevInj dinj;
     upload_inj(inj, ntrace, dinj);
-    DevBuf asrc(sizeof(float) * ntrace * pb_.nt);
+    DevBuf asrc(sizeof(float) * (size_t)ntrace * pb_.nt);
     CK(cudaMemcpyAsync(asrc.p, adj_src, asrc.bytes, cudaMemcpyHostToDevice, s));
     grad_.alloc(sizeof(double) * nm * n);
     grad_.zero(s);
-
+    rot_ = 0;
     fields_.zero(s);
-    float *base = fields_.as<float>();
-    float *lv[3][3];
-    for (int l = 0; l < 3; l++)
-        for (int c = 0; c < 3; c++) lv[l][c] = base + ((int64_t)l * nc + (c < nc ? c : 0)) * n;
-    float **prev = lv[0], **curr = lv[1], **next = lv[2];
-    init_prev(dinj, asrc.as<float>(), prev);
+    init_prev(dinj, asrc.as<float>(), level(0));
     const int sub = pb_.sub;
     for (int it = 0; it < pb_.nt - 1; it++) {
-        if ((pb_.nt - 1 - it) % sub == 0 && it != 0) image((pb_.nt - 1 - it) / sub, curr, prev);
-        step(it, prev, curr, next, it > 0);
-        inject(dinj, asrc.as<float>(), it, next);
-        float **t = prev;
-        prev = curr;
-        curr = next;
-        next = t;
+        if ((pb_.nt - 1 - it) % sub == 0 && it != 0) image((pb_.nt - 1 - it) / sub, level(1), level(0));
+        step(level(0), level(1), level(2), it > 0);
+        inject(dinj, asrc.as<float>(), it, level(2));
+        rot_ = (rot_ + 1) % 3;
     }
-    image(0, curr, prev);
+    image(0, level(1), level(0));
     DevBuf gf(sizeof(float) * nm * n);
     k_d2f<<<(unsigned)((nm * n + 255) / 256), 256, 0, s>>>(grad_.as<double>(), gf.as<float>(), nm * n);
     CK(cudaGetLastError());

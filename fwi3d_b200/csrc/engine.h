@@ -1,5 +1,7 @@
 // Device engine: owns the GPU state of one propagation problem (model, tables,
-// wavefields, snapshots) and runs the time loops on a CUDA stream.
+// wavefields of a batch of shots, snapshots) and runs the time loops on a
+// CUDA stream.  All shots of a batch share the model and step in lockstep;
+// one kernel launch advances every shot.
 #pragma once
 
 #include <cstdint>
@@ -45,19 +47,22 @@ struct Problem {
     int taper[6];
     float taper_strength;
     float free_surface_stiffness;
-    bool grad_fp64 = true;
+    int nshots = 1;
     int ncomp() const { return nmodels == 2 ? 1 : 3; }
     int64_t nxyz() const { return (int64_t)nx * ny * nz; }
 };
 
-// Injection / extraction tables on the device.
+// Injection table on the device: entry k adds w[k]*src[trace[k]][it] to field
+// component c at global point gidx[k] = shot*nxyz + point.
 struct DevInj {
     int n[3] = {0, 0, 0};
     DevBuf gidx[3], trace[3], w[3];
     int ntrace = 0;
 };
+// Extraction table: receiver row k (= shot*nr + r) reads 27 weighted points.
 struct DevExt {
-    int nrec = 0;
+    int nrec = 0;   // total rows over the batch
+    int nr = 0;     // receivers per shot
     DevBuf gidx, w;
 };
 
@@ -66,18 +71,28 @@ public:
     Engine(int device, const Problem &pb);
     ~Engine();
 
-    // Converted model [nmodels][nxyz] (host), boundary divisors and taper tables are built here.
+    const Problem &problem() const { return pb_; }
+    void *stream() const { return stream_; }
+
+    // Converted model [nmodels][nxyz] (host); boundary divisors and taper tables are built here.
     void set_model(const float *conv_model);
 
-    // Forward propagation of one shot.  src: [ntrace][nt] (host, propagation
-    // sampling); rcv out: [nrcomp][nrec][nt] (host).  When store is set and
-    // sub > 0 the snapshots for a later adjoint are kept on the device.
-    void forward(const InjTable &inj, int ntrace_src, const float *src, const ExtTable &ext, int nrcomp, float *rcv,
-                 bool store);
+    // --- batched modeling -------------------------------------------------
+    // Tables of all shots (gidx already offset by shot), sources [ntrace][nt]
+    // at the propagation sampling, receivers per shot.
+    void set_sources(const InjTable &inj, int ntrace, const float *src);
+    void set_receivers(const ExtTable &ext, int nr_per_shot);
+    void reset();                         // zero wavefields, apply the initial condition
+    void run(int it0, int nsteps);        // advance all shots by nsteps from time index it0 (async)
+    void extract_last();                  // receivers at it = nt-1 (after the last step)
+    void copy_traces(float *rcv);         // [nshots][nrcomp][nr][nt] raw traces (host)
+    int launches_per_step() const;
 
-    // Adjoint propagation + imaging; adj_src: [ntrace][nt]; grad out: [min(3,nm)][nxyz]
-    // (host, float, before H quadrature and chain rule).
-    void adjoint(const InjTable &inj, int ntrace_src, const float *adj_src, float *grad);
+    // --- single-shot operator path ------------------------------------------
+    // forward: full time loop; keeps snapshots when store && sub > 0
+    void forward(const InjTable &inj, int ntrace, const float *src, const ExtTable &ext, float *rcv, bool store);
+    // adjoint + imaging; grad out: [min(3,nm)][nxyz] float (before H quadrature and chain rule)
+    void adjoint(const InjTable &inj, int ntrace, const float *adj_src, float *grad);
 
     bool has_snapshots() const { return snaps_valid_; }
     int64_t device_bytes() const;
@@ -85,19 +100,21 @@ public:
 
 private:
     void upload_inj(const InjTable &t, int ntrace, DevInj &d);
-    void init_prev(const DevInj &inj, const float *src_dev, float *prev[3]);
-    void step(int it, float *prev[3], float *curr[3], float *next[3], bool taper_prev);
-    void inject(const DevInj &inj, const float *src_dev, int it, float *next[3]);
-    void extract(const DevExt &ext, float *curr[3], float *rcv_dev, int nrcomp, int it);
-    void image(int itl, float *curr[3], float *prevs[3]);
+    void init_prev(const DevInj &inj, const float *src_dev, float *prev);
+    void step(float *prev, float *curr, float *next, bool taper_prev);
+    void inject(const DevInj &inj, const float *src_dev, int it, float *next);
+    void extract(const DevExt &ext, const float *curr, float *rcv_dev, int it);
+    void image(int itl, const float *curr, const float *prevl);
+    float *level(int l) const;
 
     int device_;
     Problem pb_;
     void *stream_ = nullptr;
     DevBuf model_;                 // [nm][nxyz]
-    DevBuf fields_;                // 3 levels x ncomp x nxyz
-    DevBuf aux_;                   // elastic derivative scratch
-    DevBuf snaps_;                 // [nsnap][ncomp][nxyz]
+    DevBuf fields_;                // [3 levels][nshots][ncomp][nxyz]
+    int rot_ = 0;                  // rotation of the three time levels
+    DevBuf aux_;                   // elastic derivative scratch [nshots][naux][nxyz]
+    DevBuf snaps_;                 // [nsnap][ncomp][nxyz] (single shot)
     int nsnap_ = 0;
     bool snaps_valid_ = false;
     DevBuf grad_;                  // [3][nxyz] double

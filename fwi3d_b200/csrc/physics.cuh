@@ -47,7 +47,25 @@ struct StepArgs {
     int scale;                 // any face absorbing
     const float *tap[6];       // taper factors tz_lo[nz], tz_hi[nz], tx_lo[nx], tx_hi[nx], ty_lo[ny], ty_hi[ny]
     int taper_prev;
+    // batch layout: shot s of a field component c lives at curr[c] + s*sst
+    int nyb;                   // y blocks per shot in the launch grid
+    int64_t sst;               // wavefield shot stride (floats)
+    int64_t ast;               // derivative-scratch shot stride (floats)
 };
+
+// Pointers of shot s.
+FWI_HD StepArgs shot_args(const StepArgs &a, int s)
+{
+    StepArgs b = a;
+    for (int c = 0; c < 3; c++) {
+        if (b.curr[c]) b.curr[c] += s * a.sst;
+        if (b.prev[c]) b.prev[c] += s * a.sst;
+        if (b.next[c]) b.next[c] += s * a.sst;
+    }
+    for (int k = 0; k < 9; k++)
+        if (b.aux[k]) b.aux[k] += s * a.ast;
+    return b;
+}
 
 // ---------------------------------------------------------------------------
 // Taper and absorbing-boundary scaling
@@ -407,7 +425,19 @@ struct AuxArgs {
     const float *curr[3];
     float *aux[9];
     float *dlag[3];  // optional: u_x[0], u_y[1], u_z[2] (kept for imaging), may be null
+    int nyb;
+    int64_t sst, ast;
 };
+
+FWI_HD AuxArgs shot_args(const AuxArgs &a, int s)
+{
+    AuxArgs b = a;
+    for (int c = 0; c < 3; c++)
+        if (b.curr[c]) b.curr[c] += s * a.sst;
+    for (int k = 0; k < 9; k++)
+        if (b.aux[k]) b.aux[k] += s * a.ast;
+    return b;
+}
 
 template <int PH>
 FWI_HD void elastic_aux_point(const AuxArgs &a, int ix, int iy, int iz)

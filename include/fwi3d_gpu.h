@@ -71,8 +71,6 @@ typedef struct fwi_param {
     float deltamin, deltamax, epsilonmin, epsilonmax, gammamin, gammamax;
     int soft_clip;
     int verbose;
-    /* GPU-specific */
-    int grad_fp64;            /* accumulate imaging sums in FP64 (default 1) */
 } fwi_param;
 
 void fwi_param_default(fwi_param *p);
@@ -110,6 +108,27 @@ void fwi_op_destroy(fwi_op *op);
 int fwi_forward_batch(int device, const fwi_grid *grid, int nmodels, const fwi_param *par, const float *model,
                       const float *wavelet, int wavelet_ncomp, int nt_data, float dt_data, int nshots,
                       const float *sxyz, int nr, const float *rxyz, float *data);
+
+/* Batched modeling session: nshots shots sharing one device-resident model
+ * advance in lockstep, one kernel launch per operator per time step for the
+ * whole batch.  fwi_forward_batch is create + reset + run(all) + traces.
+ * Calls on one session must come from one host thread at a time. */
+typedef struct fwi_batch fwi_batch;
+
+int fwi_batch_create(fwi_batch **b, int device, const fwi_grid *grid, int nmodels, const fwi_param *par,
+                     const float *model, const float *wavelet, int wavelet_ncomp, int nt_data, float dt_data,
+                     int nshots, const float *sxyz, int nr, const float *rxyz);
+/* Zero the wavefields and apply the initial condition (time index 0). */
+int fwi_batch_reset(fwi_batch *b);
+/* Enqueue nsteps time steps on the session's stream (asynchronous). */
+int fwi_batch_run(fwi_batch *b, int nsteps);
+int fwi_batch_sync(fwi_batch *b);
+/* The cudaStream_t the session launches on (for event timing). */
+int fwi_batch_stream(fwi_batch *b, void **stream);
+/* Data [nshots][nrcomp][nr][nt_data] after the full time axis was run. */
+int fwi_batch_traces(fwi_batch *b, float *data);
+int fwi_batch_get_info(const fwi_batch *b, fwi_op_info *info, int *launches_per_step);
+void fwi_batch_destroy(fwi_batch *b);
 
 /* Message of the last failing call on this thread. */
 const char *fwi_last_error(void);

@@ -101,3 +101,14 @@ def test_config1_full_size(oracle_fp32):
     e32, e64 = rel(d, ref32), rel(d, ref64)
     print(f"config1: vs fp32 {e32:.3e}  vs fp64 {e64:.3e}  fp32-vs-fp64 {rel(ref32, ref64):.3e}")
     assert e32 < TRACE_TOL
+
+
+def test_batch_matches_single_shot_operator():
+    """Shots batched in one launch give the traces of separate operators."""
+    sv = synth.elastic_layered(n=28, nsteps=120, taper=6, rec_stride=4, nshots=3)
+    for s in range(3):
+        sv.par.sxyz[s] = [(0.3 + 0.2 * s) * 28 * sv.dx, (0.5 - 0.1 * s) * 28 * sv.dx, 0.2 * 28 * sv.dx]
+    batch = ops.forward_batch(sv)
+    for s in range(3):
+        single = ops.from_survey(sv, s).forward(False, sv.model)
+        assert rel(batch[s], single) < 1e-6
