@@ -11,10 +11,12 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "engine.h"
 #include "imaging.cuh"
+#include "fused.cuh"
 #include "physics.cuh"
 
 namespace fwi {
@@ -67,25 +69,31 @@ namespace {
 
 constexpr int BZ = 32, BX = 4, BY = 2;
 
-__device__ __forceinline__ bool point_of(const Dims &g, int nyb, int &ix, int &iy, int &iz, int &s)
+// Launch grid z covers (y blocks of planes [y0, y1)) x shots.
+__device__ __forceinline__ bool point_of(const Dims &g, int nyb, int y0, int y1, int &ix, int &iy, int &iz, int &s)
 {
     iz = blockIdx.x * BZ + threadIdx.x;
     ix = blockIdx.y * BX + threadIdx.y;
     s = blockIdx.z / nyb;
-    iy = (blockIdx.z % nyb) * BY + threadIdx.z;
-    return iz < g.nz && ix < g.nx && iy < g.ny;
+    iy = y0 + (blockIdx.z % nyb) * BY + threadIdx.z;
+    return iz < g.nz && ix < g.nx && iy < y1;
+}
+__device__ __forceinline__ bool point_of(const Dims &g, int nyb, int &ix, int &iy, int &iz, int &s)
+{
+    return point_of(g, nyb, 0, g.ny, ix, iy, iz, s);
 }
 
-int yblocks(const Dims &g) { return (g.ny + BY - 1) / BY; }
-dim3 grid_of(const Dims &g, int nshots)
+int yblocks(int ny) { return (ny + BY - 1) / BY; }
+int yblocks(const Dims &g) { return yblocks(g.ny); }
+dim3 grid_of(const Dims &g, int nshots, int ny_launch = -1)
 {
-    return dim3((g.nz + BZ - 1) / BZ, (g.nx + BX - 1) / BX, yblocks(g) * nshots);
+    return dim3((g.nz + BZ - 1) / BZ, (g.nx + BX - 1) / BX, yblocks(ny_launch < 0 ? g.ny : ny_launch) * nshots);
 }
 
 __global__ void k_acoustic_step(StepArgs a)
 {
     int ix, iy, iz, s;
-    if (!point_of(a.g, a.nyb, ix, iy, iz, s)) return;
+    if (!point_of(a.g, a.nyb, a.y0, a.y1, ix, iy, iz, s)) return;
     const StepArgs b = shot_args(a, s);
     b.next[0][b.g.idx(ix, iy, iz)] = acoustic_point(b, ix, iy, iz);
 }
@@ -94,7 +102,7 @@ template <int PH>
 __global__ void k_elastic_aux(AuxArgs a)
 {
     int ix, iy, iz, s;
-    if (!point_of(a.g, a.nyb, ix, iy, iz, s)) return;
+    if (!point_of(a.g, a.nyb, a.y0, a.y1, ix, iy, iz, s)) return;
     elastic_aux_point<PH>(shot_args(a, s), ix, iy, iz);
 }
 
@@ -102,7 +110,7 @@ template <int PH>
 __global__ void k_elastic_step(StepArgs a)
 {
     int ix, iy, iz, s;
-    if (!point_of(a.g, a.nyb, ix, iy, iz, s)) return;
+    if (!point_of(a.g, a.nyb, a.y0, a.y1, ix, iy, iz, s)) return;
     const StepArgs b = shot_args(a, s);
     const int64_t i = b.g.idx(ix, iy, iz);
     const float v0 = elastic_point<PH>(b, 0, ix, iy, iz);
@@ -111,6 +119,42 @@ __global__ void k_elastic_step(StepArgs a)
     b.next[0][i] = v0;
     b.next[1][i] = v1;
     b.next[2][i] = v2;
+}
+
+// Fused elastic step over planes [ylo, yhi) (see fused.cuh).  grid: (z tiles,
+// x tiles, y chunks x shots), block (TZ, TX).
+template <int PH>
+__global__ void __launch_bounds__(fz::NT, 2) k_elastic_fused(const __grid_constant__ StepArgs a, int nchunks)
+{
+    extern __shared__ __align__(16) unsigned char fz_smem[];
+    FusedCtx c;
+    c.a = &a;
+    c.sm = reinterpret_cast<FusedSmem *>(fz_smem);
+    const int tid = threadIdx.x + fz::TZ * threadIdx.y;
+    c.shot = blockIdx.z / nchunks;
+    const int ch = blockIdx.z - c.shot * nchunks;
+    c.so = c.shot * a.sst;
+    tile_range(blockIdx.x, a.g.nz, fz::TZ, c.z0, c.zend);
+    tile_range(blockIdx.y, a.g.nx, fz::TX, c.x0, c.xend);
+    const int len = a.y1 - a.y0;
+    const int ya = a.y0 + (int)((int64_t)len * ch / nchunks);
+    const int yb = a.y0 + (int)((int64_t)len * (ch + 1) / nchunks);
+    if (ya >= yb) return;
+    FusedThread th;
+#pragma unroll
+    for (int k = 0; k < 5; k++) th.qmu[k] = th.qeps[k] = th.q66[k] = th.qT[k] = th.qX1[k] = th.qZ1[k] = 0.f;
+    fz_prologue<PH>(c, tid, ya);
+    __syncthreads();
+    for (int y = ya - 4; y < yb; y++) {
+        fz_load_u(c, tid, y + 4);
+        if (y >= ya) fz_load_mat<PH>(c, tid, y);
+        __syncthreads();
+        fz_column<PH>(c, th, tid, y + 2);
+        if (y >= ya) fz_derived<PH>(c, tid, y);
+        __syncthreads();
+        if (y >= ya) fz_output<PH>(c, th, tid, y);
+        __syncthreads();
+    }
 }
 
 // Post-injection: next += taper(scale(dt^2 (w s)/rho)) (elastic) or dt^2 (w s) K
@@ -219,6 +263,15 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     const int nc = pb.ncomp();
     fields_.alloc(sizeof(float) * 3 * (size_t)pb.nshots * nc * n);
     if (pb.nmodels != 2) aux_.alloc(sizeof(float) * (size_t)pb.nshots * (pb.nmodels == 6 ? 9 : 7) * n);
+    const char *env = std::getenv("FWI_FUSED");
+    fused_ = pb.nmodels != 2 && !(env && env[0] == '0') && pb.nx >= fz::TX && pb.nz >= fz::TZ &&
+             pb.ny > 2 * fz::YPAD;
+    if (fused_) {
+        CK(cudaFuncSetAttribute(k_elastic_fused<ELASTIC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(FusedSmem)));
+        CK(cudaFuncSetAttribute(k_elastic_fused<VTI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(FusedSmem)));
+    }
 }
 
 Engine::~Engine()
@@ -325,6 +378,8 @@ StepArgs make_step_args(const Problem &pb, const float *m, const float *const sd
     a.scale = scale;
     a.alpha_fs = (float)(0.2508560249 / pb.free_surface_stiffness);
     a.nyb = yblocks(a.g);
+    a.y0 = 0;
+    a.y1 = pb.ny;
     a.sst = (int64_t)pb.ncomp() * n;
     a.ast = (int64_t)(pb.nmodels == 6 ? 9 : 7) * n;
     return a;
@@ -362,37 +417,79 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         a.next[c] = next + c * n;
     }
     a.taper_prev = taper_prev ? 1 : 0;
-    const dim3 blk(BZ, BX, BY), grd = grid_of(g, pb_.nshots);
+    const dim3 blk(BZ, BX, BY);
+    // per-point launch over planes [y0, y1)
+    auto range = [&](StepArgs &st, int y0, int y1) {
+        st.y0 = y0;
+        st.y1 = y1;
+        st.nyb = yblocks(y1 - y0);
+        return grid_of(g, pb_.nshots, y1 - y0);
+    };
     if (pb_.nmodels == 2) {
-        k_acoustic_step<<<grd, blk, 0, s>>>(a);
+        k_acoustic_step<<<range(a, 0, pb_.ny), blk, 0, s>>>(a);
+        CK(cudaGetLastError());
+        return;
+    }
+    AuxArgs x;
+    std::memset(&x, 0, sizeof(x));
+    x.g = g;
+    x.dx = pb_.dx;
+    x.dy = pb_.dy;
+    x.dz = pb_.dz;
+    x.sst = a.sst;
+    x.ast = a.ast;
+    for (int k = 0; k < pb_.nmodels; k++) x.m[k] = a.m[k];
+    for (int c = 0; c < 3; c++) x.curr[c] = curr + c * n;
+    float *ab = aux_.as<float>();
+    if (pb_.nmodels == 3) {
+        // one shared divergence array in slots 0..2, then the six derivatives
+        x.aux[AUX_T0] = x.aux[AUX_T1] = x.aux[AUX_T2] = ab;
+        for (int k = 3; k < 9; k++) x.aux[k] = ab + (k - 2) * n;
     } else {
-        AuxArgs x;
-        std::memset(&x, 0, sizeof(x));
-        x.g = g;
-        x.dx = pb_.dx;
-        x.dy = pb_.dy;
-        x.dz = pb_.dz;
-        x.nyb = a.nyb;
-        x.sst = a.sst;
-        x.ast = a.ast;
-        for (int k = 0; k < pb_.nmodels; k++) x.m[k] = a.m[k];
-        for (int c = 0; c < 3; c++) x.curr[c] = curr + c * n;
-        float *ab = aux_.as<float>();
-        if (pb_.nmodels == 3) {
-            // one shared divergence array in slots 0..2, then the six derivatives
-            x.aux[AUX_T0] = x.aux[AUX_T1] = x.aux[AUX_T2] = ab;
-            for (int k = 3; k < 9; k++) x.aux[k] = ab + (k - 2) * n;
+        for (int k = 0; k < 9; k++) x.aux[k] = ab + k * n;
+    }
+    for (int k = 0; k < 9; k++) a.aux[k] = x.aux[k];
+    auto aux_range = [&](int y0, int y1) {
+        x.y0 = y0;
+        x.y1 = y1;
+        x.nyb = yblocks(y1 - y0);
+        const dim3 grd = grid_of(g, pb_.nshots, y1 - y0);
+        if (pb_.nmodels == 3) k_elastic_aux<ELASTIC><<<grd, blk, 0, s>>>(x);
+        else k_elastic_aux<VTI><<<grd, blk, 0, s>>>(x);
+    };
+    auto step_range = [&](int y0, int y1) {
+        const dim3 grd = range(a, y0, y1);
+        if (pb_.nmodels == 3) k_elastic_step<ELASTIC><<<grd, blk, 0, s>>>(a);
+        else k_elastic_step<VTI><<<grd, blk, 0, s>>>(a);
+    };
+    const int P = fz::YPAD;
+    if (!fused_) {
+        aux_range(0, pb_.ny);
+        step_range(0, pb_.ny);
+    } else {
+        // planes near the y walls: per-point kernels (derivative scratch two planes deeper)
+        if (pb_.ny < 2 * (P + 2)) {
+            aux_range(0, pb_.ny);
         } else {
-            for (int k = 0; k < 9; k++) x.aux[k] = ab + k * n;
+            aux_range(0, P + 2);
+            aux_range(pb_.ny - P - 2, pb_.ny);
         }
-        for (int k = 0; k < 9; k++) a.aux[k] = x.aux[k];
-        if (pb_.nmodels == 3) {
-            k_elastic_aux<ELASTIC><<<grd, blk, 0, s>>>(x);
-            k_elastic_step<ELASTIC><<<grd, blk, 0, s>>>(a);
-        } else {
-            k_elastic_aux<VTI><<<grd, blk, 0, s>>>(x);
-            k_elastic_step<VTI><<<grd, blk, 0, s>>>(a);
-        }
+        step_range(0, P);
+        step_range(pb_.ny - P, pb_.ny);
+        // interior planes: fused kernel
+        StepArgs f = a;
+        f.y0 = P;
+        f.y1 = pb_.ny - P;
+        for (int k = 0; k < 9; k++) f.aux[k] = nullptr;
+        const int kz = (pb_.nz + fz::TZ - 1) / fz::TZ, kx = (pb_.nx + fz::TX - 1) / fz::TX;
+        const int tiles = kz * kx * pb_.nshots;
+        int nch = (600 + tiles - 1) / tiles;
+        nch = std::max(1, std::min(nch, (f.y1 - f.y0) / 16));
+        const dim3 grd(kz, kx, nch * pb_.nshots), fblk(fz::TZ, fz::TX);
+        if (pb_.nmodels == 3)
+            k_elastic_fused<ELASTIC><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch);
+        else
+            k_elastic_fused<VTI><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch);
     }
     CK(cudaGetLastError());
 }
@@ -426,7 +523,7 @@ void Engine::extract(const DevExt &ext, const float *curr, float *rcv_dev, int i
 
 int Engine::launches_per_step() const
 {
-    int k = (pb_.nmodels == 2 ? 1 : 2);  // step (+ derivative pass)
+    int k = (pb_.nmodels == 2 ? 1 : (fused_ ? (pb_.ny < 2 * (fz::YPAD + 2) ? 4 : 5) : 2));
     if (ext_.nrec) k += 1;
     for (int c = 0; c < 3; c++) k += inj_.n[c] ? 1 : 0;
     return k;

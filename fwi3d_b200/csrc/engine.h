@@ -123,6 +123,7 @@ private:
     DevBuf taper_;                 // packed taper tables
     const float *taper_ptr_[6] = {};
     int scale_ = 0;
+    bool fused_ = false;           // fused elastic kernel for the interior planes
     DevBuf src_dev_, rcv_dev_;
     DevInj inj_;
     DevExt ext_;

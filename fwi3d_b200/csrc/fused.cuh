@@ -1,0 +1,423 @@
+// Fused elastic time step (isotropic and VTI): one kernel computes, for every
+// output point, all operator terms of the reference's step (we_op.cpp:646-836,
+// 1297-1497) -- D2var x9, D1 of the stress combination, the six mixed mult_D
+// terms -- plus SAT, leapfrog update, absorbing scaling and taper, reading each
+// wavefield and model array from HBM once.
+//
+// Blocking: a CTA owns a TZ x TX tile of (z, x) columns (z = lanes, x = warps)
+// and marches along y.  Shared memory holds a ring of the last 7 planes of the
+// three displacement components over the tile plus a 4-point halo, and, for the
+// output plane, the first-derivative combinations whose x/z derivatives are
+// taken (tile plus 2-point halo).  Quantities differentiated along y are kept
+// per thread in 5-deep register queues.  The x/z tiling (tile_range) gives the
+// rows of the SBP boundary closures to the first and last tiles, whose windows
+// hold every sample those rows read; first derivatives at closure rows of the
+// halo are taken from global memory.  Planes within 8 of the y walls are left
+// to the per-point kernels (the launch covers y in [8, ny-8)).
+//
+// Every helper is a host/device function of (context, thread index) so a CPU
+// harness can run the same phases thread by thread.
+#pragma once
+
+#include "physics.cuh"
+
+namespace fwi {
+
+namespace fz {
+constexpr int TZ = 32, TX = 16, NT = TZ * TX;
+constexpr int HW = 4;                          // halo of the displacement ring
+constexpr int ZW = TZ + 2 * HW, XW = TX + 2 * HW;
+constexpr int HD = 2;                          // halo of the derived planes
+constexpr int ZH = TZ + 2 * HD, XH = TX + 2 * HD;
+constexpr int NRING = 7;
+constexpr int YPAD = 8;                        // y planes per side left to the per-point kernels
+}  // namespace fz
+
+// Derived-plane slots.
+enum { DV_T0 = 0, DV_T2 = 1, DV_Y0 = 2, DV_Z0 = 3, DV_X2 = 4, DV_Y2 = 5, NDV = 6 };
+// Material planes over the derived region: mu, lambda, (VTI) c13, eps, c66.
+enum { MP_MU = 0, MP_LAM = 1, MP_C13 = 2, MP_EPS = 3, MP_C66 = 4, NMP = 5 };
+
+struct FusedSmem {
+    float u[fz::NRING][3][fz::XW][fz::ZW];
+    float dv[NDV][fz::XH][fz::ZH];
+    float mp[NMP][fz::XH][fz::ZH];
+};
+
+// Per-thread state carried along the march (registers on the GPU).
+struct FusedThread {
+    float qmu[5];   // mu at y-2..y+2 (own column)
+    float qeps[5];  // eps (VTI)
+    float q66[5];   // c66 (VTI)
+    float qT[5];    // stress combination differentiated along y (T iso, T1 VTI)
+    float qX1[5];   // P * Dx u1
+    float qZ1[5];   // mu * Dz u1
+};
+
+struct FusedCtx {
+    const StepArgs *a; // launch arguments (pointers of shot 0)
+    int shot;
+    int64_t so;        // wavefield offset of this shot (shot * sst)
+    int x0, z0;        // tile (window) origin
+    int xend, zend;    // end of this tile's output rows
+    FusedSmem *sm;
+};
+
+// Smem line accessors (global index -> smem slot).
+struct SZ {  // along z at fixed (slot, comp, xw)
+    const float *p;  // &u[slot][c][xw][0]
+    int off;         // global z of smem position 0
+    FWI_HD float operator()(int k) const { return p[k - off]; }
+};
+struct SX {  // along x at fixed zw
+    const float *p;  // &arr[0][zw]
+    int off;         // global x of smem position 0
+    int stride;
+    FWI_HD float operator()(int k) const { return p[(k - off) * stride]; }
+};
+
+FWI_HD int ring(int q) { return ((q % fz::NRING) + fz::NRING) % fz::NRING; }
+
+// ---------------------------------------------------------------------------
+// Phase A: load displacement plane q (tile + 4 halo) into its ring slot.
+// ---------------------------------------------------------------------------
+FWI_HD void fz_load_u(FusedCtx &c, int tid, int q)
+{
+    const Dims &g = c.a->g;
+    const int slot = ring(q);
+    for (int p = tid; p < fz::XW * fz::ZW; p += fz::NT) {
+        const int xw = p / fz::ZW, zw = p - xw * fz::ZW;
+        const int ix = c.x0 - fz::HW + xw, iz = c.z0 - fz::HW + zw;
+        const bool in = ix >= 0 && ix < g.nx && iz >= 0 && iz < g.nz;
+        const int64_t i = in ? g.idx(ix, q, iz) : 0;
+        for (int k = 0; k < 3; k++) c.sm->u[slot][k][xw][zw] = in ? c.a->curr[k][c.so + i] : 0.f;
+    }
+}
+
+// Material planes at y over the derived region.
+template <int PH>
+FWI_HD void fz_load_mat(FusedCtx &c, int tid, int y)
+{
+    const Dims &g = c.a->g;
+    for (int p = tid; p < fz::XH * fz::ZH; p += fz::NT) {
+        const int xh = p / fz::ZH, zh = p - xh * fz::ZH;
+        const int ix = c.x0 - fz::HD + xh, iz = c.z0 - fz::HD + zh;
+        const bool in = ix >= 0 && ix < g.nx && iz >= 0 && iz < g.nz;
+        const int64_t i = in ? g.idx(ix, y, iz) : 0;
+        c.sm->mp[MP_MU][xh][zh] = in ? c.a->m[1][i] : 0.f;
+        c.sm->mp[MP_LAM][xh][zh] = in ? c.a->m[0][i] : 0.f;
+        if (PH == VTI) {
+            c.sm->mp[MP_C13][xh][zh] = in ? c.a->m[3][i] : 0.f;
+            c.sm->mp[MP_EPS][xh][zh] = in ? c.a->m[4][i] : 0.f;
+            c.sm->mp[MP_C66][xh][zh] = in ? c.a->m[5][i] : 0.f;
+        }
+    }
+}
+
+// D1 row (unscaled) at global index i of a line; interior rows from smem,
+// closure rows from global memory.
+template <class S>
+FWI_HD float d1_sg(const S &s, const Line &gl, int i, int n)
+{
+    if (i < 4 || i >= n - 4) return d1_row(gl, i, n);
+    const SbpTables &t = sbp();
+    return t.d1c0 * (s(i + 1) - s(i - 1)) + t.d1c1 * (s(i + 2) - s(i - 2));
+}
+
+// First derivatives of displacement component k at (ix, q, iz) along x, y, z
+// from the ring (with the 1/h).  ixw/izw: smem coordinates in the ring window.
+FWI_HD float fz_dx(const FusedCtx &c, int k, int q, int ix, int iz, int izw)
+{
+    const Dims &g = c.a->g;
+    const SX s{&c.sm->u[ring(q)][k][0][izw], c.x0 - fz::HW, fz::ZW};
+    return d1_sg(s, g.lx(c.a->curr[k] + c.so, q, iz), ix, g.nx) / c.a->dx;
+}
+FWI_HD float fz_dz(const FusedCtx &c, int k, int q, int ix, int ixw, int iz)
+{
+    const Dims &g = c.a->g;
+    const SZ s{&c.sm->u[ring(q)][k][ixw][0], c.z0 - fz::HW};
+    return d1_sg(s, g.lz(c.a->curr[k] + c.so, ix, q), iz, g.nz) / c.a->dz;
+}
+// Dy at plane q: interior rows only (the fused launch keeps q in [6, ny-6)).
+FWI_HD float fz_dy(const FusedCtx &c, int k, int q, int ixw, int izw)
+{
+    const SbpTables &t = sbp();
+    const float um2 = c.sm->u[ring(q - 2)][k][ixw][izw], um1 = c.sm->u[ring(q - 1)][k][ixw][izw];
+    const float up1 = c.sm->u[ring(q + 1)][k][ixw][izw], up2 = c.sm->u[ring(q + 2)][k][ixw][izw];
+    return (t.d1c0 * (up1 - um1) + t.d1c1 * (up2 - um2)) / c.a->dy;
+}
+
+// ---------------------------------------------------------------------------
+// Phase B1: derived quantities of plane y over the derived region.
+// ---------------------------------------------------------------------------
+template <int PH>
+FWI_HD void fz_derived(FusedCtx &c, int tid, int y)
+{
+    const Dims &g = c.a->g;
+    for (int p = tid; p < fz::XH * fz::ZH; p += fz::NT) {
+        const int xh = p / fz::ZH, zh = p - xh * fz::ZH;
+        const int ix = c.x0 - fz::HD + xh, iz = c.z0 - fz::HD + zh;
+        float *dv0 = &c.sm->dv[0][xh][zh];
+        const int stride = fz::XH * fz::ZH;
+        if (ix < 0 || ix >= g.nx || iz < 0 || iz >= g.nz) {
+            for (int k = 0; k < NDV; k++) dv0[k * stride] = 0.f;
+            continue;
+        }
+        const int ixw = xh + (fz::HW - fz::HD), izw = zh + (fz::HW - fz::HD);
+        const float ux0 = fz_dx(c, 0, y, ix, iz, izw);
+        const float uy1 = fz_dy(c, 1, y, ixw, izw);
+        const float uz2 = fz_dz(c, 2, y, ix, ixw, iz);
+        const float mu = c.sm->mp[MP_MU][xh][zh], lam = c.sm->mp[MP_LAM][xh][zh];
+        const float uy0 = fz_dy(c, 0, y, ixw, izw);
+        const float uz0 = fz_dz(c, 0, y, ix, ixw, iz);
+        const float ux2 = fz_dx(c, 2, y, ix, iz, izw);
+        const float uy2 = fz_dy(c, 2, y, ixw, izw);
+        if (PH == ELASTIC) {
+            const float T = lam * (ux0 + uy1 + uz2);
+            dv0[DV_T0 * stride] = T;
+            dv0[DV_T2 * stride] = T;
+            dv0[DV_Y0 * stride] = uy0;  // multiplied by the coefficient at the tap (mult_D)
+        } else {
+            const float c13 = c.sm->mp[MP_C13][xh][zh], eps = c.sm->mp[MP_EPS][xh][zh];
+            const float c66 = c.sm->mp[MP_C66][xh][zh];
+            const float c11c = (1.f + 2.f * eps) * lam;
+            const float c12 = (1.f + 2.f * eps) * (lam + 2.f * mu) - 2.f * c66;
+            dv0[DV_T0 * stride] = c11c * ux0 + c12 * uy1 + c13 * uz2;
+            dv0[DV_T2 * stride] = c13 * (ux0 + uy1) + lam * uz2;
+            dv0[DV_Y0 * stride] = uy0;
+        }
+        dv0[DV_Z0 * stride] = uz0;
+        dv0[DV_X2 * stride] = ux2;
+        dv0[DV_Y2 * stride] = uy2;
+    }
+}
+
+// Phase B2: own-column quantities of plane q = y+2 pushed into the y queues.
+template <int PH>
+FWI_HD void fz_column(FusedCtx &c, FusedThread &th, int tid, int q)
+{
+    const Dims &g = c.a->g;
+    const int lz = tid % fz::TZ, lx = tid / fz::TZ;
+    const int ix = c.x0 + lx, iz = c.z0 + lz;
+    for (int k = 0; k < 4; k++) {
+        th.qmu[k] = th.qmu[k + 1];
+        th.qeps[k] = th.qeps[k + 1];
+        th.q66[k] = th.q66[k + 1];
+        th.qT[k] = th.qT[k + 1];
+        th.qX1[k] = th.qX1[k + 1];
+        th.qZ1[k] = th.qZ1[k + 1];
+    }
+    if (ix >= g.nx || iz >= g.nz) {
+        th.qmu[4] = th.qeps[4] = th.q66[4] = th.qT[4] = th.qX1[4] = th.qZ1[4] = 0.f;
+        return;
+    }
+    const int ixw = lx + fz::HW, izw = lz + fz::HW;
+    const int64_t i = g.idx(ix, q, iz);
+    const float mu = c.a->m[1][i], lam = c.a->m[0][i];
+    th.qmu[4] = mu;
+    const float ux0 = fz_dx(c, 0, q, ix, iz, izw);
+    const float uy1 = fz_dy(c, 1, q, ixw, izw);
+    const float uz2 = fz_dz(c, 2, q, ix, ixw, iz);
+    const float ux1 = fz_dx(c, 1, q, ix, iz, izw);
+    const float uz1 = fz_dz(c, 1, q, ix, ixw, iz);
+    if (PH == ELASTIC) {
+        th.qT[4] = lam * (ux0 + uy1 + uz2);
+        th.qX1[4] = ux1;
+    } else {
+        const float c13 = c.a->m[3][i], eps = c.a->m[4][i], c66 = c.a->m[5][i];
+        th.qeps[4] = eps;
+        th.q66[4] = c66;
+        const float c11c = (1.f + 2.f * eps) * lam;
+        const float c12 = (1.f + 2.f * eps) * (lam + 2.f * mu) - 2.f * c66;
+        th.qT[4] = c11c * uy1 + c12 * ux0 + c13 * uz2;
+        th.qX1[4] = ux1;
+    }
+    th.qZ1[4] = uz1;
+}
+
+// ---------------------------------------------------------------------------
+// Phase C: output point (own column) of plane y.
+// ---------------------------------------------------------------------------
+// Interior D2var weights for the five taps (the reference's grouping).
+struct W5 {
+    float w0, wm1, wp1, wm2, wp2;
+};
+FWI_HD W5 d2w(float fm2, float fm1, float f0, float fp1, float fp2)
+{
+    const float *cc = sbp().d2in;
+    W5 w;
+    w.w0 = cc[0] * f0 + cc[1] * (fm1 + fp1) + cc[2] * (fm2 + fp2);
+    w.wm1 = cc[3] * fm2 + cc[4] * fm1 + cc[5] * f0 + cc[6] * fp1;
+    w.wp1 = cc[3] * fp2 + cc[4] * fp1 + cc[5] * f0 + cc[6] * fm1;
+    w.wm2 = cc[7] * fm2 + cc[8] * fm1 + cc[9] * f0;
+    w.wp2 = cc[7] * fp2 + cc[8] * fp1 + cc[9] * f0;
+    return w;
+}
+FWI_HD float d2apply(const W5 &w, float ad2, float um2, float um1, float u0, float up1, float up2)
+{
+    return ad2 * (w.w0 * u0 + w.wm1 * um1 + w.wp1 * up1 + w.wm2 * um2 + w.wp2 * up2);
+}
+// Interior D1 (unscaled) from five taps.
+FWI_HD float d1i(float am2, float am1, float ap1, float ap2)
+{
+    const SbpTables &t = sbp();
+    return t.d1c0 * (ap1 - am1) + t.d1c1 * (ap2 - am2);
+}
+// Interior mult_D (unscaled): D1 of a*m with per-tap products.
+FWI_HD float d1m(float am2, float mm2, float am1, float mm1, float ap1, float mp1, float ap2, float mp2)
+{
+    const SbpTables &t = sbp();
+    return t.d1c0 * (ap1 * mp1 - am1 * mm1) + t.d1c1 * (ap2 * mp2 - am2 * mm2);
+}
+
+// Smem accessors of the output phase.
+FWI_HD SX ux_line(const FusedCtx &c, int slot, int k, int izw) { return SX{&c.sm->u[slot][k][0][izw], c.x0 - fz::HW, fz::ZW}; }
+FWI_HD SZ uz_line(const FusedCtx &c, int slot, int k, int ixw) { return SZ{&c.sm->u[slot][k][ixw][0], c.z0 - fz::HW}; }
+FWI_HD SX mx_line(const FusedCtx &c, int m, int zh) { return SX{&c.sm->mp[m][0][zh], c.x0 - fz::HD, fz::ZH}; }
+FWI_HD SZ mz_line(const FusedCtx &c, int m, int xh) { return SZ{&c.sm->mp[m][xh][0], c.z0 - fz::HD}; }
+FWI_HD SX dx_line(const FusedCtx &c, int d, int zh) { return SX{&c.sm->dv[d][0][zh], c.x0 - fz::HD, fz::ZH}; }
+FWI_HD SZ dz_line(const FusedCtx &c, int d, int xh) { return SZ{&c.sm->dv[d][xh][0], c.z0 - fz::HD}; }
+template <class E, class M>
+struct C11bS {
+    E eps;
+    M mu;
+    FWI_HD float operator()(int k) const { return 2.f * (1.f + 2.f * eps(k)) * mu(k); }
+};
+
+template <int PH>
+FWI_HD void fz_output(FusedCtx &c, const FusedThread &th, int tid, int y)
+{
+    const StepArgs &a = *c.a;
+    const Dims &g = a.g;
+    const int lz = tid % fz::TZ, lx = tid / fz::TZ;
+    const int ix = c.x0 + lx, iz = c.z0 + lz;
+    if (ix >= c.xend || iz >= c.zend) return;
+    const int64_t i = g.idx(ix, y, iz);
+    const bool xin = ix >= 6 && ix < g.nx - 6;
+    const bool zin = iz >= 6 && iz < g.nz - 6;
+    const int ixw = lx + fz::HW, izw = lz + fz::HW;
+    const int xh = lx + fz::HD, zh = lz + fz::HD;
+    const FusedSmem &s = *c.sm;
+    const int r0 = ring(y), rm1 = ring(y - 1), rm2 = ring(y - 2), rp1 = ring(y + 1), rp2 = ring(y + 2);
+    const float idx2 = 1.0f / (a.dx * a.dx), idy2 = 1.0f / (a.dy * a.dy);
+
+    float acc[3];
+    // ---- D2var terms (we_op.cpp:647-657, 1298-1308) ----
+    const SX mux = mx_line(c, MP_MU, zh);
+    const SZ muz = mz_line(c, MP_MU, xh);
+    if (PH == ELASTIC) {
+        W5 wx{}, wz{};
+        if (xin) wx = d2w(mux(ix - 2), mux(ix - 1), mux(ix), mux(ix + 1), mux(ix + 2));
+        if (zin) wz = d2w(muz(iz - 2), muz(iz - 1), muz(iz), muz(iz + 1), muz(iz + 2));
+        const W5 wy = d2w(th.qmu[0], th.qmu[1], th.qmu[2], th.qmu[3], th.qmu[4]);
+        for (int k = 0; k < 3; k++) {
+            const float adx = (k == 0 ? 2.0f : 1.0f) / (a.dx * a.dx);
+            const float ady = (k == 1 ? 2.0f : 1.0f) / (a.dy * a.dy);
+            const float adz = (k == 2 ? 2.0f : 1.0f) / (a.dz * a.dz);
+            const SX ul = ux_line(c, r0, k, izw);
+            const SZ uzl = uz_line(c, r0, k, ixw);
+            float v = xin ? d2apply(wx, adx, ul(ix - 2), ul(ix - 1), ul(ix), ul(ix + 1), ul(ix + 2))
+                          : d2var_row(ul, mux, ix, g.nx, adx);
+            v += d2apply(wy, ady, s.u[rm2][k][ixw][izw], s.u[rm1][k][ixw][izw], s.u[r0][k][ixw][izw],
+                         s.u[rp1][k][ixw][izw], s.u[rp2][k][ixw][izw]);
+            v += zin ? d2apply(wz, adz, uzl(iz - 2), uzl(iz - 1), uzl(iz), uzl(iz + 1), uzl(iz + 2))
+                     : d2var_row(uzl, muz, iz, g.nz, adz);
+            acc[k] = v;
+        }
+    } else {
+        // VTI: comp0 x:c11b y:c66 z:mu ; comp1 x:c66 y:c11b z:mu ; comp2 mu, mu, 2mu
+        const C11bS<SX, SX> bx{mx_line(c, MP_EPS, zh), mux};
+        const SX c6x = mx_line(c, MP_C66, zh);
+        W5 wxb{}, wx6{}, wxm{}, wz{};
+        if (xin) {
+            wxb = d2w(bx(ix - 2), bx(ix - 1), bx(ix), bx(ix + 1), bx(ix + 2));
+            wx6 = d2w(c6x(ix - 2), c6x(ix - 1), c6x(ix), c6x(ix + 1), c6x(ix + 2));
+            wxm = d2w(mux(ix - 2), mux(ix - 1), mux(ix), mux(ix + 1), mux(ix + 2));
+        }
+        if (zin) wz = d2w(muz(iz - 2), muz(iz - 1), muz(iz), muz(iz + 1), muz(iz + 2));
+        float qb[5];
+        for (int k = 0; k < 5; k++) qb[k] = 2.f * (1.f + 2.f * th.qeps[k]) * th.qmu[k];
+        const W5 wyb = d2w(qb[0], qb[1], qb[2], qb[3], qb[4]);
+        const W5 wy6 = d2w(th.q66[0], th.q66[1], th.q66[2], th.q66[3], th.q66[4]);
+        const W5 wym = d2w(th.qmu[0], th.qmu[1], th.qmu[2], th.qmu[3], th.qmu[4]);
+        for (int k = 0; k < 3; k++) {
+            const W5 &wx = k == 0 ? wxb : (k == 1 ? wx6 : wxm);
+            const W5 &wy = k == 0 ? wy6 : (k == 1 ? wyb : wym);
+            const float adz = (k == 2 ? 2.0f : 1.0f) / (a.dz * a.dz);
+            const SX ul = ux_line(c, r0, k, izw);
+            const SZ uzl = uz_line(c, r0, k, ixw);
+            float v;
+            if (xin) v = d2apply(wx, idx2, ul(ix - 2), ul(ix - 1), ul(ix), ul(ix + 1), ul(ix + 2));
+            else if (k == 0) v = d2var_row(ul, bx, ix, g.nx, idx2);
+            else if (k == 1) v = d2var_row(ul, c6x, ix, g.nx, idx2);
+            else v = d2var_row(ul, mux, ix, g.nx, idx2);
+            v += d2apply(wy, idy2, s.u[rm2][k][ixw][izw], s.u[rm1][k][ixw][izw], s.u[r0][k][ixw][izw],
+                         s.u[rp1][k][ixw][izw], s.u[rp2][k][ixw][izw]);
+            v += zin ? d2apply(wz, adz, uzl(iz - 2), uzl(iz - 1), uzl(iz), uzl(iz + 1), uzl(iz + 2))
+                     : d2var_row(uzl, muz, iz, g.nz, adz);
+            acc[k] = v;
+        }
+    }
+
+    // ---- D1 of the stress combinations and the mixed terms (we_op.cpp:661-688, 1312-1349) ----
+    const SX Px = (PH == VTI) ? mx_line(c, MP_C66, zh) : mux;
+    const float *qP = (PH == VTI) ? th.q66 : th.qmu;
+    // comp 0: Dx(T0)/dx + Dy(P u_x1)/dy + Dz(mu u_x2)/dy (dy as in the reference, we_op.cpp:678)
+    acc[0] += d1_row(dx_line(c, DV_T0, zh), ix, g.nx) / a.dx;
+    acc[0] += d1m(th.qX1[0], qP[0], th.qX1[1], qP[1], th.qX1[3], qP[3], th.qX1[4], qP[4]) / a.dy;
+    acc[0] += d1_prod_row(dz_line(c, DV_X2, xh), muz, iz, g.nz) / a.dy;
+    // comp 1: Dy(T1)/dy + Dx(P u_y0)/dx + Dz(mu u_y2)/dz
+    acc[1] += d1i(th.qT[0], th.qT[1], th.qT[3], th.qT[4]) / a.dy;
+    acc[1] += d1_prod_row(dx_line(c, DV_Y0, zh), Px, ix, g.nx) / a.dx;
+    acc[1] += d1_prod_row(dz_line(c, DV_Y2, xh), muz, iz, g.nz) / a.dz;
+    // comp 2: Dz(T2)/dz + Dx(mu u_z0)/dx + Dy(mu u_z1)/dy
+    acc[2] += d1_row(dz_line(c, DV_T2, xh), iz, g.nz) / a.dz;
+    acc[2] += d1_prod_row(dx_line(c, DV_Z0, zh), mux, ix, g.nx) / a.dx;
+    acc[2] += d1m(th.qZ1[0], th.qmu[0], th.qZ1[1], th.qmu[1], th.qZ1[3], th.qmu[3], th.qZ1[4], th.qmu[4]) / a.dy;
+
+    // ---- SAT on x/z faces, update, scaling, taper ----
+    const float dt2 = a.dt * a.dt;
+    const float rho = a.m[2][i];
+    const bool face = ix == 0 || ix == g.nx - 1 || iz == 0 || iz == g.nz - 1;
+    const bool tz = a.tap[0][iz] != 1.f || a.tap[1][iz] != 1.f || a.tap[2][ix] != 1.f || a.tap[3][ix] != 1.f ||
+                    a.tap[4][y] != 1.f || a.tap[5][y] != 1.f;
+    if (face) {
+        const StepArgs sa = shot_args(a, c.shot);
+        for (int k = 0; k < 3; k++) acc[k] = elastic_sat<PH>(sa, acc[k], k, ix, y, iz);
+    }
+    for (int k = 0; k < 3; k++) {
+        float v = acc[k];
+        const float p = a.prev[k][c.so + i];
+        const float pe = (a.taper_prev && tz) ? taper(a, p, ix, y, iz) : p;
+        v = dt2 * v / rho + 2.f * s.u[r0][k][ixw][izw] - pe;
+        if (face) v = boundary_scale(a, v, k, ix, y, iz);
+        if (tz) v = taper(a, v, ix, y, iz);
+        a.next[k][c.so + i] = v;
+    }
+}
+
+// Tile origin and end of the output rows of tile k along an axis of n points
+// tiled by T: regular tiles start at k*T, the last one is shifted to end at n
+// and the one before it stops where the last begins, so that every row of the
+// SBP closures belongs to the first or the last tile, whose windows hold all
+// samples those rows read.
+FWI_HD void tile_range(int k, int n, int T, int &origin, int &end)
+{
+    const int K = (n + T - 1) / T;
+    if (k == K - 1) {
+        origin = n - T;
+        end = n;
+    } else {
+        origin = k * T;
+        end = k * T + T < n - T ? k * T + T : n - T;
+    }
+}
+
+// The march of one CTA over output planes [ya, yb) (all inside [8, ny-8)).
+template <int PH>
+FWI_HD void fz_prologue(FusedCtx &c, int tid, int ya)
+{
+    for (int q = ya - 4; q < ya; q++) fz_load_u(c, tid, q);
+}
+
+}  // namespace fwi

@@ -174,11 +174,42 @@ inline float sincf_ref(float x)
 }
 }  // namespace
 
+namespace {
+// Sinc-resampler taps of one output sample: the weights depend on the two time
+// axes only, so they are evaluated once (with the reference's mixed float /
+// double semantics, operator.cpp:472-520) and applied to every trace.
+struct SincTaps {
+    std::vector<int> first, count;  // per output sample
+    std::vector<float> s;           // windowed-sinc factor (float, as returned by sinc())
+    std::vector<double> win;        // cosine window (double)
+};
+SincTaps sinc_taps(int hl, int nt_in, float dt_in, int nt_out, float dt_out)
+{
+    SincTaps T;
+    T.first.resize(nt_out);
+    T.count.resize(nt_out);
+    const float a = 0.5f;
+    for (int itd = 0; itd < nt_out; itd++) {
+        const float t = itd * dt_out;
+        const int itm0 = (int)std::floor((double)(t / dt_in));
+        const int lo = std::max(0, itm0 - hl + 1), hi = std::min(nt_in - 1, itm0 + hl);
+        T.first[itd] = lo;
+        T.count[itd] = std::max(0, hi - lo + 1);
+        for (int itm = lo; itm <= hi; itm++) {
+            T.s.push_back(sincf_ref((float)(M_PI * (t - itm * dt_in) / dt_in)));
+            T.win.push_back(a + (1 - a) * std::cos(M_PI * (itm - t / dt_in) / hl));
+        }
+    }
+    return T;
+}
+}  // namespace
+
 void resample_forward(bool sinc, int hl, const float *in, int nt_in, float dt_in, float *out, int nt_out, float dt_out,
                       int ntr)
 {
     if (!sinc) {
         // operator.cpp:424-444
+#pragma omp parallel for schedule(static)
         for (int ix = 0; ix < ntr; ix++)
             for (int it = 0; it < nt_out; it++) {
                 const int i = std::min(nt_in - 1, (int)std::floor((double)(it * dt_out / dt_in)));
@@ -189,20 +220,21 @@ void resample_forward(bool sinc, int hl, const float *in, int nt_in, float dt_in
             }
         return;
     }
-    // operator.cpp:472-494, alpha = 0.5
-    const float a = 0.5f;
-    for (int ix = 0; ix < ntr; ix++)
+    const SincTaps T = sinc_taps(hl, nt_in, dt_in, nt_out, dt_out);
+    std::vector<size_t> off(nt_out + 1, 0);
+    for (int itd = 0; itd < nt_out; itd++) off[itd + 1] = off[itd] + T.count[itd];
+#pragma omp parallel for schedule(static)
+    for (int ix = 0; ix < ntr; ix++) {
+        const float *src = in + (size_t)ix * nt_in;
         for (int itd = 0; itd < nt_out; itd++) {
-            const float t = itd * dt_out;
-            const int itm0 = (int)std::floor((double)(t / dt_in));
             float acc = 0.f;
-            for (int itm = std::max(0, itm0 - hl + 1); itm <= std::min(nt_in - 1, itm0 + hl); itm++) {
-                const float s = sincf_ref((float)(M_PI * (t - itm * dt_in) / dt_in));
-                const double win = a + (1 - a) * std::cos(M_PI * (itm - t / dt_in) / hl);
-                acc = (float)((double)acc + (double)(in[(size_t)ix * nt_in + itm] * s) * win);
+            for (int k = 0; k < T.count[itd]; k++) {
+                const size_t q = off[itd] + k;
+                acc = (float)((double)acc + (double)(src[T.first[itd] + k] * T.s[q]) * T.win[q]);
             }
             out[(size_t)ix * nt_out + itd] = acc;
         }
+    }
 }
 
 void resample_adjoint(bool sinc, int hl, float *in, int nt_in, float dt_in, const float *out, int nt_out, float dt_out,
@@ -210,6 +242,7 @@ void resample_adjoint(bool sinc, int hl, float *in, int nt_in, float dt_in, cons
 {
     // accumulates into `in` (callers zero it first for add=false), operator.cpp:446-520
     if (!sinc) {
+#pragma omp parallel for schedule(static)
         for (int ix = 0; ix < ntr; ix++)
             for (int it = 0; it < nt_out; it++) {
                 const int i = std::min(nt_in - 1, (int)std::floor((double)(it * dt_out / dt_in)));
@@ -221,18 +254,20 @@ void resample_adjoint(bool sinc, int hl, float *in, int nt_in, float dt_in, cons
             }
         return;
     }
-    const float a = 0.5f;
-    for (int ix = 0; ix < ntr; ix++)
-        for (int itd = 0; itd < nt_out; itd++) {
-            const float t = itd * dt_out;
-            const int itm0 = (int)std::floor((double)(t / dt_in));
-            for (int itm = std::max(0, itm0 - hl + 1); itm <= std::min(nt_in - 1, itm0 + hl); itm++) {
-                const float s = sincf_ref((float)(M_PI * (t - itm * dt_in) / dt_in));
-                const double win = a + (1 - a) * std::cos(M_PI * (itm - t / dt_in) / hl);
-                float &dst = in[(size_t)ix * nt_in + itm];
-                dst = (float)((double)dst + (double)(out[(size_t)ix * nt_out + itd] * s) * win);
+    const SincTaps T = sinc_taps(hl, nt_in, dt_in, nt_out, dt_out);
+    std::vector<size_t> off(nt_out + 1, 0);
+    for (int itd = 0; itd < nt_out; itd++) off[itd + 1] = off[itd] + T.count[itd];
+#pragma omp parallel for schedule(static)
+    for (int ix = 0; ix < ntr; ix++) {
+        float *dst = in + (size_t)ix * nt_in;
+        const float *src = out + (size_t)ix * nt_out;
+        for (int itd = 0; itd < nt_out; itd++)
+            for (int k = 0; k < T.count[itd]; k++) {
+                const size_t q = off[itd] + k;
+                float &d = dst[T.first[itd] + k];
+                d = (float)((double)d + (double)(src[itd] * T.s[q]) * T.win[q]);
             }
-        }
+    }
 }
 
 void apply_ht(bool inv, const float *in, float *out, int ntr, int nt, float dt)

@@ -49,6 +49,7 @@ struct StepArgs {
     int taper_prev;
     // batch layout: shot s of a field component c lives at curr[c] + s*sst
     int nyb;                   // y blocks per shot in the launch grid
+    int y0, y1;                // planes [y0, y1) covered by the launch
     int64_t sst;               // wavefield shot stride (floats)
     int64_t ast;               // derivative-scratch shot stride (floats)
 };
@@ -426,6 +427,7 @@ struct AuxArgs {
     float *aux[9];
     float *dlag[3];  // optional: u_x[0], u_y[1], u_z[2] (kept for imaging), may be null
     int nyb;
+    int y0, y1;
     int64_t sst, ast;
 };
 
