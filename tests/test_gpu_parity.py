@@ -117,12 +117,12 @@ def test_batch_matches_single_shot_operator():
 # --- grids large enough for the fused interior kernel (nz >= 32, nx >= 16, ny > 16) ---
 
 def _elastic_fused(mt=True):
-    sv = synth.elastic_layered(n=40, nsteps=150, taper=6, rec_stride=3, nshots=1)
+    sv = synth.elastic_layered(n=48, nsteps=150, taper=6, rec_stride=3, nshots=1)
     # non-cubic grid so that tiles, chunks and closures all differ per axis
     sv.model = np.ascontiguousarray(sv.model[:, :36, :40, :48])
     sv.nx, sv.ny, sv.nz = 40, 36, 48
     sv.par.sxyz = [[0.5 * 40 * sv.dx, 0.45 * 36 * sv.dx, 0.3 * 48 * sv.dx]]
-    sv.par.rxyz = [[r for r in sv.par.rxyz[0] if r[1] <= 35 * sv.dx]]
+    sv.par.rxyz = [[r for r in sv.par.rxyz[0] if r[0] <= 39 * sv.dx and r[1] <= 35 * sv.dx]]
     sv.par.mt = mt
     return sv
 
