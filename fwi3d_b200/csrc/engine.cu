@@ -264,7 +264,9 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     fields_.alloc(sizeof(float) * 3 * (size_t)pb.nshots * nc * n);
     if (pb.nmodels != 2) aux_.alloc(sizeof(float) * (size_t)pb.nshots * (pb.nmodels == 6 ? 9 : 7) * n);
     const char *env = std::getenv("FWI_FUSED");
-    fused_ = pb.nmodels != 2 && !(env && env[0] == '0') && pb.nx >= fz::TX && pb.nz >= fz::TZ &&
+    // The tiling keeps every SBP closure row in the first or the last tile only
+    // when each axis is at least one tile plus the 6 closure rows long.
+    fused_ = pb.nmodels != 2 && !(env && env[0] == '0') && pb.nx >= fz::TX + 6 && pb.nz >= fz::TZ + 6 &&
              pb.ny > 2 * fz::YPAD;
     if (fused_) {
         CK(cudaFuncSetAttribute(k_elastic_fused<ELASTIC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
