@@ -123,8 +123,8 @@ __global__ void k_elastic_step(StepArgs a)
 
 // Fused elastic step over planes [ylo, yhi) (see fused.cuh).  grid: (z tiles,
 // x tiles, y chunks x shots), block (TZ, TX).
-template <int PH>
-__global__ void __launch_bounds__(fz::NT, 2) k_elastic_fused(const __grid_constant__ StepArgs a, int nchunks)
+template <int PH, int MINB>
+__global__ void __launch_bounds__(fz::NT, MINB) k_elastic_fused(const __grid_constant__ StepArgs a, int nchunks)
 {
     extern __shared__ __align__(16) unsigned char fz_smem[];
     FusedCtx c;
@@ -146,7 +146,8 @@ __global__ void __launch_bounds__(fz::NT, 2) k_elastic_fused(const __grid_consta
     fz_prologue<PH>(c, tid, ya);
     __syncthreads();
     for (int y = ya - 4; y < yb; y++) {
-        fz_load_u(c, tid, y + 4);
+        fz_slots(c, y);
+        fz_load_u(c, tid, y + 4, c.sl[6]);
         if (y >= ya) fz_load_mat<PH>(c, tid, y);
         __syncthreads();
         fz_column<PH>(c, th, tid, y + 2);
@@ -268,10 +269,18 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     // when each axis is at least one tile plus the 6 closure rows long.
     fused_ = pb.nmodels != 2 && !(env && env[0] == '0') && pb.nx >= fz::TX + 6 && pb.nz >= fz::TZ + 6 &&
              pb.ny > 2 * fz::YPAD;
+    // Occupancy variant of the fused kernel: 1 CTA per SM with up to 128
+    // registers (default) or 2 CTAs per SM with 64 registers.
+    const char *mb = std::getenv("FWI_FUSED_MINB");
+    fused_minb_ = (mb && mb[0] == '2') ? 2 : 1;
     if (fused_) {
-        CK(cudaFuncSetAttribute(k_elastic_fused<ELASTIC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CK(cudaFuncSetAttribute(k_elastic_fused<ELASTIC, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(FusedSmem)));
-        CK(cudaFuncSetAttribute(k_elastic_fused<VTI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CK(cudaFuncSetAttribute(k_elastic_fused<VTI, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(FusedSmem)));
+        CK(cudaFuncSetAttribute(k_elastic_fused<ELASTIC, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(FusedSmem)));
+        CK(cudaFuncSetAttribute(k_elastic_fused<VTI, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(FusedSmem)));
     }
 }
@@ -370,6 +379,14 @@ StepArgs make_step_args(const Problem &pb, const float *m, const float *const sd
     a.dy = pb.dy;
     a.dz = pb.dz;
     a.dt = pb.dt;
+    a.idx = 1.0f / pb.dx;
+    a.idy = 1.0f / pb.dy;
+    a.idz = 1.0f / pb.dz;
+    const float d[3] = {pb.dx, pb.dy, pb.dz};
+    for (int k = 0; k < 3; k++) {
+        a.ad1[k] = 1.0f / (d[k] * d[k]);
+        a.ad2[k] = 2.0f / (d[k] * d[k]);
+    }
     const int64_t n = pb.nxyz();
     for (int k = 0; k < pb.nmodels; k++) a.m[k] = m + k * n;
     for (int f = 0; f < 6; f++) {
@@ -485,13 +502,17 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         for (int k = 0; k < 9; k++) f.aux[k] = nullptr;
         const int kz = (pb_.nz + fz::TZ - 1) / fz::TZ, kx = (pb_.nx + fz::TX - 1) / fz::TX;
         const int tiles = kz * kx * pb_.nshots;
-        int nch = (600 + tiles - 1) / tiles;
+        const int target = 148 * fused_minb_ * 4;  // about four waves of resident CTAs
+        int nch = (target + tiles - 1) / tiles;
         nch = std::max(1, std::min(nch, (f.y1 - f.y0) / 16));
         const dim3 grd(kz, kx, nch * pb_.nshots), fblk(fz::TZ, fz::TX);
-        if (pb_.nmodels == 3)
-            k_elastic_fused<ELASTIC><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch);
-        else
-            k_elastic_fused<VTI><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch);
+        if (fused_minb_ == 2) {
+            if (pb_.nmodels == 3) k_elastic_fused<ELASTIC, 2><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch);
+            else k_elastic_fused<VTI, 2><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch);
+        } else {
+            if (pb_.nmodels == 3) k_elastic_fused<ELASTIC, 1><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch);
+            else k_elastic_fused<VTI, 1><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch);
+        }
     }
     CK(cudaGetLastError());
 }

@@ -124,6 +124,7 @@ private:
     const float *taper_ptr_[6] = {};
     int scale_ = 0;
     bool fused_ = false;           // fused elastic kernel for the interior planes
+    int fused_minb_ = 1;           // resident CTAs per SM the fused kernel is compiled for
     DevBuf src_dev_, rcv_dev_;
     DevInj inj_;
     DevExt ext_;

@@ -60,8 +60,10 @@ struct FusedCtx {
     int64_t so;        // wavefield offset of this shot (shot * sst)
     int x0, z0;        // tile (window) origin
     int xend, zend;    // end of this tile's output rows
+    int sl[7];         // ring slots of planes y-2 .. y+4 for the current march step
     FusedSmem *sm;
 };
+
 
 // Smem line accessors (global index -> smem slot).
 struct SZ {  // along z at fixed (slot, comp, xw)
@@ -78,13 +80,22 @@ struct SX {  // along x at fixed zw
 
 FWI_HD int ring(int q) { return ((q % fz::NRING) + fz::NRING) % fz::NRING; }
 
+// Ring slots of planes y-2 .. y+4.
+FWI_HD void fz_slots(FusedCtx &c, int y)
+{
+    int s = ring(y - 2);
+    for (int k = 0; k < 7; k++) {
+        c.sl[k] = s;
+        s = s + 1 == fz::NRING ? 0 : s + 1;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Phase A: load displacement plane q (tile + 4 halo) into its ring slot.
 // ---------------------------------------------------------------------------
-FWI_HD void fz_load_u(FusedCtx &c, int tid, int q)
+FWI_HD void fz_load_u(FusedCtx &c, int tid, int q, int slot)
 {
     const Dims &g = c.a->g;
-    const int slot = ring(q);
     for (int p = tid; p < fz::XW * fz::ZW; p += fz::NT) {
         const int xw = p / fz::ZW, zw = p - xw * fz::ZW;
         const int ix = c.x0 - fz::HW + xw, iz = c.z0 - fz::HW + zw;
@@ -126,25 +137,26 @@ FWI_HD float d1_sg(const S &s, const Line &gl, int i, int n)
 
 // First derivatives of displacement component k at (ix, q, iz) along x, y, z
 // from the ring (with the 1/h).  ixw/izw: smem coordinates in the ring window.
-FWI_HD float fz_dx(const FusedCtx &c, int k, int q, int ix, int iz, int izw)
+FWI_HD float fz_dx(const FusedCtx &c, int k, int q, int slot, int ix, int iz, int izw)
 {
     const Dims &g = c.a->g;
-    const SX s{&c.sm->u[ring(q)][k][0][izw], c.x0 - fz::HW, fz::ZW};
-    return d1_sg(s, g.lx(c.a->curr[k] + c.so, q, iz), ix, g.nx) / c.a->dx;
+    const SX s{&c.sm->u[slot][k][0][izw], c.x0 - fz::HW, fz::ZW};
+    return d1_sg(s, g.lx(c.a->curr[k] + c.so, q, iz), ix, g.nx) * c.a->idx;
 }
-FWI_HD float fz_dz(const FusedCtx &c, int k, int q, int ix, int ixw, int iz)
+FWI_HD float fz_dz(const FusedCtx &c, int k, int q, int slot, int ix, int ixw, int iz)
 {
     const Dims &g = c.a->g;
-    const SZ s{&c.sm->u[ring(q)][k][ixw][0], c.z0 - fz::HW};
-    return d1_sg(s, g.lz(c.a->curr[k] + c.so, ix, q), iz, g.nz) / c.a->dz;
+    const SZ s{&c.sm->u[slot][k][ixw][0], c.z0 - fz::HW};
+    return d1_sg(s, g.lz(c.a->curr[k] + c.so, ix, q), iz, g.nz) * c.a->idz;
 }
-// Dy at plane q: interior rows only (the fused launch keeps q in [6, ny-6)).
-FWI_HD float fz_dy(const FusedCtx &c, int k, int q, int ixw, int izw)
+// Dy at a plane from the ring slots of its four neighbours: interior rows only
+// (the fused launch keeps every differentiated plane in [6, ny-6)).
+FWI_HD float fz_dy(const FusedCtx &c, int k, const int *sn, int ixw, int izw)
 {
     const SbpTables &t = sbp();
-    const float um2 = c.sm->u[ring(q - 2)][k][ixw][izw], um1 = c.sm->u[ring(q - 1)][k][ixw][izw];
-    const float up1 = c.sm->u[ring(q + 1)][k][ixw][izw], up2 = c.sm->u[ring(q + 2)][k][ixw][izw];
-    return (t.d1c0 * (up1 - um1) + t.d1c1 * (up2 - um2)) / c.a->dy;
+    const float um2 = c.sm->u[sn[0]][k][ixw][izw], um1 = c.sm->u[sn[1]][k][ixw][izw];
+    const float up1 = c.sm->u[sn[2]][k][ixw][izw], up2 = c.sm->u[sn[3]][k][ixw][izw];
+    return (t.d1c0 * (up1 - um1) + t.d1c1 * (up2 - um2)) * c.a->idy;
 }
 
 // ---------------------------------------------------------------------------
@@ -164,14 +176,16 @@ FWI_HD void fz_derived(FusedCtx &c, int tid, int y)
             continue;
         }
         const int ixw = xh + (fz::HW - fz::HD), izw = zh + (fz::HW - fz::HD);
-        const float ux0 = fz_dx(c, 0, y, ix, iz, izw);
-        const float uy1 = fz_dy(c, 1, y, ixw, izw);
-        const float uz2 = fz_dz(c, 2, y, ix, ixw, iz);
+        const int s0 = c.sl[2];
+        const int sn[4] = {c.sl[0], c.sl[1], c.sl[3], c.sl[4]};
+        const float ux0 = fz_dx(c, 0, y, s0, ix, iz, izw);
+        const float uy1 = fz_dy(c, 1, sn, ixw, izw);
+        const float uz2 = fz_dz(c, 2, y, s0, ix, ixw, iz);
         const float mu = c.sm->mp[MP_MU][xh][zh], lam = c.sm->mp[MP_LAM][xh][zh];
-        const float uy0 = fz_dy(c, 0, y, ixw, izw);
-        const float uz0 = fz_dz(c, 0, y, ix, ixw, iz);
-        const float ux2 = fz_dx(c, 2, y, ix, iz, izw);
-        const float uy2 = fz_dy(c, 2, y, ixw, izw);
+        const float uy0 = fz_dy(c, 0, sn, ixw, izw);
+        const float uz0 = fz_dz(c, 0, y, s0, ix, ixw, iz);
+        const float ux2 = fz_dx(c, 2, y, s0, ix, iz, izw);
+        const float uy2 = fz_dy(c, 2, sn, ixw, izw);
         if (PH == ELASTIC) {
             const float T = lam * (ux0 + uy1 + uz2);
             dv0[DV_T0 * stride] = T;
@@ -215,11 +229,14 @@ FWI_HD void fz_column(FusedCtx &c, FusedThread &th, int tid, int q)
     const int64_t i = g.idx(ix, q, iz);
     const float mu = c.a->m[1][i], lam = c.a->m[0][i];
     th.qmu[4] = mu;
-    const float ux0 = fz_dx(c, 0, q, ix, iz, izw);
-    const float uy1 = fz_dy(c, 1, q, ixw, izw);
-    const float uz2 = fz_dz(c, 2, q, ix, ixw, iz);
-    const float ux1 = fz_dx(c, 1, q, ix, iz, izw);
-    const float uz1 = fz_dz(c, 1, q, ix, ixw, iz);
+    // plane q = y+2 sits in slot sl[4]; its neighbours q-2..q+2 in sl[2..6]
+    const int s0 = c.sl[4];
+    const int sn[4] = {c.sl[2], c.sl[3], c.sl[5], c.sl[6]};
+    const float ux0 = fz_dx(c, 0, q, s0, ix, iz, izw);
+    const float uy1 = fz_dy(c, 1, sn, ixw, izw);
+    const float uz2 = fz_dz(c, 2, q, s0, ix, ixw, iz);
+    const float ux1 = fz_dx(c, 1, q, s0, ix, iz, izw);
+    const float uz1 = fz_dz(c, 1, q, s0, ix, ixw, iz);
     if (PH == ELASTIC) {
         th.qT[4] = lam * (ux0 + uy1 + uz2);
         th.qX1[4] = ux1;
@@ -298,8 +315,8 @@ FWI_HD void fz_output(FusedCtx &c, const FusedThread &th, int tid, int y)
     const int ixw = lx + fz::HW, izw = lz + fz::HW;
     const int xh = lx + fz::HD, zh = lz + fz::HD;
     const FusedSmem &s = *c.sm;
-    const int r0 = ring(y), rm1 = ring(y - 1), rm2 = ring(y - 2), rp1 = ring(y + 1), rp2 = ring(y + 2);
-    const float idx2 = 1.0f / (a.dx * a.dx), idy2 = 1.0f / (a.dy * a.dy);
+    const int r0 = c.sl[2], rm1 = c.sl[1], rm2 = c.sl[0], rp1 = c.sl[3], rp2 = c.sl[4];
+    const float idx2 = a.ad1[0], idy2 = a.ad1[1];
 
     float acc[3];
     // ---- D2var terms (we_op.cpp:647-657, 1298-1308) ----
@@ -311,9 +328,9 @@ FWI_HD void fz_output(FusedCtx &c, const FusedThread &th, int tid, int y)
         if (zin) wz = d2w(muz(iz - 2), muz(iz - 1), muz(iz), muz(iz + 1), muz(iz + 2));
         const W5 wy = d2w(th.qmu[0], th.qmu[1], th.qmu[2], th.qmu[3], th.qmu[4]);
         for (int k = 0; k < 3; k++) {
-            const float adx = (k == 0 ? 2.0f : 1.0f) / (a.dx * a.dx);
-            const float ady = (k == 1 ? 2.0f : 1.0f) / (a.dy * a.dy);
-            const float adz = (k == 2 ? 2.0f : 1.0f) / (a.dz * a.dz);
+            const float adx = k == 0 ? a.ad2[0] : a.ad1[0];
+            const float ady = k == 1 ? a.ad2[1] : a.ad1[1];
+            const float adz = k == 2 ? a.ad2[2] : a.ad1[2];
             const SX ul = ux_line(c, r0, k, izw);
             const SZ uzl = uz_line(c, r0, k, ixw);
             float v = xin ? d2apply(wx, adx, ul(ix - 2), ul(ix - 1), ul(ix), ul(ix + 1), ul(ix + 2))
@@ -343,7 +360,7 @@ FWI_HD void fz_output(FusedCtx &c, const FusedThread &th, int tid, int y)
         for (int k = 0; k < 3; k++) {
             const W5 &wx = k == 0 ? wxb : (k == 1 ? wx6 : wxm);
             const W5 &wy = k == 0 ? wy6 : (k == 1 ? wyb : wym);
-            const float adz = (k == 2 ? 2.0f : 1.0f) / (a.dz * a.dz);
+            const float adz = k == 2 ? a.ad2[2] : a.ad1[2];
             const SX ul = ux_line(c, r0, k, izw);
             const SZ uzl = uz_line(c, r0, k, ixw);
             float v;
@@ -363,17 +380,17 @@ FWI_HD void fz_output(FusedCtx &c, const FusedThread &th, int tid, int y)
     const SX Px = (PH == VTI) ? mx_line(c, MP_C66, zh) : mux;
     const float *qP = (PH == VTI) ? th.q66 : th.qmu;
     // comp 0: Dx(T0)/dx + Dy(P u_x1)/dy + Dz(mu u_x2)/dy (dy as in the reference, we_op.cpp:678)
-    acc[0] += d1_row(dx_line(c, DV_T0, zh), ix, g.nx) / a.dx;
-    acc[0] += d1m(th.qX1[0], qP[0], th.qX1[1], qP[1], th.qX1[3], qP[3], th.qX1[4], qP[4]) / a.dy;
-    acc[0] += d1_prod_row(dz_line(c, DV_X2, xh), muz, iz, g.nz) / a.dy;
+    acc[0] += d1_row(dx_line(c, DV_T0, zh), ix, g.nx) * a.idx;
+    acc[0] += d1m(th.qX1[0], qP[0], th.qX1[1], qP[1], th.qX1[3], qP[3], th.qX1[4], qP[4]) * a.idy;
+    acc[0] += d1_prod_row(dz_line(c, DV_X2, xh), muz, iz, g.nz) * a.idy;
     // comp 1: Dy(T1)/dy + Dx(P u_y0)/dx + Dz(mu u_y2)/dz
-    acc[1] += d1i(th.qT[0], th.qT[1], th.qT[3], th.qT[4]) / a.dy;
-    acc[1] += d1_prod_row(dx_line(c, DV_Y0, zh), Px, ix, g.nx) / a.dx;
-    acc[1] += d1_prod_row(dz_line(c, DV_Y2, xh), muz, iz, g.nz) / a.dz;
+    acc[1] += d1i(th.qT[0], th.qT[1], th.qT[3], th.qT[4]) * a.idy;
+    acc[1] += d1_prod_row(dx_line(c, DV_Y0, zh), Px, ix, g.nx) * a.idx;
+    acc[1] += d1_prod_row(dz_line(c, DV_Y2, xh), muz, iz, g.nz) * a.idz;
     // comp 2: Dz(T2)/dz + Dx(mu u_z0)/dx + Dy(mu u_z1)/dy
-    acc[2] += d1_row(dz_line(c, DV_T2, xh), iz, g.nz) / a.dz;
-    acc[2] += d1_prod_row(dx_line(c, DV_Z0, zh), mux, ix, g.nx) / a.dx;
-    acc[2] += d1m(th.qZ1[0], th.qmu[0], th.qZ1[1], th.qmu[1], th.qZ1[3], th.qmu[3], th.qZ1[4], th.qmu[4]) / a.dy;
+    acc[2] += d1_row(dz_line(c, DV_T2, xh), iz, g.nz) * a.idz;
+    acc[2] += d1_prod_row(dx_line(c, DV_Z0, zh), mux, ix, g.nx) * a.idx;
+    acc[2] += d1m(th.qZ1[0], th.qmu[0], th.qZ1[1], th.qmu[1], th.qZ1[3], th.qmu[3], th.qZ1[4], th.qmu[4]) * a.idy;
 
     // ---- SAT on x/z faces, update, scaling, taper ----
     const float dt2 = a.dt * a.dt;
@@ -381,15 +398,14 @@ FWI_HD void fz_output(FusedCtx &c, const FusedThread &th, int tid, int y)
     const bool face = ix == 0 || ix == g.nx - 1 || iz == 0 || iz == g.nz - 1;
     const bool tz = a.tap[0][iz] != 1.f || a.tap[1][iz] != 1.f || a.tap[2][ix] != 1.f || a.tap[3][ix] != 1.f ||
                     a.tap[4][y] != 1.f || a.tap[5][y] != 1.f;
-    if (face) {
-        const StepArgs sa = shot_args(a, c.shot);
-        for (int k = 0; k < 3; k++) acc[k] = elastic_sat<PH>(sa, acc[k], k, ix, y, iz);
-    }
+    if (face)
+        for (int k = 0; k < 3; k++) acc[k] = elastic_sat<PH>(a, acc[k], k, ix, y, iz, c.so);
+    const float irho = 1.0f / rho;
     for (int k = 0; k < 3; k++) {
         float v = acc[k];
         const float p = a.prev[k][c.so + i];
         const float pe = (a.taper_prev && tz) ? taper(a, p, ix, y, iz) : p;
-        v = dt2 * v / rho + 2.f * s.u[r0][k][ixw][izw] - pe;
+        v = dt2 * v * irho + 2.f * s.u[r0][k][ixw][izw] - pe;
         if (face) v = boundary_scale(a, v, k, ix, y, iz);
         if (tz) v = taper(a, v, ix, y, iz);
         a.next[k][c.so + i] = v;
@@ -417,7 +433,7 @@ FWI_HD void tile_range(int k, int n, int T, int &origin, int &end)
 template <int PH>
 FWI_HD void fz_prologue(FusedCtx &c, int tid, int ya)
 {
-    for (int q = ya - 4; q < ya; q++) fz_load_u(c, tid, q);
+    for (int q = ya - 4; q < ya; q++) fz_load_u(c, tid, q, ring(q));
 }
 
 }  // namespace fwi

@@ -35,6 +35,8 @@ enum Aux { AUX_T0 = 0, AUX_T1 = 1, AUX_T2 = 2, AUX_X1 = 3, AUX_X2 = 4, AUX_Y0 = 
 struct StepArgs {
     Dims g;
     float dx, dy, dz, dt;
+    float idx, idy, idz;       // 1/h per axis
+    float ad1[3], ad2[3];      // a/(h*h) per axis (x, y, z) for a = 1 and a = 2, as the reference forms them
     // converted model: acoustic {K, 1/rho}; elastic {lambda, mu, rho}; VTI {lambda, mu, rho, c13, eps, c66}
     const float *m[6];
     const float *curr[3];
@@ -103,9 +105,9 @@ FWI_HD float boundary_scale(const StepArgs &a, float v, int c, int ix, int iy, i
     return v / a.sdiv[f][c][off];
 }
 
-FWI_HD float prev_eff(const StepArgs &a, int c, int64_t i, int ix, int iy, int iz)
+FWI_HD float prev_eff(const StepArgs &a, int c, int64_t i, int ix, int iy, int iz, int64_t so = 0)
 {
-    const float p = a.prev[c][i];
+    const float p = a.prev[c][so + i];
     return a.taper_prev ? taper(a, p, ix, iy, iz) : p;
 }
 
@@ -330,8 +332,9 @@ FWI_HD SatTerm sat_coefs(const StepArgs &a, int n, int c, int64_t i, bool absorb
 }
 
 template <int PH>
-FWI_HD float elastic_face(const StepArgs &a, float acc, int c, int n, bool hi, int ix, int iy, int iz)
+FWI_HD float elastic_face(const StepArgs &a, float acc, int c, int n, bool hi, int ix, int iy, int iz, int64_t so = 0)
 {
+    const float *cu[3] = {a.curr[0] + so, a.curr[1] + so, a.curr[2] + so};
     const Dims &g = a.g;
     const int64_t i = g.idx(ix, iy, iz);
     const bool absorbing = a.bc[2 * (n == 0 ? 1 : (n == 1 ? 2 : 0)) + (hi ? 1 : 0)] == BC_ABSORB;
@@ -344,29 +347,29 @@ FWI_HD float elastic_face(const StepArgs &a, float acc, int c, int n, bool hi, i
     float T1 = 0.f, T2 = 0.f, N0 = 0.f, S;
     if (n == 2) {
         d1 = a.dx; d2 = a.dy; dn = a.dz;
-        const float *in1 = (c == 2) ? a.curr[0] : a.curr[2];
-        const float *in2 = (c == 2) ? a.curr[1] : a.curr[2];
+        const float *in1 = (c == 2) ? cu[0] : cu[2];
+        const float *in2 = (c == 2) ? cu[1] : cu[2];
         if (s.f1 != 0.f) T1 = d1_row(g.lx(in1, iy, iz), ix, g.nx);
         if (s.f2 != 0.f) T2 = d1_row(g.ly(in2, ix, iz), iy, g.ny);
-        const Line l3 = g.lz(a.curr[c], ix, iy);
+        const Line l3 = g.lz(cu[c], ix, iy);
         if (s.f3 != 0.f) N0 = d1_wall(l3, g.nz, hi);
         S = sbound(l3, g.nz, hi);
     } else if (n == 0) {
         d1 = a.dy; d2 = a.dz; dn = a.dx;
-        const float *in1 = (c == 0) ? a.curr[1] : a.curr[0];
-        const float *in2 = (c == 0) ? a.curr[2] : a.curr[0];
+        const float *in1 = (c == 0) ? cu[1] : cu[0];
+        const float *in2 = (c == 0) ? cu[2] : cu[0];
         if (s.f1 != 0.f) T1 = d1_row(g.ly(in1, ix, iz), iy, g.ny);
         if (s.f2 != 0.f) T2 = d1_row(g.lz(in2, ix, iy), iz, g.nz);
-        const Line l3 = g.lx(a.curr[c], iy, iz);
+        const Line l3 = g.lx(cu[c], iy, iz);
         if (s.f3 != 0.f) N0 = d1_wall(l3, g.nx, hi);
         S = sbound(l3, g.nx, hi);
     } else {
         d1 = a.dx; d2 = a.dz; dn = a.dy;
-        const float *in1 = (c == 1) ? a.curr[0] : a.curr[1];
-        const float *in2 = (c == 1) ? a.curr[2] : a.curr[1];
+        const float *in1 = (c == 1) ? cu[0] : cu[1];
+        const float *in2 = (c == 1) ? cu[2] : cu[1];
         if (s.f1 != 0.f) T1 = d1_row(g.lx(in1, iy, iz), ix, g.nx);
         if (s.f2 != 0.f) T2 = d1_row(g.lz(in2, ix, iy), iz, g.nz);
-        const Line l3 = g.ly(a.curr[c], ix, iz);
+        const Line l3 = g.ly(cu[c], ix, iz);
         if (s.f3 != 0.f) N0 = d1_wall(l3, g.ny, hi);
         S = sbound(l3, g.ny, hi);
     }
@@ -384,24 +387,24 @@ FWI_HD float elastic_face(const StepArgs &a, float acc, int c, int n, bool hi, i
         if (s.f3 != 0.f) v = v + s.f3 * N0 / dn;
     }
     v = v + s.f4 * S / dn;
-    if (s.f5 != 0.f) v = v - s.f5 * prev_eff(a, c, i, ix, iy, iz) / a.dt;
+    if (s.f5 != 0.f) v = v - s.f5 * prev_eff(a, c, i, ix, iy, iz, so) / a.dt;
     return acc - adh * v;
 }
 
 template <int PH>
-FWI_HD float elastic_sat(const StepArgs &a, float acc, int c, int ix, int iy, int iz)
+FWI_HD float elastic_sat(const StepArgs &a, float acc, int c, int ix, int iy, int iz, int64_t so = 0)
 {
     const Dims &g = a.g;
     // order of the reference: top, bottom, left, right, front, back
-    if (iz == 0 && (a.bc[TOP] == BC_FREE || a.bc[TOP] == BC_ABSORB)) acc = elastic_face<PH>(a, acc, c, 2, false, ix, iy, iz);
+    if (iz == 0 && (a.bc[TOP] == BC_FREE || a.bc[TOP] == BC_ABSORB)) acc = elastic_face<PH>(a, acc, c, 2, false, ix, iy, iz, so);
     if (iz == g.nz - 1 && (a.bc[BOTTOM] == BC_FREE || a.bc[BOTTOM] == BC_ABSORB))
-        acc = elastic_face<PH>(a, acc, c, 2, true, ix, iy, iz);
-    if (ix == 0 && (a.bc[LEFT] == BC_FREE || a.bc[LEFT] == BC_ABSORB)) acc = elastic_face<PH>(a, acc, c, 0, false, ix, iy, iz);
+        acc = elastic_face<PH>(a, acc, c, 2, true, ix, iy, iz, so);
+    if (ix == 0 && (a.bc[LEFT] == BC_FREE || a.bc[LEFT] == BC_ABSORB)) acc = elastic_face<PH>(a, acc, c, 0, false, ix, iy, iz, so);
     if (ix == g.nx - 1 && (a.bc[RIGHT] == BC_FREE || a.bc[RIGHT] == BC_ABSORB))
-        acc = elastic_face<PH>(a, acc, c, 0, true, ix, iy, iz);
-    if (iy == 0 && (a.bc[FRONT] == BC_FREE || a.bc[FRONT] == BC_ABSORB)) acc = elastic_face<PH>(a, acc, c, 1, false, ix, iy, iz);
+        acc = elastic_face<PH>(a, acc, c, 0, true, ix, iy, iz, so);
+    if (iy == 0 && (a.bc[FRONT] == BC_FREE || a.bc[FRONT] == BC_ABSORB)) acc = elastic_face<PH>(a, acc, c, 1, false, ix, iy, iz, so);
     if (iy == g.ny - 1 && (a.bc[BACK] == BC_FREE || a.bc[BACK] == BC_ABSORB))
-        acc = elastic_face<PH>(a, acc, c, 1, true, ix, iy, iz);
+        acc = elastic_face<PH>(a, acc, c, 1, true, ix, iy, iz, so);
     return acc;
 }
 
