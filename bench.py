@@ -134,6 +134,18 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def max_over_ranks(value, world, device=None):
+    """Max of a per-rank scalar over all ranks (the timing rule for N > 1);
+    works with the nccl (device tensor) and gloo (CPU tensor) backends."""
+    if world <= 1:
+        return float(value)
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def cpu_reference(n_steps, threads, n=256):
     """Reference CPU code (oracle/_ref, built from the reference sources): one
     shot of the workload over an n_steps window; returns pt-updates/s."""
@@ -214,9 +226,7 @@ def run_ours(args, rank, world, local):
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
     if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, world, device="cuda")
         torch.distributed.barrier()
     lib.fwi_batch_destroy(h)
 
@@ -240,10 +250,7 @@ def run_ours(args, rank, world, local):
                                          1, we.shape[-1], sv_e.dt_data, ns, _lib.fptr(sx), nr, _lib.fptr(rx),
                                          _lib.fptr(out)))
         te = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([te], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            te = float(t.item())
+        te = max_over_ranks(te, world, device="cuda")
         nsteps_e = we.shape[-1] - 1
         h2d = model.nbytes + we.nbytes + sx.nbytes + rx.nbytes
         e2e = {"value": world * units_per_step * nsteps_e / te, "unit": "pt/s",

@@ -158,6 +158,70 @@ __global__ void __launch_bounds__(fz::NT, MINB) k_elastic_fused(const __grid_con
     }
 }
 
+// SAT penalties of the elastic faces for the planes [a.y0, a.y1) computed by
+// the fused kernel: next += taper(scale(dt^2 sat / rho)), the contribution the
+// reference adds to the operator sum before the update (we_op.cpp:697-804);
+// update, scaling and taper are linear in it.  Each boundary point of the
+// slab is enumerated once: z faces whole, x faces without z edges, y faces
+// (when inside the slab) without x and z edges.
+__device__ __forceinline__ bool face_point(const Dims &g, int y0, int y1, int64_t k, int &ix, int &iy, int &iz)
+{
+    const int ly = y1 - y0;
+    const int64_t nzf = (int64_t)g.nx * ly;          // each z face
+    const int64_t nxf = (int64_t)(g.nz - 2) * ly;    // each x face
+    const int64_t nyf = (int64_t)(g.nx - 2) * (g.nz - 2);
+    if (k < 2 * nzf) {
+        const int side = (int)(k / nzf);
+        const int64_t r = k - side * nzf;
+        iz = side ? g.nz - 1 : 0;
+        ix = (int)(r % g.nx);
+        iy = y0 + (int)(r / g.nx);
+        return true;
+    }
+    k -= 2 * nzf;
+    if (k < 2 * nxf) {
+        const int side = (int)(k / nxf);
+        const int64_t r = k - side * nxf;
+        ix = side ? g.nx - 1 : 0;
+        iz = 1 + (int)(r % (g.nz - 2));
+        iy = y0 + (int)(r / (g.nz - 2));
+        return true;
+    }
+    k -= 2 * nxf;
+    for (int side = 0; side < 2; side++) {
+        const int yy = side ? g.ny - 1 : 0;
+        if (yy < y0 || yy >= y1) continue;
+        if (k < nyf) {
+            iy = yy;
+            iz = 1 + (int)(k % (g.nz - 2));
+            ix = 1 + (int)(k / (g.nz - 2));
+            return true;
+        }
+        k -= nyf;
+    }
+    return false;
+}
+
+template <int PH>
+__global__ void k_elastic_face_sat(const __grid_constant__ StepArgs a, int64_t npts)
+{
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= npts) return;
+    int ix, iy, iz;
+    if (!face_point(a.g, a.y0, a.y1, k, ix, iy, iz)) return;
+    const int64_t so = (int64_t)blockIdx.y * a.sst;
+    const int64_t i = a.g.idx(ix, iy, iz);
+    const float f = a.dt * a.dt / a.m[2][i];
+    for (int c = 0; c < 3; c++) {
+        const float sat = elastic_sat<PH>(a, 0.f, c, ix, iy, iz, so);
+        if (sat == 0.f) continue;
+        float v = f * sat;
+        v = boundary_scale(a, v, c, ix, iy, iz);
+        v = taper(a, v, ix, iy, iz);
+        a.next[c][so + i] += v;
+    }
+}
+
 // Post-injection: next += taper(scale(dt^2 (w s)/rho)) (elastic) or dt^2 (w s) K
 // (acoustic).  Equivalent to the reference's injection into the operator sum
 // before the update (we_op.cpp:691-693): update, scaling and taper are linear in it.
@@ -392,6 +456,7 @@ StepArgs make_step_args(const Problem &pb, const float *m, const float *const sd
     for (int f = 0; f < 6; f++) {
         a.bc[f] = pb.bc[f];
         a.tap[f] = tap[f];
+        a.tw[f] = std::max(0, pb.taper[f]);
         for (int c = 0; c < 3; c++) a.sdiv[f][c] = sdiv[f][c];
     }
     a.scale = scale;
@@ -513,6 +578,12 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
             if (pb_.nmodels == 3) k_elastic_fused<ELASTIC, 1><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch);
             else k_elastic_fused<VTI, 1><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch);
         }
+        // SAT of the x/z faces of the fused planes
+        const int64_t ly = f.y1 - f.y0;
+        const int64_t nf = 2 * (int64_t)pb_.nx * ly + 2 * (int64_t)(pb_.nz - 2) * ly;
+        const dim3 sgrd((unsigned)((nf + 127) / 128), pb_.nshots);
+        if (pb_.nmodels == 3) k_elastic_face_sat<ELASTIC><<<sgrd, 128, 0, s>>>(f, nf);
+        else k_elastic_face_sat<VTI><<<sgrd, 128, 0, s>>>(f, nf);
     }
     CK(cudaGetLastError());
 }
@@ -546,7 +617,7 @@ void Engine::extract(const DevExt &ext, const float *curr, float *rcv_dev, int i
 
 int Engine::launches_per_step() const
 {
-    int k = (pb_.nmodels == 2 ? 1 : (fused_ ? (pb_.ny < 2 * (fz::YPAD + 2) ? 4 : 5) : 2));
+    int k = (pb_.nmodels == 2 ? 1 : (fused_ ? (pb_.ny < 2 * (fz::YPAD + 2) ? 5 : 6) : 2));
     if (ext_.nrec) k += 1;
     for (int c = 0; c < 3; c++) k += inj_.n[c] ? 1 : 0;
     return k;

@@ -77,6 +77,25 @@ struct SX {  // along x at fixed zw
     int stride;
     FWI_HD float operator()(int k) const { return p[(k - off) * stride]; }
 };
+// Window-clamped variants (closure rows of halo positions).
+struct SZc {
+    const float *p;
+    int off, len;
+    FWI_HD float operator()(int k) const
+    {
+        const int j = k - off;
+        return p[j < 0 ? 0 : (j >= len ? len - 1 : j)];
+    }
+};
+struct SXc {
+    const float *p;
+    int off, stride, len;
+    FWI_HD float operator()(int k) const
+    {
+        const int j = k - off;
+        return p[(j < 0 ? 0 : (j >= len ? len - 1 : j)) * stride];
+    }
+};
 
 FWI_HD int ring(int q) { return ((q % fz::NRING) + fz::NRING) % fz::NRING; }
 
@@ -125,29 +144,29 @@ FWI_HD void fz_load_mat(FusedCtx &c, int tid, int y)
     }
 }
 
-// D1 row (unscaled) at global index i of a line; interior rows from smem,
-// closure rows from global memory.
+// D1 row (unscaled) at global index i of a smem line.  Closure rows read
+// samples 0..5 or n-6..n-1, which lie in the window for every position whose
+// value an output row uses; halo positions outside that set are clamped to
+// the window and their (unused) values are meaningless.
 template <class S>
-FWI_HD float d1_sg(const S &s, const Line &gl, int i, int n)
+FWI_HD float d1_sg(const S &s, int i, int n)
 {
-    if (i < 4 || i >= n - 4) return d1_row(gl, i, n);
     const SbpTables &t = sbp();
+    if (i < 4 || i >= n - 4) return d1_row(s, i, n);
     return t.d1c0 * (s(i + 1) - s(i - 1)) + t.d1c1 * (s(i + 2) - s(i - 2));
 }
 
 // First derivatives of displacement component k at (ix, q, iz) along x, y, z
 // from the ring (with the 1/h).  ixw/izw: smem coordinates in the ring window.
-FWI_HD float fz_dx(const FusedCtx &c, int k, int q, int slot, int ix, int iz, int izw)
+FWI_HD float fz_dx(const FusedCtx &c, int k, int slot, int ix, int izw)
 {
-    const Dims &g = c.a->g;
-    const SX s{&c.sm->u[slot][k][0][izw], c.x0 - fz::HW, fz::ZW};
-    return d1_sg(s, g.lx(c.a->curr[k] + c.so, q, iz), ix, g.nx) * c.a->idx;
+    const SXc s{&c.sm->u[slot][k][0][izw], c.x0 - fz::HW, fz::ZW, fz::XW};
+    return d1_sg(s, ix, c.a->g.nx) * c.a->idx;
 }
-FWI_HD float fz_dz(const FusedCtx &c, int k, int q, int slot, int ix, int ixw, int iz)
+FWI_HD float fz_dz(const FusedCtx &c, int k, int slot, int ixw, int iz)
 {
-    const Dims &g = c.a->g;
-    const SZ s{&c.sm->u[slot][k][ixw][0], c.z0 - fz::HW};
-    return d1_sg(s, g.lz(c.a->curr[k] + c.so, ix, q), iz, g.nz) * c.a->idz;
+    const SZc s{&c.sm->u[slot][k][ixw][0], c.z0 - fz::HW, fz::ZW};
+    return d1_sg(s, iz, c.a->g.nz) * c.a->idz;
 }
 // Dy at a plane from the ring slots of its four neighbours: interior rows only
 // (the fused launch keeps every differentiated plane in [6, ny-6)).
@@ -178,13 +197,13 @@ FWI_HD void fz_derived(FusedCtx &c, int tid, int y)
         const int ixw = xh + (fz::HW - fz::HD), izw = zh + (fz::HW - fz::HD);
         const int s0 = c.sl[2];
         const int sn[4] = {c.sl[0], c.sl[1], c.sl[3], c.sl[4]};
-        const float ux0 = fz_dx(c, 0, y, s0, ix, iz, izw);
+        const float ux0 = fz_dx(c, 0, s0, ix, izw);
         const float uy1 = fz_dy(c, 1, sn, ixw, izw);
-        const float uz2 = fz_dz(c, 2, y, s0, ix, ixw, iz);
+        const float uz2 = fz_dz(c, 2, s0, ixw, iz);
         const float mu = c.sm->mp[MP_MU][xh][zh], lam = c.sm->mp[MP_LAM][xh][zh];
         const float uy0 = fz_dy(c, 0, sn, ixw, izw);
-        const float uz0 = fz_dz(c, 0, y, s0, ix, ixw, iz);
-        const float ux2 = fz_dx(c, 2, y, s0, ix, iz, izw);
+        const float uz0 = fz_dz(c, 0, s0, ixw, iz);
+        const float ux2 = fz_dx(c, 2, s0, ix, izw);
         const float uy2 = fz_dy(c, 2, sn, ixw, izw);
         if (PH == ELASTIC) {
             const float T = lam * (ux0 + uy1 + uz2);
@@ -232,11 +251,11 @@ FWI_HD void fz_column(FusedCtx &c, FusedThread &th, int tid, int q)
     // plane q = y+2 sits in slot sl[4]; its neighbours q-2..q+2 in sl[2..6]
     const int s0 = c.sl[4];
     const int sn[4] = {c.sl[2], c.sl[3], c.sl[5], c.sl[6]};
-    const float ux0 = fz_dx(c, 0, q, s0, ix, iz, izw);
+    const float ux0 = fz_dx(c, 0, s0, ix, izw);
     const float uy1 = fz_dy(c, 1, sn, ixw, izw);
-    const float uz2 = fz_dz(c, 2, q, s0, ix, ixw, iz);
-    const float ux1 = fz_dx(c, 1, q, s0, ix, iz, izw);
-    const float uz1 = fz_dz(c, 1, q, s0, ix, ixw, iz);
+    const float uz2 = fz_dz(c, 2, s0, ixw, iz);
+    const float ux1 = fz_dx(c, 1, s0, ix, izw);
+    const float uz1 = fz_dz(c, 1, s0, ixw, iz);
     if (PH == ELASTIC) {
         th.qT[4] = lam * (ux0 + uy1 + uz2);
         th.qX1[4] = ux1;
@@ -287,6 +306,36 @@ FWI_HD float d1m(float am2, float mm2, float am1, float mm1, float ap1, float mp
     return t.d1c0 * (ap1 * mp1 - am1 * mm1) + t.d1c1 * (ap2 * mp2 - am2 * mm2);
 }
 
+// D2var closure row: the 8 weights sum_k B[r][j][k] f(k) of the row, then
+// applied to the field (spatial_operators.hpp:58-81).
+struct W8 {
+    float w[8];
+};
+template <class F>
+FWI_HD W8 d2closure_weights(const F &f, int i, int n)
+{
+    const SbpTables &t = sbp();
+    const bool hi = i >= n - 6;
+    const int r = hi ? n - 1 - i : i;
+    float fk[8];
+    for (int k = 0; k < 8; k++) fk[k] = f(hi ? n - 1 - k : k);
+    W8 w;
+    for (int j = 0; j < 8; j++) {
+        float v = 0.f;
+        for (int k = 0; k < 8; k++) v += t.d2b[r][j][k] * fk[k];
+        w.w[j] = v;
+    }
+    return w;
+}
+template <class U>
+FWI_HD float d2closure_apply(const W8 &w, const U &u, int i, int n, float ad2)
+{
+    const bool hi = i >= n - 6;
+    float acc = 0.f;
+    for (int j = 0; j < 8; j++) acc += ad2 * w.w[j] * u(hi ? n - 1 - j : j);
+    return acc;
+}
+
 // Smem accessors of the output phase.
 FWI_HD SX ux_line(const FusedCtx &c, int slot, int k, int izw) { return SX{&c.sm->u[slot][k][0][izw], c.x0 - fz::HW, fz::ZW}; }
 FWI_HD SZ uz_line(const FusedCtx &c, int slot, int k, int ixw) { return SZ{&c.sm->u[slot][k][ixw][0], c.z0 - fz::HW}; }
@@ -323,9 +372,13 @@ FWI_HD void fz_output(FusedCtx &c, const FusedThread &th, int tid, int y)
     const SX mux = mx_line(c, MP_MU, zh);
     const SZ muz = mz_line(c, MP_MU, xh);
     if (PH == ELASTIC) {
+        // one set of weights per axis serves the three components (all use mu)
         W5 wx{}, wz{};
+        W8 wxc{}, wzc{};
         if (xin) wx = d2w(mux(ix - 2), mux(ix - 1), mux(ix), mux(ix + 1), mux(ix + 2));
+        else wxc = d2closure_weights(mux, ix, g.nx);
         if (zin) wz = d2w(muz(iz - 2), muz(iz - 1), muz(iz), muz(iz + 1), muz(iz + 2));
+        else wzc = d2closure_weights(muz, iz, g.nz);
         const W5 wy = d2w(th.qmu[0], th.qmu[1], th.qmu[2], th.qmu[3], th.qmu[4]);
         for (int k = 0; k < 3; k++) {
             const float adx = k == 0 ? a.ad2[0] : a.ad1[0];
@@ -334,11 +387,11 @@ FWI_HD void fz_output(FusedCtx &c, const FusedThread &th, int tid, int y)
             const SX ul = ux_line(c, r0, k, izw);
             const SZ uzl = uz_line(c, r0, k, ixw);
             float v = xin ? d2apply(wx, adx, ul(ix - 2), ul(ix - 1), ul(ix), ul(ix + 1), ul(ix + 2))
-                          : d2var_row(ul, mux, ix, g.nx, adx);
+                          : d2closure_apply(wxc, ul, ix, g.nx, adx);
             v += d2apply(wy, ady, s.u[rm2][k][ixw][izw], s.u[rm1][k][ixw][izw], s.u[r0][k][ixw][izw],
                          s.u[rp1][k][ixw][izw], s.u[rp2][k][ixw][izw]);
             v += zin ? d2apply(wz, adz, uzl(iz - 2), uzl(iz - 1), uzl(iz), uzl(iz + 1), uzl(iz + 2))
-                     : d2var_row(uzl, muz, iz, g.nz, adz);
+                     : d2closure_apply(wzc, uzl, iz, g.nz, adz);
             acc[k] = v;
         }
     } else {
@@ -392,14 +445,11 @@ FWI_HD void fz_output(FusedCtx &c, const FusedThread &th, int tid, int y)
     acc[2] += d1_prod_row(dx_line(c, DV_Z0, zh), mux, ix, g.nx) * a.idx;
     acc[2] += d1m(th.qZ1[0], th.qmu[0], th.qZ1[1], th.qmu[1], th.qZ1[3], th.qmu[3], th.qZ1[4], th.qmu[4]) * a.idy;
 
-    // ---- SAT on x/z faces, update, scaling, taper ----
+    // ---- update, scaling, taper (SAT is added by the face kernel) ----
     const float dt2 = a.dt * a.dt;
     const float rho = a.m[2][i];
     const bool face = ix == 0 || ix == g.nx - 1 || iz == 0 || iz == g.nz - 1;
-    const bool tz = a.tap[0][iz] != 1.f || a.tap[1][iz] != 1.f || a.tap[2][ix] != 1.f || a.tap[3][ix] != 1.f ||
-                    a.tap[4][y] != 1.f || a.tap[5][y] != 1.f;
-    if (face)
-        for (int k = 0; k < 3; k++) acc[k] = elastic_sat<PH>(a, acc[k], k, ix, y, iz, c.so);
+    const bool tz = in_taper(a, ix, y, iz);
     const float irho = 1.0f / rho;
     for (int k = 0; k < 3; k++) {
         float v = acc[k];

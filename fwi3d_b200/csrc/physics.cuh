@@ -48,6 +48,7 @@ struct StepArgs {
     const float *sdiv[6][3];   // absorbing-boundary divisors (1+scaler) on the owning face, per component
     int scale;                 // any face absorbing
     const float *tap[6];       // taper factors tz_lo[nz], tz_hi[nz], tx_lo[nx], tx_hi[nx], ty_lo[ny], ty_hi[ny]
+    int tw[6];                 // taper widths top, bottom, left, right, front, back
     int taper_prev;
     // batch layout: shot s of a field component c lives at curr[c] + s*sst
     int nyb;                   // y blocks per shot in the launch grid
@@ -73,6 +74,14 @@ FWI_HD StepArgs shot_args(const StepArgs &a, int s)
 // ---------------------------------------------------------------------------
 // Taper and absorbing-boundary scaling
 // ---------------------------------------------------------------------------
+// True where any taper factor differs from one (the reference tapers the
+// first taper_top rows from the top, the last taper_bottom rows, etc.).
+FWI_HD bool in_taper(const StepArgs &a, int ix, int iy, int iz)
+{
+    return iz < a.tw[0] || iz >= a.g.nz - a.tw[1] || ix < a.tw[2] || ix >= a.g.nx - a.tw[3] || iy < a.tw[4] ||
+           iy >= a.g.ny - a.tw[5];
+}
+
 FWI_HD float taper(const StepArgs &a, float v, int ix, int iy, int iz)
 {
     v = v * a.tap[0][iz];
