@@ -160,13 +160,26 @@ FWI_HD float d1_sg(const S &s, int i, int n)
 // from the ring (with the 1/h).  ixw/izw: smem coordinates in the ring window.
 FWI_HD float fz_dx(const FusedCtx &c, int k, int slot, int ix, int izw)
 {
-    const SXc s{&c.sm->u[slot][k][0][izw], c.x0 - fz::HW, fz::ZW, fz::XW};
-    return d1_sg(s, ix, c.a->g.nx) * c.a->idx;
+    const float *p = &c.sm->u[slot][k][0][izw];
+    const int j = ix - (c.x0 - fz::HW);
+    if (ix >= 4 && ix < c.a->g.nx - 4) {
+        const SbpTables &t = sbp();
+        return (t.d1c0 * (p[(j + 1) * fz::ZW] - p[(j - 1) * fz::ZW]) + t.d1c1 * (p[(j + 2) * fz::ZW] - p[(j - 2) * fz::ZW])) *
+               c.a->idx;
+    }
+    const SXc s{p, c.x0 - fz::HW, fz::ZW, fz::XW};
+    return d1_row(s, ix, c.a->g.nx) * c.a->idx;
 }
 FWI_HD float fz_dz(const FusedCtx &c, int k, int slot, int ixw, int iz)
 {
-    const SZc s{&c.sm->u[slot][k][ixw][0], c.z0 - fz::HW, fz::ZW};
-    return d1_sg(s, iz, c.a->g.nz) * c.a->idz;
+    const float *p = &c.sm->u[slot][k][ixw][0];
+    const int j = iz - (c.z0 - fz::HW);
+    if (iz >= 4 && iz < c.a->g.nz - 4) {
+        const SbpTables &t = sbp();
+        return (t.d1c0 * (p[j + 1] - p[j - 1]) + t.d1c1 * (p[j + 2] - p[j - 2])) * c.a->idz;
+    }
+    const SZc s{p, c.z0 - fz::HW, fz::ZW};
+    return d1_row(s, iz, c.a->g.nz) * c.a->idz;
 }
 // Dy at a plane from the ring slots of its four neighbours: interior rows only
 // (the fused launch keeps every differentiated plane in [6, ny-6)).
