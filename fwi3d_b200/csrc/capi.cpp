@@ -500,4 +500,11 @@ int fwi_forward_batch(int device, const fwi_grid *grid, int nmodels, const fwi_p
     return rc;
 }
 
+int fwi_elastic_step_static(const fwi_grid *grid, int nmodels, const int *bc, float dt, const float *model,
+                            const float *prev, const float *curr, float *next, void *stream)
+{
+    if (!grid || !bc || !model || !prev || !curr || !next) return fail(FWI_ERR_ARG, "null argument");
+    return guarded([&] { fwi::static_elastic_step(*grid, nmodels, bc, dt, model, prev, curr, next, stream); });
+}
+
 }  // extern "C"

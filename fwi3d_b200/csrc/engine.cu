@@ -13,6 +13,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
+#include <string>
 
 #include "engine.h"
 #include "imaging.cuh"
@@ -769,6 +771,160 @@ void Engine::adjoint(const InjTable &inj, int ntrace, const float *adj_src, floa
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(grad, gf.p, gf.bytes, cudaMemcpyDeviceToHost, s));
     sync();
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free elastic step on caller-owned buffers (fwi_elastic_step_static)
+// ---------------------------------------------------------------------------
+// The first-derivative scratch of this entry point is the file-scope array
+// below: kStaticMaxPoints grid points x 9 derivative fields = 9 MiB.  Nothing
+// in it needs to start at zero, because k_elastic_aux writes every point that
+// k_elastic_step reads in the same call.  All calls on one device share it,
+// so calls that overlap in time on one device (two streams, two host threads)
+// race on it; the caller serialises them.  The per-point step kernel always
+// multiplies by the six taper tables; a taper-free step points all six at a
+// second static array of ones, written once at set-up.
+namespace {
+constexpr int64_t kStaticMaxPoints = int64_t(1) << 18;  // 262,144 points, e.g. 64^3
+constexpr int kStaticMaxAxis = 2048;                    // >= 2^18 / (12 * 12)
+constexpr int kStaticMaxDevices = 64;
+}  // namespace
+
+static __device__ __align__(256) float g_static_aux[9 * kStaticMaxPoints];
+static __device__ __align__(256) float g_static_ones[kStaticMaxAxis];
+
+namespace {
+__global__ void k_static_fill_ones()
+{
+    for (int i = threadIdx.x; i < kStaticMaxAxis; i += blockDim.x) g_static_ones[i] = 1.f;
+}
+
+struct StaticScratch {
+    float *aux = nullptr;   // device address of g_static_aux
+    float *ones = nullptr;  // device address of g_static_ones
+};
+std::mutex g_static_mu;
+StaticScratch g_static[kStaticMaxDevices];
+
+// Set-up, once per device with that device current: resolve the scratch
+// addresses, fill the table of ones and load the SBP coefficient tables into
+// constant memory.  These are synchronous runtime calls, so the first call on
+// a device belongs before any stream capture on it.
+StaticScratch static_scratch(int dev)
+{
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    StaticScratch &st = g_static[dev];
+    if (!st.aux) {
+        float *aux = nullptr, *ones = nullptr;
+        cudaError_t e = cudaGetSymbolAddress((void **)&aux, g_static_aux);
+        if (e == cudaSuccess) e = cudaGetSymbolAddress((void **)&ones, g_static_ones);
+        if (e != cudaSuccess || !aux || !ones)
+            throw FwiError(FWI_ERR_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
+        init_sbp_tables();
+        CK(cudaMemcpyToSymbol(c_sbp, &g_sbp_host, sizeof(SbpTables)));
+        k_static_fill_ones<<<1, 256, 0, 0>>>();
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(0));
+        st.ones = ones;
+        st.aux = aux;
+    }
+    return st;
+}
+
+void require_device_ptr(const void *p, int dev, const char *name)
+{
+    cudaPointerAttributes at;
+    CK(cudaPointerGetAttributes(&at, p));
+    if ((at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) || at.device != dev)
+        throw FwiError(FWI_ERR_ARG, std::string(name) + " is not device memory of the current device");
+}
+}  // namespace
+
+void static_elastic_step(const fwi_grid &grid, int nmodels, const int bc[6], float dt, const float *model,
+                         const float *prev, const float *curr, float *next, void *stream)
+{
+    if (nmodels != 3 && nmodels != 6) throw FwiError(FWI_ERR_ARG, "nmodels must be 3 (elastic) or 6 (VTI)");
+    if (grid.nx < 12 || grid.ny < 12 || grid.nz < 12)
+        throw FwiError(FWI_ERR_ARG, "each grid axis needs at least 12 points (two 6-row SBP closures)");
+    const int64_t n = (int64_t)grid.nx * grid.ny * grid.nz;
+    if (n > kStaticMaxPoints)
+        throw FwiError(FWI_ERR_ARG, "grid of " + std::to_string(n) + " points exceeds the static scratch limit of " +
+                                        std::to_string(kStaticMaxPoints) + " points");
+    if (std::max(grid.nx, std::max(grid.ny, grid.nz)) > kStaticMaxAxis)
+        throw FwiError(FWI_ERR_ARG, "a grid axis exceeds " + std::to_string(kStaticMaxAxis) + " points");
+    if (!(grid.dx > 0 && grid.dy > 0 && grid.dz > 0 && dt > 0)) throw FwiError(FWI_ERR_ARG, "spacings and dt must be > 0");
+    for (int f = 0; f < 6; f++)
+        if (bc[f] != BC_NONE && bc[f] != BC_FREE)
+            throw FwiError(FWI_ERR_UNSUPPORTED,
+                           "only bc 0 (none) and 1 (traction-free) faces: absorbing and rigid faces need the "
+                           "model-dependent boundary tables that the operator and batch paths build");
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) throw FwiError(FWI_ERR_NOGPU, "no CUDA device");
+    if (dev >= kStaticMaxDevices) throw FwiError(FWI_ERR_ARG, "device ordinal above the static set-up table");
+    require_device_ptr(model, dev, "model");
+    require_device_ptr(prev, dev, "prev");
+    require_device_ptr(curr, dev, "curr");
+    require_device_ptr(next, dev, "next");
+    const StaticScratch st = static_scratch(dev);
+    float *scr = st.aux;
+
+    Problem pb{};
+    pb.nmodels = nmodels;
+    pb.nx = grid.nx;
+    pb.ny = grid.ny;
+    pb.nz = grid.nz;
+    pb.dx = grid.dx;
+    pb.dy = grid.dy;
+    pb.dz = grid.dz;
+    pb.dt = dt;
+    pb.nt = 2;
+    pb.sub = 0;
+    for (int f = 0; f < 6; f++) {
+        pb.bc[f] = bc[f];
+        pb.taper[f] = 0;
+    }
+    pb.taper_strength = 0.f;
+    pb.free_surface_stiffness = 1.f;
+    pb.nshots = 1;
+    const float *no_sdiv[6][3] = {};  // read only when a face is absorbing
+    const float *ones[6] = {st.ones, st.ones, st.ones, st.ones, st.ones, st.ones};
+    StepArgs a = make_step_args(pb, model, no_sdiv, ones, 0);
+    AuxArgs x;
+    std::memset(&x, 0, sizeof(x));
+    x.g = a.g;
+    x.dx = pb.dx;
+    x.dy = pb.dy;
+    x.dz = pb.dz;
+    for (int k = 0; k < nmodels; k++) x.m[k] = a.m[k];
+    for (int c = 0; c < 3; c++) {
+        a.curr[c] = x.curr[c] = curr + c * n;
+        a.prev[c] = prev + c * n;
+        a.next[c] = next + c * n;
+    }
+    a.taper_prev = 0;
+    // scratch layout as the engine's: elastic shares one divergence slot for T0..T2
+    if (nmodels == 3) {
+        x.aux[AUX_T0] = x.aux[AUX_T1] = x.aux[AUX_T2] = scr;
+        for (int k = 3; k < 9; k++) x.aux[k] = scr + (k - 2) * n;
+    } else {
+        for (int k = 0; k < 9; k++) x.aux[k] = scr + k * n;
+    }
+    for (int k = 0; k < 9; k++) a.aux[k] = x.aux[k];
+    a.y0 = x.y0 = 0;
+    a.y1 = x.y1 = pb.ny;
+    a.nyb = x.nyb = yblocks(pb.ny);
+    x.sst = a.sst;
+    x.ast = a.ast;
+    cudaStream_t s = (cudaStream_t)stream;
+    const dim3 blk(BZ, BX, BY), grd = grid_of(a.g, 1, pb.ny);
+    if (nmodels == 3) {
+        k_elastic_aux<ELASTIC><<<grd, blk, 0, s>>>(x);
+        k_elastic_step<ELASTIC><<<grd, blk, 0, s>>>(a);
+    } else {
+        k_elastic_aux<VTI><<<grd, blk, 0, s>>>(x);
+        k_elastic_step<VTI><<<grd, blk, 0, s>>>(a);
+    }
+    CK(cudaGetLastError());
 }
 
 }  // namespace fwi

@@ -130,4 +130,11 @@ private:
     DevExt ext_;
 };
 
+// One elastic (nmodels 3) or VTI (6) leapfrog step next = F(prev, curr) on
+// caller-owned device buffers of the current device, with the derivative
+// scratch in a static device array: no device or host allocation.  Faces bc 0
+// or 1 only, no taper, at most 2^18 grid points (fwi_elastic_step_static).
+void static_elastic_step(const fwi_grid &grid, int nmodels, const int bc[6], float dt, const float *model,
+                         const float *prev, const float *curr, float *next, void *stream);
+
 }  // namespace fwi

@@ -130,6 +130,27 @@ int fwi_batch_traces(fwi_batch *b, float *data);
 int fwi_batch_get_info(const fwi_batch *b, fwi_op_info *info, int *launches_per_step);
 void fwi_batch_destroy(fwi_batch *b);
 
+/* One elastic (nmodels 3) or VTI (nmodels 6) leapfrog step on caller-owned
+ * device buffers that allocates nothing, device or host.  No counterpart in
+ * the reference: there the step lives inside nl_we_op_*::propagate
+ * (src/cpp/we_op.cpp:623-836) on arrays the operator allocates itself.  For
+ * callers whose device memory is owned by another allocator (a PyTorch
+ * caching allocator, a serving loop that has budgeted all HBM to admitted
+ * requests): the library's own paths cudaMalloc and cudaFree, and cudaFree
+ * synchronises the whole device.
+ *   model: converted [nmodels][ny][nx][nz] (lambda, mu, rho[, c13, eps, c66]);
+ *   prev, curr (read), next (written at every point): [3][ny][nx][nz];
+ *   all on the current device; stream: a cudaStream_t (0: legacy default).
+ * Limits: at most 262,144 grid points (the static scratch is 9 x 2^18 floats,
+ * 9 MiB, reserved with the library's device code when that loads), each axis >= 12, bc[6] each 0 (none) or 1 (traction-free), no taper
+ * (FWI_ERR_ARG / FWI_ERR_UNSUPPORTED otherwise).  Nothing needs to start at
+ * zero.  The first call on a device does a one-time synchronous set-up
+ * (scratch address, coefficient tables): make it before any stream capture.
+ * All calls on a device share the one scratch array, so calls that overlap
+ * in time (other streams, other threads) race: serialise them. */
+int fwi_elastic_step_static(const fwi_grid *grid, int nmodels, const int *bc, float dt, const float *model,
+                            const float *prev, const float *curr, float *next, void *stream);
+
 /* Message of the last failing call on this thread. */
 const char *fwi_last_error(void);
 
