@@ -27,7 +27,8 @@ EXPORTS = [
     "fwi_param_default", "fwi_op_create", "fwi_op_forward", "fwi_op_jacobianT", "fwi_op_get_info",
     "fwi_op_destroy", "fwi_forward_batch", "fwi_batch_create", "fwi_batch_reset", "fwi_batch_run",
     "fwi_batch_sync", "fwi_batch_stream", "fwi_batch_traces", "fwi_batch_get_info", "fwi_batch_destroy",
-    "fwi_last_error", "fwi_version", "fwi_elastic_step_static",
+    "fwi_last_error", "fwi_version", "fwi_elastic_step_static", "fwi_batch_time_main_kernel",
+    "fwi_batch_main_kernel_time",
 ]
 
 
@@ -113,6 +114,11 @@ def load() -> C.CDLL:
     lib.fwi_elastic_step_static.argtypes = [C.POINTER(Grid), C.c_int, C.POINTER(C.c_int), C.c_float, vp, vp, vp,
                                             vp, vp]
     lib.fwi_elastic_step_static.restype = C.c_int
+    lib.fwi_batch_time_main_kernel.argtypes = [vp, C.c_int]
+    lib.fwi_batch_time_main_kernel.restype = C.c_int
+    lib.fwi_batch_main_kernel_time.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_int64),
+                                               C.POINTER(C.c_char_p)]
+    lib.fwi_batch_main_kernel_time.restype = C.c_int
     lib.fwi_last_error.restype = C.c_char_p
     lib.fwi_version.restype = C.c_char_p
     _lib = lib

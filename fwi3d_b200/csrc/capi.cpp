@@ -500,6 +500,18 @@ int fwi_forward_batch(int device, const fwi_grid *grid, int nmodels, const fwi_p
     return rc;
 }
 
+int fwi_batch_time_main_kernel(fwi_batch *b, int max_launches)
+{
+    if (!b || max_launches < 0) return fail(FWI_ERR_ARG, "bad argument");
+    return guarded([&] { b->eng->time_main_kernel(max_launches); });
+}
+
+int fwi_batch_main_kernel_time(fwi_batch *b, double *ms, int *launches, int64_t *points, const char **name)
+{
+    if (!b || !ms) return fail(FWI_ERR_ARG, "null argument");
+    return guarded([&] { *ms = b->eng->main_kernel_ms(launches, points, name); });
+}
+
 int fwi_elastic_step_static(const fwi_grid *grid, int nmodels, const int *bc, float dt, const float *model,
                             const float *prev, const float *curr, float *next, void *stream)
 {

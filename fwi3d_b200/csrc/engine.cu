@@ -357,6 +357,7 @@ Engine::~Engine()
         cudaStreamSynchronize((cudaStream_t)stream_);
         cudaStreamDestroy((cudaStream_t)stream_);
     }
+    for (void *e : kev_) cudaEventDestroy((cudaEvent_t)e);
 }
 
 void Engine::sync() { CK(cudaStreamSynchronize((cudaStream_t)stream_)); }
@@ -512,7 +513,10 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         return grid_of(g, pb_.nshots, y1 - y0);
     };
     if (pb_.nmodels == 2) {
-        k_acoustic_step<<<range(a, 0, pb_.ny), blk, 0, s>>>(a);
+        const dim3 grd = range(a, 0, pb_.ny);
+        kmark(true, "k_acoustic_step", n * pb_.nshots);
+        k_acoustic_step<<<grd, blk, 0, s>>>(a);
+        kmark(false, nullptr, 0);
         CK(cudaGetLastError());
         return;
     }
@@ -551,7 +555,9 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
     const int P = fz::YPAD;
     if (!fused_) {
         aux_range(0, pb_.ny);
+        kmark(true, "k_elastic_step", n * pb_.nshots);
         step_range(0, pb_.ny);
+        kmark(false, nullptr, 0);
     } else {
         // planes near the y walls: per-point kernels (derivative scratch two planes deeper)
         if (pb_.ny < 2 * (P + 2)) {
@@ -573,6 +579,7 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         int nch = (target + tiles - 1) / tiles;
         nch = std::max(1, std::min(nch, (f.y1 - f.y0) / 16));
         const dim3 grd(kz, kx, nch * pb_.nshots), fblk(fz::TZ, fz::TX);
+        kmark(true, "k_elastic_fused", (int64_t)(f.y1 - f.y0) * pb_.nx * pb_.nz * pb_.nshots);
         if (fused_minb_ == 2) {
             if (pb_.nmodels == 3) k_elastic_fused<ELASTIC, 2><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch);
             else k_elastic_fused<VTI, 2><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch);
@@ -580,6 +587,7 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
             if (pb_.nmodels == 3) k_elastic_fused<ELASTIC, 1><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch);
             else k_elastic_fused<VTI, 1><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch);
         }
+        kmark(false, nullptr, 0);
         // SAT of the x/z faces of the fused planes
         const int64_t ly = f.y1 - f.y0;
         const int64_t nf = 2 * (int64_t)pb_.nx * ly + 2 * (int64_t)(pb_.nz - 2) * ly;
@@ -615,6 +623,49 @@ void Engine::extract(const DevExt &ext, const float *curr, float *rcv_dev, int i
     k_extract<<<grd, 128, 0, s>>>(curr, (int64_t)nc * n, n, nc, ext.gidx.as<int64_t>(), ext.w.as<float>(), ext.nrec,
                                   ext.nr, rcv_dev, pb_.nt, it);
     CK(cudaGetLastError());
+}
+
+void Engine::kmark(bool begin, const char *name, int64_t pts)
+{
+    if (!ktime_ || kev_used_ >= (int)kev_.size() / 2) return;
+    cudaEvent_t e = (cudaEvent_t)kev_[2 * kev_used_ + (begin ? 0 : 1)];
+    CK(cudaEventRecord(e, (cudaStream_t)stream_));
+    if (begin) {
+        kname_ = name;
+        kpts_ = pts;
+    } else {
+        kev_used_++;
+    }
+}
+
+void Engine::time_main_kernel(int max_launches)
+{
+    CK(cudaSetDevice(device_));
+    sync();
+    for (void *e : kev_) cudaEventDestroy((cudaEvent_t)e);
+    kev_.clear();
+    kev_used_ = 0;
+    ktime_ = max_launches > 0;
+    for (int k = 0; k < 2 * std::max(0, max_launches); k++) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        kev_.push_back(e);
+    }
+}
+
+double Engine::main_kernel_ms(int *launches, int64_t *points, const char **name)
+{
+    sync();
+    double ms = 0;
+    for (int k = 0; k < kev_used_; k++) {
+        float t = 0;
+        CK(cudaEventElapsedTime(&t, (cudaEvent_t)kev_[2 * k], (cudaEvent_t)kev_[2 * k + 1]));
+        ms += t;
+    }
+    if (launches) *launches = kev_used_;
+    if (points) *points = kpts_;
+    if (name) *name = kname_;
+    return ms;
 }
 
 int Engine::launches_per_step() const

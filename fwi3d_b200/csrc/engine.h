@@ -94,6 +94,14 @@ public:
     // adjoint + imaging; grad out: [min(3,nm)][nxyz] float (before H quadrature and chain rule)
     void adjoint(const InjTable &inj, int ntrace, const float *adj_src, float *grad);
 
+    // Diagnostic timing of the step's main kernel (the fused interior kernel,
+    // else the per-point step kernel): a pair of CUDA events on the engine
+    // stream around each of its launches, up to max_launches (0: off).
+    void time_main_kernel(int max_launches);
+    // Summed event time since time_main_kernel(); launches timed, grid-point
+    // updates per launch and the kernel's name.  Synchronises the stream.
+    double main_kernel_ms(int *launches, int64_t *points, const char **name);
+
     bool has_snapshots() const { return snaps_valid_; }
     int64_t device_bytes() const;
     void sync();
@@ -126,6 +134,12 @@ private:
     bool fused_ = false;           // fused elastic kernel for the interior planes
     int fused_minb_ = 1;           // resident CTAs per SM the fused kernel is compiled for
     DevBuf src_dev_, rcv_dev_;
+    std::vector<void *> kev_;      // event pairs (begin, end) of the timed main-kernel launches
+    int kev_used_ = 0;
+    bool ktime_ = false;
+    const char *kname_ = "";
+    int64_t kpts_ = 0;
+    void kmark(bool begin, const char *name, int64_t pts);
     DevInj inj_;
     DevExt ext_;
 };

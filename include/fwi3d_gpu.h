@@ -128,6 +128,13 @@ int fwi_batch_stream(fwi_batch *b, void **stream);
 /* Data [nshots][nrcomp][nr][nt_data] after the full time axis was run. */
 int fwi_batch_traces(fwi_batch *b, float *data);
 int fwi_batch_get_info(const fwi_batch *b, fwi_op_info *info, int *launches_per_step);
+/* Diagnostics (no counterpart in the reference): time each launch of the
+ * step's main kernel with a pair of CUDA events on the session stream, for up
+ * to max_launches launches (0: off); read back the summed time, the number of
+ * launches timed, the grid-point updates one launch performs and the kernel
+ * name.  The read-back synchronises the session stream. */
+int fwi_batch_time_main_kernel(fwi_batch *b, int max_launches);
+int fwi_batch_main_kernel_time(fwi_batch *b, double *ms, int *launches, int64_t *points, const char **name);
 void fwi_batch_destroy(fwi_batch *b);
 
 /* One elastic (nmodels 3) or VTI (nmodels 6) leapfrog step on caller-owned
