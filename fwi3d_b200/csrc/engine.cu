@@ -19,6 +19,7 @@
 #include "engine.h"
 #include "imaging.cuh"
 #include "fused.cuh"
+#include "march.cuh"
 #include "physics.cuh"
 
 namespace fwi {
@@ -158,6 +159,40 @@ __global__ void __launch_bounds__(fz::NT, MINB) k_elastic_fused(const __grid_con
         if (y >= ya) fz_output<PH>(c, th, tid, y);
         __syncthreads();
     }
+}
+
+// Marching elastic step over every plane (see march.cuh).  grid: (z tiles,
+// x tiles, y chunks x shots), block (TZ, TX), one CTA per SM.
+template <int PH, bool XF, bool ZF>
+__device__ __forceinline__ void march_tile(const MarchCtx &c, int ya, int yb, int tid)
+{
+    m3_march<PH, XF, ZF>(c, ya, yb, [&](auto &&phase) {
+        phase(tid);
+        __syncthreads();
+    });
+}
+
+template <int PH>
+__global__ void __launch_bounds__(f3::NT, 1) k_elastic_march(const __grid_constant__ StepArgs a, int nchunks)
+{
+    extern __shared__ __align__(16) unsigned char m3_smem[];
+    MarchCtx c;
+    c.a = &a;
+    c.sm = reinterpret_cast<MarchSmem *>(m3_smem);
+    const int tid = threadIdx.x + f3::TZ * threadIdx.y;
+    const int shot = blockIdx.z / nchunks;
+    const int ch = blockIdx.z - shot * nchunks;
+    c.so = shot * a.sst;
+    tile_range(blockIdx.x, a.g.nz, f3::TZ, c.z0, c.zend);
+    tile_range(blockIdx.y, a.g.nx, f3::TX, c.x0, c.xend);
+    int ya, yb;
+    m3_chunk(a.g.ny, ch, nchunks, ya, yb);
+    if (ya >= yb) return;
+    const bool xf = m3_fast(c.x0, a.g.nx, f3::TX), zf = m3_fast(c.z0, a.g.nz, f3::TZ);
+    if (xf && zf) march_tile<PH, true, true>(c, ya, yb, tid);
+    else if (xf) march_tile<PH, true, false>(c, ya, yb, tid);
+    else if (zf) march_tile<PH, false, true>(c, ya, yb, tid);
+    else march_tile<PH, false, false>(c, ya, yb, tid);
 }
 
 // SAT penalties of the elastic faces for the planes [a.y0, a.y1) computed by
@@ -329,11 +364,23 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     const int64_t n = pb.nxyz();
     const int nc = pb.ncomp();
     fields_.alloc(sizeof(float) * 3 * (size_t)pb.nshots * nc * n);
-    if (pb.nmodels != 2) aux_.alloc(sizeof(float) * (size_t)pb.nshots * (pb.nmodels == 6 ? 9 : 7) * n);
+    // Marching kernel over all planes (FWI_MARCH=1, where its tiling applies);
+    // otherwise the interior fused kernel plus per-point kernels at the y walls.
+    const char *menv = std::getenv("FWI_MARCH");
+    march_ = pb.nmodels != 2 && (menv && menv[0] == '1') && pb.nx >= f3::TX + 6 && pb.nz >= f3::TZ + 6 &&
+             pb.ny >= 12;
+    if (pb.nmodels != 2 && !march_)
+        aux_.alloc(sizeof(float) * (size_t)pb.nshots * (pb.nmodels == 6 ? 9 : 7) * n);
+    if (march_) {
+        CK(cudaFuncSetAttribute(k_elastic_march<ELASTIC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(MarchSmem)));
+        CK(cudaFuncSetAttribute(k_elastic_march<VTI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(MarchSmem)));
+    }
     const char *env = std::getenv("FWI_FUSED");
     // The tiling keeps every SBP closure row in the first or the last tile only
     // when each axis is at least one tile plus the 6 closure rows long.
-    fused_ = pb.nmodels != 2 && !(env && env[0] == '0') && pb.nx >= fz::TX + 6 && pb.nz >= fz::TZ + 6 &&
+    fused_ = !march_ && pb.nmodels != 2 && !(env && env[0] == '0') && pb.nx >= fz::TX + 6 && pb.nz >= fz::TZ + 6 &&
              pb.ny > 2 * fz::YPAD;
     // Occupancy variant of the fused kernel: 1 CTA per SM with up to 128
     // registers (default) or 2 CTAs per SM with 64 registers.
@@ -520,6 +567,29 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         CK(cudaGetLastError());
         return;
     }
+    if (march_) {
+        const int kz = (pb_.nz + f3::TZ - 1) / f3::TZ, kx = (pb_.nx + f3::TX - 1) / f3::TX;
+        const int tiles = kz * kx * pb_.nshots;
+        const int target = 148 * 3;  // about three waves of resident CTAs
+        int nch = (target + tiles - 1) / tiles;
+        nch = std::max(1, std::min(nch, (pb_.ny - 12) / 24));
+        const dim3 grd(kz, kx, nch * pb_.nshots), mblk(f3::TZ, f3::TX);
+        kmark(true, "k_elastic_march", n * pb_.nshots);
+        if (pb_.nmodels == 3) k_elastic_march<ELASTIC><<<grd, mblk, sizeof(MarchSmem), s>>>(a, nch);
+        else k_elastic_march<VTI><<<grd, mblk, sizeof(MarchSmem), s>>>(a, nch);
+        kmark(false, nullptr, 0);
+        // SAT of every face point
+        const int64_t nf = 2 * (int64_t)pb_.nx * pb_.ny + 2 * (int64_t)(pb_.nz - 2) * pb_.ny +
+                           2 * (int64_t)(pb_.nx - 2) * (pb_.nz - 2);
+        StepArgs f = a;
+        f.y0 = 0;
+        f.y1 = pb_.ny;
+        const dim3 sgrd((unsigned)((nf + 127) / 128), pb_.nshots);
+        if (pb_.nmodels == 3) k_elastic_face_sat<ELASTIC><<<sgrd, 128, 0, s>>>(f, nf);
+        else k_elastic_face_sat<VTI><<<sgrd, 128, 0, s>>>(f, nf);
+        CK(cudaGetLastError());
+        return;
+    }
     AuxArgs x;
     std::memset(&x, 0, sizeof(x));
     x.g = g;
@@ -670,7 +740,7 @@ double Engine::main_kernel_ms(int *launches, int64_t *points, const char **name)
 
 int Engine::launches_per_step() const
 {
-    int k = (pb_.nmodels == 2 ? 1 : (fused_ ? (pb_.ny < 2 * (fz::YPAD + 2) ? 5 : 6) : 2));
+    int k = (pb_.nmodels == 2 ? 1 : (march_ ? 2 : (fused_ ? (pb_.ny < 2 * (fz::YPAD + 2) ? 5 : 6) : 2)));
     if (ext_.nrec) k += 1;
     for (int c = 0; c < 3; c++) k += inj_.n[c] ? 1 : 0;
     return k;

@@ -121,7 +121,7 @@ private:
     DevBuf model_;                 // [nm][nxyz]
     DevBuf fields_;                // [3 levels][nshots][ncomp][nxyz]
     int rot_ = 0;                  // rotation of the three time levels
-    DevBuf aux_;                   // elastic derivative scratch [nshots][naux][nxyz]
+    DevBuf aux_;                   // elastic derivative scratch [nshots][naux][nxyz] (per-point path)
     DevBuf snaps_;                 // [nsnap][ncomp][nxyz] (single shot)
     int nsnap_ = 0;
     bool snaps_valid_ = false;
@@ -131,6 +131,7 @@ private:
     DevBuf taper_;                 // packed taper tables
     const float *taper_ptr_[6] = {};
     int scale_ = 0;
+    bool march_ = false;           // marching elastic kernel over all planes
     bool fused_ = false;           // fused elastic kernel for the interior planes
     int fused_minb_ = 1;           // resident CTAs per SM the fused kernel is compiled for
     DevBuf src_dev_, rcv_dev_;

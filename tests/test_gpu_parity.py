@@ -149,14 +149,32 @@ def test_vti_fused_traces(oracle_fp32):
 
 
 def test_fused_matches_per_point(monkeypatch):
-    """The fused interior kernel and the per-point kernels agree to rounding."""
+    """The marching kernel (default), the interior fused kernel (FWI_MARCH=0)
+    and the per-point kernels (FWI_MARCH=0 FWI_FUSED=0) agree to rounding."""
     out = {}
-    for flag in ("0", "1"):
-        monkeypatch.setenv("FWI_FUSED", flag)
+    for tag, march, fused in (("p", "0", "0"), ("f", "0", "1"), ("m", "1", "1")):
+        monkeypatch.setenv("FWI_MARCH", march)
+        monkeypatch.setenv("FWI_FUSED", fused)
         for name, sv in (("e", _elastic_fused()), ("v", _vti_fused())):
-            out[name + flag] = ops.from_survey(sv).forward(False, sv.model)
-    assert rel(out["e1"], out["e0"]) < 2e-6
-    assert rel(out["v1"], out["v0"]) < 2e-6
+            out[name + tag] = ops.from_survey(sv).forward(False, sv.model)
+    for name in "ev":
+        assert rel(out[name + "f"], out[name + "p"]) < 2e-6
+        assert rel(out[name + "m"], out[name + "p"]) < 2e-6
+
+
+def test_march_chunks_and_batch(monkeypatch):
+    """Marching kernel with several y chunks per tile column and a batch of
+    shots against the per-point kernels."""
+    sv = synth.elastic_layered(n=64, nsteps=100, taper=6, rec_stride=4, nshots=3)
+    for s in range(3):
+        sv.par.sxyz[s] = [(0.3 + 0.2 * s) * 64 * sv.dx, (0.5 - 0.1 * s) * 64 * sv.dx, 0.2 * 64 * sv.dx]
+    sv.par.set_bc(2, 1, 2, 1, 2, 1)
+    monkeypatch.setenv("FWI_MARCH", "1")
+    m = ops.forward_batch(sv)
+    monkeypatch.setenv("FWI_MARCH", "0")
+    monkeypatch.setenv("FWI_FUSED", "0")
+    p = ops.forward_batch(sv)
+    assert rel(m, p) < 2e-6
 
 
 def test_elastic_fused_gradient(oracle_fp32):
