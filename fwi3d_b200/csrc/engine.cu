@@ -382,10 +382,10 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     // when each axis is at least one tile plus the 6 closure rows long.
     fused_ = !march_ && pb.nmodels != 2 && !(env && env[0] == '0') && pb.nx >= fz::TX + 6 && pb.nz >= fz::TZ + 6 &&
              pb.ny > 2 * fz::YPAD;
-    // Occupancy variant of the fused kernel: 1 CTA per SM with up to 128
-    // registers (default) or 2 CTAs per SM with 64 registers.
+    // Occupancy variant of the fused kernel: 2 CTAs per SM with 64 registers
+    // (default, the faster on B200) or 1 CTA per SM with up to 128 registers.
     const char *mb = std::getenv("FWI_FUSED_MINB");
-    fused_minb_ = (mb && mb[0] == '2') ? 2 : 1;
+    fused_minb_ = (mb && mb[0] == '1') ? 1 : 2;
     if (fused_) {
         CK(cudaFuncSetAttribute(k_elastic_fused<ELASTIC, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(FusedSmem)));

@@ -133,7 +133,7 @@ private:
     int scale_ = 0;
     bool march_ = false;           // marching elastic kernel over all planes
     bool fused_ = false;           // fused elastic kernel for the interior planes
-    int fused_minb_ = 1;           // resident CTAs per SM the fused kernel is compiled for
+    int fused_minb_ = 2;           // resident CTAs per SM the fused kernel is compiled for
     DevBuf src_dev_, rcv_dev_;
     std::vector<void *> kev_;      // event pairs (begin, end) of the timed main-kernel launches
     int kev_used_ = 0;

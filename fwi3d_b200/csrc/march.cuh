@@ -51,7 +51,7 @@ struct MarchSmem {
     float u[f3::NR][3][f3::XU][f3::ZU];
     float yd[f3::NY][NYD][f3::TX][f3::TZ];
     float dv[ND3][f3::XD][f3::ZD];
-    float mp[NMP][f3::XD][f3::ZD];
+    float mp[2][NMP][f3::XD][f3::ZD];  // double-buffered: the next plane's arrive while this one is used
 };
 
 struct MarchCtx {
@@ -59,8 +59,38 @@ struct MarchCtx {
     int64_t so;      // wavefield offset of this shot
     int x0, z0;      // tile origin
     int xend, zend;  // end of this tile's output rows
+    int mb;          // materials buffer of the plane being output
     MarchSmem *sm;
 };
+
+// One 4-byte global->shared copy: asynchronous on the GPU (cp.async, zero
+// fill when `valid` is false; `src` then only has to be a mapped address),
+// a plain copy on the host.
+template <bool ASYNC>
+FWI_HD void m3_cp4(float *dst, const float *src, bool valid)
+{
+#if defined(__CUDA_ARCH__)
+    if (ASYNC) {
+        const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 4 : 0)
+                     : "memory");
+        return;
+    }
+#endif
+    *dst = valid ? *src : 0.f;
+}
+FWI_HD void m3_cp_commit()
+{
+#if defined(__CUDA_ARCH__)
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+#endif
+}
+FWI_HD void m3_cp_wait()
+{
+#if defined(__CUDA_ARCH__)
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+#endif
+}
 
 // Ring accessors along y (own column), indexed by global plane.
 struct URing {
@@ -75,7 +105,7 @@ struct YRing {
 // ---------------------------------------------------------------------------
 // Loads
 // ---------------------------------------------------------------------------
-template <bool INSIDE>
+template <bool INSIDE, bool ASYNC>
 FWI_HD void m3_load_u(const MarchCtx &c, int tid, int q)
 {
     const Dims &g = c.a->g;
@@ -84,14 +114,14 @@ FWI_HD void m3_load_u(const MarchCtx &c, int tid, int q)
         const int xu = p / f3::ZU, zu = p - xu * f3::ZU;
         const int ix = c.x0 - f3::HU + xu, iz = c.z0 - f3::HU + zu;
         const bool in = INSIDE || (ix >= 0 && ix < g.nx && iz >= 0 && iz < g.nz);
-        const int64_t i = in ? c.so + g.idx(ix, q, iz) : 0;
+        const int64_t i = c.so + (in ? g.idx(ix, q, iz) : 0);
 #pragma unroll
-        for (int k = 0; k < 3; k++) c.sm->u[slot][k][xu][zu] = in ? c.a->curr[k][i] : 0.f;
+        for (int k = 0; k < 3; k++) m3_cp4<ASYNC>(&c.sm->u[slot][k][xu][zu], c.a->curr[k] + i, in);
     }
 }
 
-template <int PH, bool INSIDE>
-FWI_HD void m3_load_mat(const MarchCtx &c, int tid, int y)
+template <int PH, bool INSIDE, bool ASYNC>
+FWI_HD void m3_load_mat(const MarchCtx &c, int tid, int b, int y)
 {
     const Dims &g = c.a->g;
     for (int p = tid; p < f3::XD * f3::ZD; p += f3::NT) {
@@ -99,12 +129,12 @@ FWI_HD void m3_load_mat(const MarchCtx &c, int tid, int y)
         const int ix = c.x0 - f3::HD + xd, iz = c.z0 - f3::HD + zd;
         const bool in = INSIDE || (ix >= 0 && ix < g.nx && iz >= 0 && iz < g.nz);
         const int64_t i = in ? g.idx(ix, y, iz) : 0;
-        c.sm->mp[MP_MU][xd][zd] = in ? c.a->m[1][i] : 0.f;
-        c.sm->mp[MP_LAM][xd][zd] = in ? c.a->m[0][i] : 0.f;
+        m3_cp4<ASYNC>(&c.sm->mp[b][MP_MU][xd][zd], c.a->m[1] + i, in);
+        m3_cp4<ASYNC>(&c.sm->mp[b][MP_LAM][xd][zd], c.a->m[0] + i, in);
         if (PH == VTI) {
-            c.sm->mp[MP_C13][xd][zd] = in ? c.a->m[3][i] : 0.f;
-            c.sm->mp[MP_EPS][xd][zd] = in ? c.a->m[4][i] : 0.f;
-            c.sm->mp[MP_C66][xd][zd] = in ? c.a->m[5][i] : 0.f;
+            m3_cp4<ASYNC>(&c.sm->mp[b][MP_C13][xd][zd], c.a->m[3] + i, in);
+            m3_cp4<ASYNC>(&c.sm->mp[b][MP_EPS][xd][zd], c.a->m[4] + i, in);
+            m3_cp4<ASYNC>(&c.sm->mp[b][MP_C66][xd][zd], c.a->m[5] + i, in);
         }
     }
 }
@@ -116,23 +146,23 @@ template <bool XF>
 FWI_HD float m3_dx(const MarchCtx &c, int k, int slot, int xu, int zu)
 {
     const float *p = &c.sm->u[slot][k][0][zu];
-    if (XF) {
+    const int ix = c.x0 - f3::HU + xu;
+    if (XF || (ix >= 4 && ix < c.a->g.nx - 4)) {
         const SbpTables &t = sbp();
         return (t.d1c0 * (p[(xu + 1) * f3::ZU] - p[(xu - 1) * f3::ZU]) +
                 t.d1c1 * (p[(xu + 2) * f3::ZU] - p[(xu - 2) * f3::ZU])) * c.a->idx;
     }
-    const int ix = c.x0 - f3::HU + xu;
     return d1_row(SXc{p, c.x0 - f3::HU, f3::ZU, f3::XU}, ix, c.a->g.nx) * c.a->idx;
 }
 template <bool ZF>
 FWI_HD float m3_dz(const MarchCtx &c, int k, int slot, int xu, int zu)
 {
     const float *p = &c.sm->u[slot][k][xu][0];
-    if (ZF) {
+    const int iz = c.z0 - f3::HU + zu;
+    if (ZF || (iz >= 4 && iz < c.a->g.nz - 4)) {
         const SbpTables &t = sbp();
         return (t.d1c0 * (p[zu + 1] - p[zu - 1]) + t.d1c1 * (p[zu + 2] - p[zu - 2])) * c.a->idz;
     }
-    const int iz = c.z0 - f3::HU + zu;
     return d1_row(SZc{p, c.z0 - f3::HU, f3::ZU}, iz, c.a->g.nz) * c.a->idz;
 }
 // Dy at plane q: interior taps from the ring, closure rows through the ring
@@ -207,13 +237,13 @@ FWI_HD void m3_derived(const MarchCtx &c, int tid, int y)
         const float ux0 = m3_dx<XF>(c, 0, s, xu, zu);
         const float uy1 = m3_dy(c, 1, y, xu, zu);
         const float uz2 = m3_dz<ZF>(c, 2, s, xu, zu);
-        const float lam = c.sm->mp[MP_LAM][xd][zd];
+        const float lam = c.sm->mp[c.mb][MP_LAM][xd][zd];
         if (PH == ELASTIC) {
             dv0[D3_T0 * STR] = lam * (ux0 + uy1 + uz2);
         } else {
-            const float mu = c.sm->mp[MP_MU][xd][zd];
-            const float c13 = c.sm->mp[MP_C13][xd][zd], eps = c.sm->mp[MP_EPS][xd][zd];
-            const float c66 = c.sm->mp[MP_C66][xd][zd];
+            const float mu = c.sm->mp[c.mb][MP_MU][xd][zd];
+            const float c13 = c.sm->mp[c.mb][MP_C13][xd][zd], eps = c.sm->mp[c.mb][MP_EPS][xd][zd];
+            const float c66 = c.sm->mp[c.mb][MP_C66][xd][zd];
             const float c11c = (1.f + 2.f * eps) * lam;
             const float c12 = (1.f + 2.f * eps) * (lam + 2.f * mu) - 2.f * c66;
             dv0[D3_T0 * STR] = c11c * ux0 + c12 * uy1 + c13 * uz2;
@@ -272,8 +302,8 @@ FWI_HD void m3_output(const MarchCtx &c, int tid, int y)
     const float *pu0 = &s.u[0][0][xu][zu];
     auto uy = [&](int k, int p) { return pu0[(p & R) * f3::USTR + k * f3::XU * f3::ZU]; };
 
-    const SX mux{&s.mp[MP_MU][0][zd], c.x0 - f3::HD, f3::ZD};
-    const SZ muz{&s.mp[MP_MU][xd][0], c.z0 - f3::HD};
+    const SX mux{&s.mp[c.mb][MP_MU][0][zd], c.x0 - f3::HD, f3::ZD};
+    const SZ muz{&s.mp[c.mb][MP_MU][xd][0], c.z0 - f3::HD};
     float acc[3];
     if (PH == ELASTIC) {
         W5 wx{}, wz{}, wy{};
@@ -300,8 +330,8 @@ FWI_HD void m3_output(const MarchCtx &c, int tid, int y)
             acc[k] = v;
         }
     } else {
-        const C11bS<SX, SX> bx{SX{&s.mp[MP_EPS][0][zd], c.x0 - f3::HD, f3::ZD}, mux};
-        const SX c6x{&s.mp[MP_C66][0][zd], c.x0 - f3::HD, f3::ZD};
+        const C11bS<SX, SX> bx{SX{&s.mp[c.mb][MP_EPS][0][zd], c.x0 - f3::HD, f3::ZD}, mux};
+        const SX c6x{&s.mp[c.mb][MP_C66][0][zd], c.x0 - f3::HD, f3::ZD};
         W5 wxb{}, wx6{}, wxm{}, wz{}, wyb{}, wy6{}, wym{};
         if (xin) {
             wxb = d2w(bx(ix - 2), bx(ix - 1), bx(ix), bx(ix + 1), bx(ix + 2));
@@ -345,7 +375,7 @@ FWI_HD void m3_output(const MarchCtx &c, int tid, int y)
     }
 
     // ---- D1 of the stress combinations and the mixed terms (we_op.cpp:661-688, 1312-1349) ----
-    const SX Px = (PH == VTI) ? SX{&s.mp[MP_C66][0][zd], c.x0 - f3::HD, f3::ZD} : mux;
+    const SX Px = (PH == VTI) ? SX{&s.mp[c.mb][MP_C66][0][zd], c.x0 - f3::HD, f3::ZD} : mux;
     const int PY = (PH == VTI) ? YD_C66 : YD_MU;
     const SX dT0x{&s.dv[D3_T0][0][zd], c.x0 - f3::HD, f3::ZD};
     const SZ dT2z{&s.dv[PH == ELASTIC ? D3_T0 : D3_T2][xd][0], c.z0 - f3::HD};
@@ -427,37 +457,72 @@ FWI_HD void m3_range(int ny, int ya, int yb, int &q0, int &q1)
     q1 = yb == ny ? ny - 1 : yb + 1;
 }
 
-// Runs the march with `par(phase)`: every thread of the block runs phase(tid),
-// then the block synchronises.
-template <int PH, bool XF, bool ZF, class Par>
-FWI_HD void m3_march(const MarchCtx &c, int ya, int yb, Par &&par)
+// Lowest displacement plane iteration q reads (column phase and outputs).
+FWI_HD int m3_lowest(int q, int ny, const int *out, int nout)
 {
+    auto lo = [&](int p) { return p < 4 ? 0 : (p >= ny - 4 ? ny - 6 : p - 2); };
+    int low = lo(q);
+    for (int k = 0; k < nout; k++) low = lo(out[k]) < low ? lo(out[k]) : low;
+    return low;
+}
+
+// Runs the march with `par(phase)`: every thread of the block runs phase(tid),
+// then the block synchronises.  While iteration q computes, the displacement
+// planes and the materials that iteration q+1 needs are copied in
+// asynchronously, into ring slots and a materials buffer q does not read.
+template <int PH, bool XF, bool ZF, class Par>
+FWI_HD void m3_march(MarchCtx c, int ya, int yb, Par &&par)
+{
+    constexpr bool IN = XF && ZF;
     const int ny = c.a->g.ny;
     int q0, q1;
     m3_range(ny, ya, yb, q0, q1);
-    int loaded = (q0 == 0 ? 0 : q0 - 2) - 1;
+    int loaded = (q0 == 0 ? 0 : q0 - 2) - 1;  // highest plane loaded or in flight
+    int mb = 0;                                // materials buffer of the next output
+    int mp_plane = -1;                         // plane whose materials are in flight into mb
     for (int q = q0; q <= q1; q++) {
         int out[5];
         const int nout = m3_outputs(q, ny, ya, yb, out);
         const int need = m3_need(q, ny);
         const int lo = loaded + 1;
         loaded = need > loaded ? need : loaded;
+        const bool have_mp = nout && mp_plane == out[0];
         par([&](int tid) {
-            for (int p = lo; p <= need; p++) m3_load_u<XF && ZF>(c, tid, p);
-            if (nout) m3_load_mat<PH, XF && ZF>(c, tid, out[0]);
+            m3_cp_wait();
+            for (int p = lo; p <= need; p++) m3_load_u<IN, false>(c, tid, p);
+            if (nout && !have_mp) m3_load_mat<PH, IN, false>(c, tid, mb, out[0]);
         });
+        // copies for iteration q+1
+        int pf_hi = loaded, nn = 0, nout1[5];
+        if (q < q1) {
+            const int need1 = m3_need(q + 1, ny), low = m3_lowest(q, ny, out, nout);
+            while (pf_hi < need1 && pf_hi + 1 - f3::NR < low) pf_hi++;
+            nn = m3_outputs(q + 1, ny, ya, yb, nout1);
+        }
+        const int pf_lo = loaded + 1;
+        const int nmb = (mb + nout) & 1;
+        const bool pf_mp = nn > 0 && nout <= 1;
+        c.mb = mb;
         par([&](int tid) {
+            for (int p = pf_lo; p <= pf_hi; p++) m3_load_u<IN, true>(c, tid, p);
+            if (pf_mp) m3_load_mat<PH, IN, true>(c, tid, nmb, nout1[0]);
+            m3_cp_commit();
             m3_column<PH, XF, ZF>(c, tid, q);
             if (nout) m3_derived<PH, XF, ZF>(c, tid, out[0]);
         });
+        loaded = pf_hi;
         for (int k = 0; k < nout; k++) {
+            c.mb = (mb + k) & 1;
             if (k > 0) {
-                par([&](int tid) { m3_load_mat<PH, XF && ZF>(c, tid, out[k]); });
+                par([&](int tid) { m3_load_mat<PH, IN, false>(c, tid, c.mb, out[k]); });
                 par([&](int tid) { m3_derived<PH, XF, ZF>(c, tid, out[k]); });
             }
             par([&](int tid) { m3_output<PH, XF, ZF>(c, tid, out[k]); });
         }
+        mb = nmb;
+        mp_plane = pf_mp ? nout1[0] : -1;
     }
+    par([&](int) { m3_cp_wait(); });
 }
 
 // Chunk of planes [ya, yb) of chunk ch of nch along ny: interior boundaries
