@@ -28,7 +28,8 @@ EXPORTS = [
     "fwi_op_destroy", "fwi_forward_batch", "fwi_batch_create", "fwi_batch_reset", "fwi_batch_run",
     "fwi_batch_sync", "fwi_batch_stream", "fwi_batch_traces", "fwi_batch_get_info", "fwi_batch_destroy",
     "fwi_last_error", "fwi_version", "fwi_elastic_step_static", "fwi_batch_time_main_kernel",
-    "fwi_batch_main_kernel_time",
+    "fwi_batch_main_kernel_time", "fwi_objective_create", "fwi_objective_evaluate", "fwi_objective_device_bytes",
+    "fwi_objective_destroy",
 ]
 
 
@@ -58,7 +59,7 @@ class CParam(C.Structure):
         ("rhomin", C.c_float), ("rhomax", C.c_float),
         ("deltamin", C.c_float), ("deltamax", C.c_float), ("epsilonmin", C.c_float),
         ("epsilonmax", C.c_float), ("gammamin", C.c_float), ("gammamax", C.c_float),
-        ("soft_clip", C.c_int), ("verbose", C.c_int),
+        ("soft_clip", C.c_int), ("verbose", C.c_int), ("snapshot_storage", C.c_int),
     ]
 
 
@@ -119,6 +120,15 @@ def load() -> C.CDLL:
     lib.fwi_batch_main_kernel_time.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_int64),
                                                C.POINTER(C.c_char_p)]
     lib.fwi_batch_main_kernel_time.restype = C.c_int
+    lib.fwi_objective_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(Grid), C.c_int, C.POINTER(CParam), fp,
+                                         C.c_int, C.c_int, C.c_float, C.c_int, fp, C.c_int, fp, fp, C.c_int, C.c_int]
+    lib.fwi_objective_create.restype = C.c_int
+    lib.fwi_objective_evaluate.argtypes = [vp, fp, C.POINTER(C.c_double), fp, fp]
+    lib.fwi_objective_evaluate.restype = C.c_int
+    lib.fwi_objective_device_bytes.argtypes = [vp]
+    lib.fwi_objective_device_bytes.restype = C.c_int64
+    lib.fwi_objective_destroy.argtypes = [vp]
+    lib.fwi_objective_destroy.restype = None
     lib.fwi_last_error.restype = C.c_char_p
     lib.fwi_version.restype = C.c_char_p
     _lib = lib

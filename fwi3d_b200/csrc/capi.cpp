@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -102,6 +103,7 @@ struct fwi_op {
         const bool same = eng && pb.nt == p.nt && pb.dt == p.dt && pb.sub == p.sub;
         pb = p;
         if (!same) eng.reset(new Engine(device, pb));
+        eng->set_storage(par.snapshot_storage);
         eng->set_model(m.data());
         conv.swap(m);
     }
@@ -125,6 +127,21 @@ struct fwi_batch {
     int it = 0;  // time steps run since reset
     Problem pb{};
     std::unique_ptr<Engine> eng;
+};
+
+struct fwi_objective {
+    int device = 0;
+    fwi_grid grid{};
+    int nmodels = 3;
+    fwi_param par{};
+    int nt_data = 0;
+    float dt_data = 0.f;
+    int nshots = 1, nr = 0, nscomp = 1, nrcomp = 1, batch = 1;
+    std::vector<float> wavelet, sxyz, rxyz, observed;
+    double dnorm = 1.0;
+    Problem pb{};
+    std::map<int, std::unique_ptr<Engine>> eng;  // one engine per batch size
+    int64_t device_bytes = 0;
 };
 
 extern "C" {
@@ -161,6 +178,7 @@ void fwi_param_default(fwi_param *p)
     p->gammamax = 1.f;
     p->soft_clip = 0;
     p->verbose = 0;
+    p->snapshot_storage = 0;
 }
 
 const char *fwi_last_error(void) { return g_err.c_str(); }
@@ -511,6 +529,192 @@ int fwi_batch_main_kernel_time(fwi_batch *b, double *ms, int *launches, int64_t 
     if (!b || !ms) return fail(FWI_ERR_ARG, "null argument");
     return guarded([&] { *ms = b->eng->main_kernel_ms(launches, points, name); });
 }
+
+int fwi_objective_create(fwi_objective **out, int device, const fwi_grid *grid, int nmodels, const fwi_param *par,
+                         const float *wavelet, int wavelet_ncomp, int nt_data, float dt_data, int nshots,
+                         const float *sxyz, int nr, const float *rxyz, const float *observed, int normalize, int batch)
+{
+    if (!out || !grid || !par || !wavelet || !sxyz || !rxyz || !observed || nshots < 1 || nr < 1)
+        return fail(FWI_ERR_ARG, "null argument, no shot or no receiver");
+    *out = nullptr;
+    if (nmodels != 2 && nmodels != 3 && nmodels != 6)
+        return fail(FWI_ERR_ARG, "The model must contain 2, 3, or 6 parameters");
+    if (grid->nx < 12 || grid->ny < 12 || grid->nz < 12) return fail(FWI_ERR_ARG, "each grid axis needs at least 12 points");
+    if (nt_data < 2 || !(dt_data > 0)) return fail(FWI_ERR_ARG, "the wavelet needs at least 2 samples and dt > 0");
+    if (par->gl > 0) return fail(FWI_ERR_UNSUPPORTED, "DAS receivers (gl > 0) are not implemented on the GPU path");
+    return guarded([&] {
+        std::unique_ptr<fwi_objective> o(new fwi_objective());
+        o->device = device;
+        o->grid = *grid;
+        o->nmodels = nmodels;
+        o->par = *par;
+        if (nmodels == 2) o->par.mt = 0;
+        o->nt_data = nt_data;
+        o->dt_data = dt_data;
+        o->nshots = nshots;
+        o->nr = nr;
+        o->nscomp = nmodels == 2 ? 1 : (o->par.mt ? 6 : 3);
+        o->nrcomp = nmodels == 2 ? 1 : 3;
+        o->batch = batch < 1 ? nshots : std::min(batch, nshots);
+        o->wavelet = expand_wavelet(wavelet, wavelet_ncomp, nt_data, nmodels, o->par);
+        o->sxyz.assign(sxyz, sxyz + 3 * nshots);
+        o->rxyz.assign(rxyz, rxyz + (size_t)5 * nr * nshots);
+        const size_t nd = (size_t)nshots * o->nrcomp * nr * nt_data;
+        o->observed.assign(observed, observed + nd);
+        if (!finite_all(observed, (int64_t)nd)) throw FwiError(FWI_ERR_NAN, "observed data contain non-finite values");
+        double dn = 1.0;
+        if (normalize) {
+            double ss = 0;
+            for (size_t i = 0; i < nd; i++) ss += (double)observed[i] * observed[i];
+            dn = ss * dt_data;
+            if (dn < 1e-16) dn = 1.0;
+        }
+        o->dnorm = dn;
+        *out = o.release();
+    });
+}
+
+int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, float *grad, float *residual)
+{
+    if (!o || !model || !f || !grad) return fail(FWI_ERR_ARG, "null argument");
+    return guarded([&] {
+        const fwi_grid &g = o->grid;
+        const int64_t n = (int64_t)g.nx * g.ny * g.nz;
+        const int nm = std::min(3, o->nmodels);
+        if (!finite_all(model, o->nmodels * n)) throw FwiError(FWI_ERR_NAN, "model contains non-finite values");
+        std::vector<float> m(model, model + o->nmodels * n);
+        fwi_param par = o->par;
+        TimeAxis ta = analyze_model(m, o->nmodels, g.nx, g.ny, g.nz, g.dx, g.dy, g.dz, o->nt_data, o->dt_data, par);
+        if (ta.sub < 1) ta.sub = std::max(1, (int)std::lround((double)(o->dt_data / ta.dt)));
+        convert_model(m, o->nmodels, n);
+        Problem p{};
+        p.nmodels = o->nmodels;
+        p.nx = g.nx;
+        p.ny = g.ny;
+        p.nz = g.nz;
+        p.dx = g.dx;
+        p.dy = g.dy;
+        p.dz = g.dz;
+        p.dt = ta.dt;
+        p.nt = ta.nt;
+        p.sub = ta.sub;
+        for (int k = 0; k < 6; k++) p.bc[k] = std::max(0, par.bc[k]);
+        std::memcpy(p.taper, par.taper, sizeof(p.taper));
+        p.taper_strength = par.taper_strength;
+        p.free_surface_stiffness =
+            o->nmodels == 2 ? std::max(par.free_surface_stiffness, 1.0f) : par.free_surface_stiffness;
+        const int nt = p.nt, ntd = o->nt_data;
+        const int ncr = p.ncomp();
+        const int ntr = ncr * o->nr;
+        const bool sinc = par.resampling_linear == 0;
+        const float alpha = p.dt / o->dt_data;
+        // wavelet at the propagation sampling (same for every shot)
+        std::vector<float> w1((size_t)o->nscomp * nt);
+        resample_forward(sinc, par.sinc_half_length, o->wavelet.data(), ntd, o->dt_data, w1.data(), nt, p.dt, o->nscomp);
+        std::vector<double> gsum((size_t)nm * n, 0.0);
+        double fsum = 0.0;
+        o->device_bytes = 0;
+        for (int s0 = 0; s0 < o->nshots; s0 += o->batch) {
+            const int B = std::min(o->batch, o->nshots - s0);
+            p.nshots = B;
+            auto &eng = o->eng[B];
+            const bool same = eng && o->pb.nt == p.nt && o->pb.dt == p.dt && o->pb.sub == p.sub;
+            if (!same) eng.reset(new Engine(o->device, p));
+            eng->set_storage(par.snapshot_storage);
+            eng->set_model(m.data());
+            // tables of the batch (shot b of the batch at wavefield offset b)
+            InjTable inj, adj;
+            ExtTable ext;
+            ext.nrec = B * o->nr;
+            std::vector<float> src((size_t)B * o->nscomp * nt);
+            for (int b = 0; b < B; b++) {
+                const int sh = s0 + b;
+                std::memcpy(src.data() + (size_t)b * w1.size(), w1.data(), sizeof(float) * w1.size());
+                const float *sx = &o->sxyz[3 * sh];
+                PointOp pi = make_delta(p.nx, p.ny, p.nz, p.dx, p.dy, p.dz, g.ox, g.oy, g.oz, {Loc{sx[0], sx[1], sx[2]}},
+                                        par.mt != 0);
+                InjTable t = injection_table(pi, p.nx, p.ny, p.nz, ncr);
+                std::vector<Loc> rl(o->nr);
+                const float *rs = &o->rxyz[(size_t)5 * o->nr * sh];
+                for (int r = 0; r < o->nr; r++) rl[r] = Loc{rs[5 * r], rs[5 * r + 1], rs[5 * r + 2]};
+                PointOp pr = make_delta(p.nx, p.ny, p.nz, p.dx, p.dy, p.dz, g.ox, g.oy, g.oz, rl, false);
+                InjTable ta2 = injection_table(pr, p.nx, p.ny, p.nz, ncr);
+                ExtTable e = extraction_table(pr, p.nx, p.ny, p.nz);
+                for (int c = 0; c < ncr; c++) {
+                    for (size_t k = 0; k < t.gidx[c].size(); k++) {
+                        inj.gidx[c].push_back(t.gidx[c][k] + b * n);
+                        inj.trace[c].push_back(t.trace[c][k] + b * o->nscomp);
+                        inj.w[c].push_back(t.w[c][k]);
+                    }
+                    for (size_t k = 0; k < ta2.gidx[c].size(); k++) {
+                        adj.gidx[c].push_back(ta2.gidx[c][k] + b * n);
+                        adj.trace[c].push_back(ta2.trace[c][k] + b * ntr);
+                        adj.w[c].push_back(ta2.w[c][k]);
+                    }
+                }
+                for (auto gi : e.gidx) ext.gidx.push_back(gi + b * n);
+                ext.w.insert(ext.w.end(), e.w.begin(), e.w.end());
+            }
+            std::vector<float> rcv((size_t)B * ntr * nt);
+            eng->forward(inj, B * o->nscomp, src.data(), ext, rcv.data(), true);
+            if (!finite_all(rcv.data(), (int64_t)rcv.size())) throw FwiError(FWI_ERR_NAN, "non-finite values in the traces");
+            std::vector<float> asrc((size_t)B * ntr * nt);
+            std::vector<float> syn((size_t)ntr * ntd), tmp;
+            for (int b = 0; b < B; b++) {
+                const int sh = s0 + b;
+                float *r = rcv.data() + (size_t)b * ntr * nt;
+                if (par.seismotype == 1) {
+                    tmp.resize((size_t)ntr * nt);
+                    apply_dt(false, r, tmp.data(), ntr, nt, p.dt);
+                    std::memcpy(r, tmp.data(), sizeof(float) * tmp.size());
+                }
+                for (size_t i = 0; i < (size_t)ntr * nt; i++) r[i] *= alpha;
+                std::fill(syn.begin(), syn.end(), 0.f);
+                resample_adjoint(sinc, par.sinc_half_length, syn.data(), ntd, o->dt_data, r, nt, p.dt, ntr);
+                // residual and misfit (optimization.cpp:111-115, optimization.hpp:410-424), FP64 sums
+                const float *obs = &o->observed[(size_t)sh * ntr * ntd];
+                for (size_t i = 0; i < syn.size(); i++) syn[i] -= obs[i];
+                double ss = 0;
+                for (size_t i = 0; i < syn.size(); i++) ss += (double)syn[i] * syn[i];
+                for (int tr = 0; tr < ntr; tr++) {
+                    const double a0 = syn[(size_t)tr * ntd], a1 = syn[(size_t)tr * ntd + ntd - 1];
+                    ss -= 0.5 * (a0 * a0 + a1 * a1);
+                }
+                fsum += ss;
+                if (residual) std::memcpy(residual + (size_t)sh * ntr * ntd, syn.data(), sizeof(float) * syn.size());
+                // adjoint sources: Ht(r) (optimization.cpp:118), then jacobianT's data path (we_op.cpp:994-1003)
+                apply_ht(false, syn.data(), syn.data(), ntr, ntd, o->dt_data);
+                float *as = asrc.data() + (size_t)b * ntr * nt;
+                resample_forward(sinc, par.sinc_half_length, syn.data(), ntd, o->dt_data, as, nt, p.dt, ntr);
+                apply_ht(true, as, as, ntr, nt, p.dt);
+                for (int tr = 0; tr < ntr; tr++) std::reverse(as + (size_t)tr * nt, as + (size_t)(tr + 1) * nt);
+                for (size_t i = 0; i < (size_t)ntr * nt; i++) as[i] *= -alpha;
+                if (par.seismotype == 1) {
+                    tmp.resize((size_t)ntr * nt);
+                    apply_dt(true, as, tmp.data(), ntr, nt, p.dt);
+                    std::memcpy(as, tmp.data(), sizeof(float) * tmp.size());
+                }
+            }
+            std::vector<float> gb((size_t)nm * n);
+            eng->adjoint(adj, B * ntr, asrc.data(), gb.data());
+            for (size_t i = 0; i < gb.size(); i++) gsum[i] += gb[i];
+            o->device_bytes = std::max(o->device_bytes, eng->device_bytes());
+            o->pb = p;
+        }
+        // H quadrature, chain rule to (vp, vs, rho), 1/dnorm (we_op.cpp:1027-1067, optimization.cpp:194)
+        for (int64_t i = 0; i < nm * n; i++) grad[i] = (float)gsum[i];
+        for (int q = 0; q < nm; q++) apply_h3(grad + q * n, p.nx, p.ny, p.nz, p.dx, p.dy, p.dz);
+        gradient_to_velocity(grad, m.data(), o->nmodels, n);
+        const float sc = (float)(1.0 / o->dnorm);
+        for (int64_t i = 0; i < nm * n; i++) grad[i] *= sc;
+        *f = 0.5 * o->dt_data * fsum / o->dnorm;
+        if (!finite_all(grad, nm * n)) throw FwiError(FWI_ERR_NAN, "non-finite values in the gradient");
+    });
+}
+
+int64_t fwi_objective_device_bytes(const fwi_objective *o) { return o ? o->device_bytes : 0; }
+
+void fwi_objective_destroy(fwi_objective *o) { delete o; }
 
 int fwi_elastic_step_static(const fwi_grid *grid, int nmodels, const int *bc, float dt, const float *model,
                             const float *prev, const float *curr, float *next, void *stream)

@@ -7,6 +7,7 @@
 //   step      D2var + D1 terms + SAT + update + scale + taper, fused   k_*_step
 //   inject    sources (receivers' residual in the adjoint)  k_inject
 // and, every `sub` steps of the adjoint, the imaging condition k_*_image.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -798,33 +799,178 @@ void Engine::copy_traces(float *rcv)
     sync();
 }
 
+// ---------------------------------------------------------------------------
+// Snapshot storage.  FP32 keeps every snapshot as is.  FP16P keeps, per
+// snapshot k, the second-difference residual r_k = u_k - (2 e_{k-1} - e_{k-2})
+// (e = the reconstructed snapshots, FP64; predictions e_{k-1} for k = 1 and 0
+// for k = 0) as FP16 scaled by max|r_k| per shot and component.  The encoder
+// is closed-loop, so the error of every snapshot is one quantisation step of
+// its own residual, and e_{k+1} - 2 e_k + e_{k-1} -- the second time
+// difference the density imaging term uses -- is the stored residual itself.
+// The adjoint decodes backwards from the encoder's final state:
+// e_{j-1} = 2 e_j - e_{j+1} + r_{j+1}.
+// ---------------------------------------------------------------------------
+namespace {
+__device__ __forceinline__ double enc_pred(const double *e1, const double *e2, int64_t i, int k)
+{
+    return k >= 2 ? 2.0 * e1[i] - e2[i] : (k == 1 ? e1[i] : 0.0);
+}
+
+// grid (x: points, y: shot*ncomp); e: [2][nsc][n], level 0 = e_{k-1}, level 1 = e_{k-2}
+__global__ void k_enc_max(const float *u, const double *e, int64_t n, int nsc, int k, unsigned *amax)
+{
+    const int sc = blockIdx.y;
+    const double *e1 = e + (int64_t)sc * n, *e2 = e + ((int64_t)nsc + sc) * n;
+    const float *us = u + (int64_t)sc * n;
+    float m = 0.f;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        m = fmaxf(m, (float)fabs((double)us[i] - enc_pred(e1, e2, i, k)));
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(&amax[sc], __float_as_uint(m));
+}
+
+__global__ void k_enc_quant(const float *u, double *e, int64_t n, int nsc, int k, const unsigned *amax, __half *q,
+                            float *scales)
+{
+    const int sc = blockIdx.y;
+    double *e1 = e + (int64_t)sc * n, *e2 = e + ((int64_t)nsc + sc) * n;
+    const float *us = u + (int64_t)sc * n;
+    __half *qs = q + (int64_t)sc * n;
+    float sf = __uint_as_float(amax[sc]);
+    if (!(sf > 0.f)) sf = 1.f;
+    if (blockIdx.x == 0 && threadIdx.x == 0) scales[sc] = sf;
+    const double sd = sf;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double p = enc_pred(e1, e2, i, k);
+        const __half h = __float2half_rn((float)(((double)us[i] - p) / sd));
+        qs[i] = h;
+        const double ek = p + (double)__half2float(h) * sd;
+        e2[i] = e1[i];
+        e1[i] = ek;
+    }
+}
+
+// One backward step: state (A = e_{j+1}, B = e_j) -> (e_j, e_{j-1}); out = float(e_{j-1}).
+__global__ void k_dec_step(double *e, int64_t n, int nsc, const __half *q, const float *scales, float *out)
+{
+    const int sc = blockIdx.y;
+    double *A = e + (int64_t)sc * n, *B = e + ((int64_t)nsc + sc) * n;
+    const __half *qs = q + (int64_t)sc * n;
+    const double sd = scales[sc];
+    float *o = out + (int64_t)sc * n;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double b = B[i];
+        const double v = 2.0 * b - A[i] + (double)__half2float(qs[i]) * sd;
+        A[i] = b;
+        B[i] = v;
+        o[i] = (float)v;
+    }
+}
+
+__global__ void k_d2f_strided(const double *in, float *out, int64_t n)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (float)in[i];
+}
+
+dim3 stream_grid(int64_t n, int nsc)
+{
+    const int64_t bx = std::min<int64_t>((n + 255) / 256, 1184);
+    return dim3((unsigned)std::max<int64_t>(bx, 1), (unsigned)nsc);
+}
+}  // namespace
+
+void Engine::snap_store(int k)
+{
+    cudaStream_t s = (cudaStream_t)stream_;
+    const int64_t n = pb_.nxyz();
+    const int nsc = pb_.nshots * pb_.ncomp();
+    if (k > nsnap_ - 1) return;
+    nwritten_ = std::max(nwritten_, k + 1);
+    if (storage_ == STORE_FP32) {
+        CK(cudaMemcpyAsync(snaps_.as<float>() + (int64_t)k * nsc * n, level(1), sizeof(float) * nsc * n,
+                           cudaMemcpyDeviceToDevice, s));
+        return;
+    }
+    CK(cudaMemsetAsync(amax_.p, 0, amax_.bytes, s));
+    const dim3 grd = stream_grid(n, nsc);
+    k_enc_max<<<grd, 256, 0, s>>>(level(1), enc_.as<double>(), n, nsc, k, amax_.as<unsigned>());
+    k_enc_quant<<<grd, 256, 0, s>>>(level(1), enc_.as<double>(), n, nsc, k, amax_.as<unsigned>(),
+                                    snapq_.as<__half>() + (int64_t)k * nsc * n, snaps_scale_.as<float>() + (int64_t)k * nsc);
+    CK(cudaGetLastError());
+}
+
+const float *Engine::snap_fp32(int kk)
+{
+    const int64_t n = pb_.nxyz();
+    const int nsc = pb_.nshots * pb_.ncomp();
+    if (storage_ == STORE_FP32) return snaps_.as<float>() + (int64_t)kk * nsc * n;
+    if (kk >= nwritten_) return snapz_.as<float>();
+    cudaStream_t s = (cudaStream_t)stream_;
+    const dim3 grd = stream_grid(n, nsc);
+    while (kk < dec_lo_) {
+        // decode e_{dec_lo_-1} with the residual of snapshot dec_lo_+1
+        const int j = dec_lo_;
+        k_dec_step<<<grd, 256, 0, s>>>(enc_.as<double>(), n, nsc, snapq_.as<__half>() + (int64_t)(j + 1) * nsc * n,
+                                       snaps_scale_.as<float>() + (int64_t)(j + 1) * nsc,
+                                       snaps_.as<float>() + (int64_t)((j - 1) % 3) * nsc * n);
+        CK(cudaGetLastError());
+        dec_lo_ = j - 1;
+    }
+    return snaps_.as<float>() + (int64_t)(kk % 3) * nsc * n;
+}
+
 void Engine::forward(const InjTable &inj, int ntrace, const float *src, const ExtTable &ext, float *rcv, bool store)
 {
     CK(cudaSetDevice(device_));
     cudaStream_t s = (cudaStream_t)stream_;
     const int64_t n = pb_.nxyz();
-    const int nc = pb_.ncomp();
-    if (pb_.nshots != 1) throw FwiError(FWI_ERR_ARG, "the operator path runs one shot");
+    const int nsc = pb_.nshots * pb_.ncomp();
     set_sources(inj, ntrace, src);
-    set_receivers(ext, ext.nrec);
+    set_receivers(ext, ext.nrec / pb_.nshots);
     snaps_valid_ = false;
+    nwritten_ = 0;
     const bool keep = store && pb_.sub > 0;
     if (keep) {
         nsnap_ = 1 + pb_.nt / pb_.sub;
-        snaps_.alloc(sizeof(float) * (size_t)nsnap_ * nc * n);
-        snaps_.zero(s);
+        // FP16P needs at least three stored snapshots to decode backwards
+        const int written = 1 + (pb_.nt - 1) / pb_.sub;
+        if (storage_ == STORE_FP16P && written < 3) storage_ = STORE_FP32;
+        if (storage_ == STORE_FP32) {
+            snapq_.alloc(0);
+            snaps_scale_.alloc(0);
+            enc_.alloc(0);
+            snapz_.alloc(0);
+            snaps_.alloc(sizeof(float) * (size_t)nsnap_ * nsc * n);
+            snaps_.zero(s);
+        } else {
+            snaps_.alloc(sizeof(float) * 3 * (size_t)nsc * n);
+            snapq_.alloc(sizeof(__half) * (size_t)nsnap_ * nsc * n);
+            snaps_scale_.alloc(sizeof(float) * (size_t)nsnap_ * nsc);
+            enc_.alloc(sizeof(double) * 2 * (size_t)nsc * n);
+            enc_.zero(s);
+            amax_.alloc(sizeof(unsigned) * (size_t)nsc);
+            snapz_.alloc(sizeof(float) * (size_t)nsc * n);
+            snapz_.zero(s);
+        }
     }
     reset();
-    auto snap = [&](int k) {
-        if (k > nsnap_ - 1) return;
-        CK(cudaMemcpyAsync(snaps_.as<float>() + (int64_t)k * nc * n, level(1), sizeof(float) * nc * n,
-                           cudaMemcpyDeviceToDevice, s));
-    };
     for (int it = 0; it < pb_.nt - 1; it++) {
-        if (keep && it % pb_.sub == 0) snap(it / pb_.sub);
+        if (keep && it % pb_.sub == 0) snap_store(it / pb_.sub);
         run(it, 1);
     }
-    if (keep && (pb_.nt - 1) % pb_.sub == 0) snap((pb_.nt - 1) / pb_.sub);
+    if (keep && (pb_.nt - 1) % pb_.sub == 0) snap_store((pb_.nt - 1) / pb_.sub);
+    if (keep && storage_ == STORE_FP16P) {
+        // decoder starts from the encoder's final state (e_K, e_{K-1})
+        const int K = nwritten_ - 1;
+        const double *e = enc_.as<double>();
+        const dim3 grd = stream_grid((int64_t)nsc * n, 1);
+        k_d2f_strided<<<grd, 256, 0, s>>>(e, snaps_.as<float>() + (int64_t)(K % 3) * nsc * n, (int64_t)nsc * n);
+        k_d2f_strided<<<grd, 256, 0, s>>>(e + (int64_t)nsc * n, snaps_.as<float>() + (int64_t)((K - 1) % 3) * nsc * n,
+                                          (int64_t)nsc * n);
+        CK(cudaGetLastError());
+        dec_lo_ = K - 1;
+    }
     extract_last();
     copy_traces(rcv);
     snaps_valid_ = keep;
@@ -845,21 +991,26 @@ void Engine::image(int itl, const float *curr, const float *prevl)
     a.itl = itl;
     a.last = pb_.nt / pb_.sub;
     for (int k = 0; k < pb_.nmodels; k++) a.m[k] = model_.as<float>() + k * n;
+    const float *lev[3];
     for (int l = 0; l < 3; l++) {
         const int k = itl - 1 + l;
-        const int kk = std::min(std::max(k, 0), nsnap_ - 1);
-        for (int c = 0; c < 3; c++) a.fwd[l][c] = snaps_.as<float>() + ((int64_t)kk * nc + (c < nc ? c : 0)) * n;
-    }
-    for (int c = 0; c < 3; c++) {
-        const int cc = c < nc ? c : 0;
-        a.adj[c] = curr + cc * n;
-        a.lag[c] = prevl + cc * n;
-        a.grad[c] = grad_.as<double>() + (int64_t)(c < (pb_.nmodels == 2 ? 2 : 3) ? c : 0) * n;
+        lev[l] = snap_fp32(std::min(std::max(k, 0), nsnap_ - 1));
     }
     const dim3 blk(BZ, BX, BY), grd = grid_of(a.g, 1);
-    if (pb_.nmodels == 2) k_acoustic_image<<<grd, blk, 0, s>>>(a);
-    else if (pb_.nmodels == 3) k_elastic_image<ELASTIC><<<grd, blk, 0, s>>>(a);
-    else k_elastic_image<VTI><<<grd, blk, 0, s>>>(a);
+    for (int sh = 0; sh < pb_.nshots; sh++) {
+        const int64_t so = (int64_t)sh * nc * n;
+        for (int l = 0; l < 3; l++)
+            for (int c = 0; c < 3; c++) a.fwd[l][c] = lev[l] + so + (int64_t)(c < nc ? c : 0) * n;
+        for (int c = 0; c < 3; c++) {
+            const int cc = c < nc ? c : 0;
+            a.adj[c] = curr + so + cc * n;
+            a.lag[c] = prevl + so + cc * n;
+            a.grad[c] = grad_.as<double>() + (int64_t)(c < (pb_.nmodels == 2 ? 2 : 3) ? c : 0) * n;
+        }
+        if (pb_.nmodels == 2) k_acoustic_image<<<grd, blk, 0, s>>>(a);
+        else if (pb_.nmodels == 3) k_elastic_image<ELASTIC><<<grd, blk, 0, s>>>(a);
+        else k_elastic_image<VTI><<<grd, blk, 0, s>>>(a);
+    }
     CK(cudaGetLastError());
 }
 
@@ -892,6 +1043,7 @@ void Engine::adjoint(const InjTable &inj, int ntrace, const float *adj_src, floa
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(grad, gf.p, gf.bytes, cudaMemcpyDeviceToHost, s));
     sync();
+    snaps_valid_ = storage_ == STORE_FP32;  // the FP16P decoder state is consumed
 }
 
 // ---------------------------------------------------------------------------

@@ -88,11 +88,17 @@ public:
     void copy_traces(float *rcv);         // [nshots][nrcomp][nr][nt] raw traces (host)
     int launches_per_step() const;
 
-    // --- single-shot operator path ------------------------------------------
-    // forward: full time loop; keeps snapshots when store && sub > 0
+    // --- operator / gradient path (one shot or a batch of shots) -------------
+    // Snapshot storage of the forward wavefield for the imaging condition.
+    enum Storage { STORE_FP32 = 0, STORE_FP16P = 1 };
+    void set_storage(int mode) { storage_ = mode; }
+    // forward: full time loop; keeps snapshots when store && sub > 0.  Tables of
+    // all shots (as set_sources/set_receivers); rcv [nshots][ncomp][nr][nt].
     void forward(const InjTable &inj, int ntrace, const float *src, const ExtTable &ext, float *rcv, bool store);
-    // adjoint + imaging; grad out: [min(3,nm)][nxyz] float (before H quadrature and chain rule)
+    // adjoint + imaging of every shot of the batch; grad out: [min(3,nm)][nxyz]
+    // float, summed over the shots in FP64 (before H quadrature and chain rule)
     void adjoint(const InjTable &inj, int ntrace, const float *adj_src, float *grad);
+    int64_t snapshot_bytes() const { return snaps_.bytes + snapq_.bytes + enc_.bytes + snapz_.bytes; }
 
     // Diagnostic timing of the step's main kernel (the fused interior kernel,
     // else the per-point step kernel): a pair of CUDA events on the engine
@@ -122,8 +128,18 @@ private:
     DevBuf fields_;                // [3 levels][nshots][ncomp][nxyz]
     int rot_ = 0;                  // rotation of the three time levels
     DevBuf aux_;                   // elastic derivative scratch [nshots][naux][nxyz] (per-point path)
-    DevBuf snaps_;                 // [nsnap][ncomp][nxyz] (single shot)
+    DevBuf snaps_;                 // FP32 storage: [nsnap][nshots][ncomp][nxyz]; FP16P: 3-slot decode ring
+    DevBuf snapq_;                 // FP16P: second-difference residuals [nsnap][nshots][ncomp][nxyz] (half)
+    DevBuf snaps_scale_;           // FP16P: residual scales [nsnap][nshots*ncomp] (float)
+    DevBuf enc_;                   // FP16P: encoder/decoder state, two FP64 levels [2][nshots][ncomp][nxyz]
+    DevBuf amax_;                  // FP16P: per (shot, comp) max |residual| of one snapshot
+    DevBuf snapz_;                 // FP16P: zero snapshot (indices past the last forward state)
+    int storage_ = STORE_FP32;
     int nsnap_ = 0;
+    int nwritten_ = 0;             // snapshots 0..nwritten_-1 hold forward states, the rest are zero
+    int dec_lo_ = 0;               // FP16P decoder: state holds snapshots dec_lo_, dec_lo_+1
+    void snap_store(int k);
+    const float *snap_fp32(int kk);  // FP32 view of snapshot kk (decoding as needed)
     bool snaps_valid_ = false;
     DevBuf grad_;                  // [3][nxyz] double
     DevBuf sdiv_;                  // boundary divisors, packed

@@ -78,6 +78,7 @@ def to_cparam(p: Param) -> _lib.CParam:
     c.epsilonmin, c.epsilonmax = p.epsilonmin, p.epsilonmax
     c.gammamin, c.gammamax = p.gammamin, p.gammamax
     c.soft_clip, c.verbose = int(bool(p.soft_clip)), p.verbose
+    c.snapshot_storage = int(getattr(p, "snapshot_storage", 0))
     return c
 
 
@@ -227,3 +228,65 @@ def forward_batch(sv, device: int = 0) -> np.ndarray:
                                      _lib.fptr(w), ncomp, w.shape[-1], sv.dt_data, ns, _lib.fptr(sx), nr,
                                      _lib.fptr(rx), _lib.fptr(out)))
     return out
+
+
+class FwiObjective:
+    """FWI objective of all shots of a survey on the device (the reference's
+    nlls_fwi, optimization.cpp:5-197): ``evaluate(model)`` returns the misfit
+    (FP64), the gradient in the model's parametrisation and the residuals.
+
+    ``batch`` shots advance in lockstep per launch; ``sv.par.snapshot_storage``
+    selects FP32 or FP16 second-difference snapshot storage."""
+
+    def __init__(self, sv, observed: np.ndarray, normalize: bool = True, batch: Optional[int] = None,
+                 device: int = 0):
+        lib = _lib.load()
+        self.sv = sv
+        self.ns = len(sv.par.sxyz)
+        self.nr = len(sv.par.rxyz[0])
+        if any(len(r) != self.nr for r in sv.par.rxyz):
+            raise _lib.FwiError(_lib.FWI_ERR_ARG, "every shot needs the same receiver count")
+        self.nm = min(3, sv.nmodels)
+        w = np.ascontiguousarray(sv.wavelet, dtype=np.float32)
+        ncomp = 1 if w.ndim == 1 else w.shape[0]
+        self.nt_data = w.shape[-1]
+        self.nrcomp = 1 if sv.nmodels == 2 else 3
+        obs = np.ascontiguousarray(observed, dtype=np.float32)
+        if obs.size != self.ns * self.nrcomp * self.nr * self.nt_data:
+            raise _lib.FwiError(_lib.FWI_ERR_ARG, f"observed data of shape {obs.shape} do not match the survey")
+        sx = np.ascontiguousarray(np.asarray(sv.par.sxyz, dtype=np.float32)[:, :3])
+        rx = np.ascontiguousarray(np.asarray(sv.par.rxyz, dtype=np.float32).reshape(self.ns, self.nr, 5))
+        dom = Domain(sv.nx, sv.ny, sv.nz, sv.dx, sv.dy, sv.dz, sv.nmodels, sv.ox, sv.oy, sv.oz)
+        self.shape = dom.shape
+        cp = to_cparam(sv.par)
+        h = C.c_void_p()
+        _lib.check(lib.fwi_objective_create(C.byref(h), device, C.byref(dom.grid()), sv.nmodels, C.byref(cp),
+                                            _lib.fptr(w), ncomp, self.nt_data, sv.dt_data, self.ns, _lib.fptr(sx),
+                                            self.nr, _lib.fptr(rx), _lib.fptr(obs), int(bool(normalize)),
+                                            int(batch or self.ns)))
+        self._h = h
+
+    def evaluate(self, model: np.ndarray, want_residual: bool = False):
+        m = np.ascontiguousarray(model, dtype=np.float32)
+        if m.size != int(np.prod(self.shape)):
+            raise _lib.FwiError(_lib.FWI_ERR_ARG, f"model of shape {m.shape}, expected {self.shape}")
+        g = np.zeros((self.nm,) + tuple(self.shape[1:]), dtype=np.float32)
+        r = np.zeros((self.ns, self.nrcomp, self.nr, self.nt_data), dtype=np.float32) if want_residual else None
+        f = C.c_double()
+        _lib.check(_lib.load().fwi_objective_evaluate(self._h, _lib.fptr(m), C.byref(f), _lib.fptr(g),
+                                                      _lib.fptr(r) if r is not None else None))
+        return (f.value, g, r) if want_residual else (f.value, g)
+
+    def device_bytes(self) -> int:
+        return int(_lib.load().fwi_objective_device_bytes(self._h))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.load().fwi_objective_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -89,6 +89,10 @@ class Param:
     nthreads: int = 0
     verbose: int = 0
 
+    # gradient snapshot storage (no reference counterpart): 0 FP32, 1 FP16
+    # second-difference residuals with per-snapshot scales
+    snapshot_storage: int = 0
+
     def copy(self) -> "Param":
         return copy.deepcopy(self)
 

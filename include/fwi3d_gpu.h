@@ -71,6 +71,8 @@ typedef struct fwi_param {
     float deltamin, deltamax, epsilonmin, epsilonmax, gammamin, gammamax;
     int soft_clip;
     int verbose;
+    int snapshot_storage;     /* gradient snapshots: 0 FP32 (as the reference), 1 FP16 second-difference
+                                 residuals with per-snapshot scales (half the memory); no reference counterpart */
 } fwi_param;
 
 void fwi_param_default(fwi_param *p);
@@ -157,6 +159,31 @@ void fwi_batch_destroy(fwi_batch *b);
  * in time (other streams, other threads) race: serialise them. */
 int fwi_elastic_step_static(const fwi_grid *grid, int nmodels, const int *bc, float dt, const float *model,
                             const float *prev, const float *curr, float *next, void *stream);
+
+/* Full-waveform-inversion objective of a shot gather on the device: the
+ * nlls_fwi objective of the reference (src/cpp/optimization.cpp:5-197,
+ * src/include/optimization.hpp:403-430) without data weights, filters,
+ * envelopes or source scaling.  Shots are processed `batch` at a time in
+ * lockstep; per evaluation
+ *   f    = 0.5 dt_data (sum r^2 - 0.5 sum_traces (r_0^2 + r_{nt-1}^2)) / dnorm,
+ *   grad = J^T Ht(r) summed over shots / dnorm, in (vp, vs, rho) like jacobianT,
+ * with r = synthetic - observed, dnorm = dt_data |observed|^2 when `normalize`
+ * (else 1).  Misfit and gradient sums are FP64 (the reference sums in data_t);
+ * the gradient is the sum of the per-shot gradients (the reference's
+ * apply_jacobianT(add=true) chaining, we_op.cpp:968-972 and 1069-1075, also
+ * passes the earlier shots' sum through H and the chain rule again; the
+ * per-shot operator path above reproduces that when a caller needs it).
+ * observed: [nshots][nrcomp][nr][nt_data]; residual (optional, may be null):
+ * same layout; grad: [min(3,nmodels)][ny][nx][nz]. */
+typedef struct fwi_objective fwi_objective;
+int fwi_objective_create(fwi_objective **o, int device, const fwi_grid *grid, int nmodels, const fwi_param *par,
+                         const float *wavelet, int wavelet_ncomp, int nt_data, float dt_data, int nshots,
+                         const float *sxyz, int nr, const float *rxyz, const float *observed, int normalize,
+                         int batch);
+int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, float *grad, float *residual);
+/* Device bytes of the last evaluation (wavefields, snapshots, model, tables). */
+int64_t fwi_objective_device_bytes(const fwi_objective *o);
+void fwi_objective_destroy(fwi_objective *o);
 
 /* Message of the last failing call on this thread. */
 const char *fwi_last_error(void);
