@@ -104,6 +104,7 @@ struct fwi_op {
         pb = p;
         if (!same) eng.reset(new Engine(device, pb));
         eng->set_storage(par.snapshot_storage);
+        eng->set_snapshot_budget((int64_t)((double)par.snapshot_budget_gb * 1e9));
         eng->set_model(m.data());
         conv.swap(m);
     }
@@ -179,6 +180,7 @@ void fwi_param_default(fwi_param *p)
     p->soft_clip = 0;
     p->verbose = 0;
     p->snapshot_storage = 0;
+    p->snapshot_budget_gb = 0.f;
 }
 
 const char *fwi_last_error(void) { return g_err.c_str(); }
@@ -621,6 +623,7 @@ int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, floa
             const bool same = eng && o->pb.nt == p.nt && o->pb.dt == p.dt && o->pb.sub == p.sub;
             if (!same) eng.reset(new Engine(o->device, p));
             eng->set_storage(par.snapshot_storage);
+            eng->set_snapshot_budget((int64_t)((double)par.snapshot_budget_gb * 1e9));
             eng->set_model(m.data());
             // tables of the batch (shot b of the batch at wavefield offset b)
             InjTable inj, adj;

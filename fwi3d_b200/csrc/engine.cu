@@ -784,7 +784,7 @@ void Engine::reset()
 void Engine::run(int it0, int nsteps)
 {
     for (int it = it0; it < it0 + nsteps && it < pb_.nt - 1; it++) {
-        extract(ext_, level(1), rcv_dev_.as<float>(), it);
+        if (!no_extract_) extract(ext_, level(1), rcv_dev_.as<float>(), it);
         step(level(0), level(1), level(2), it > 0);
         inject(inj_, src_dev_.as<float>(), it, level(2));
         rot_ = (rot_ + 1) % 3;
@@ -887,6 +887,16 @@ void Engine::snap_store(int k)
     const int nsc = pb_.nshots * pb_.ncomp();
     if (k > nsnap_ - 1) return;
     nwritten_ = std::max(nwritten_, k + 1);
+    if (seg_L_ > 0) {
+        // checkpoint j holds (prev, curr) at snapshot ckpt_index(j)
+        const int j = k == 0 ? 0 : ((k + 1) % seg_L_ == 0 ? (k + 1) / seg_L_ : -1);
+        if (j >= 0 && j < nseg_) {
+            float *c = ckpt_.as<float>() + (int64_t)j * 2 * nsc * n;
+            CK(cudaMemcpyAsync(c, level(0), sizeof(float) * nsc * n, cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(c + (int64_t)nsc * n, level(1), sizeof(float) * nsc * n, cudaMemcpyDeviceToDevice, s));
+        }
+        return;
+    }
     if (storage_ == STORE_FP32) {
         CK(cudaMemcpyAsync(snaps_.as<float>() + (int64_t)k * nsc * n, level(1), sizeof(float) * nsc * n,
                            cudaMemcpyDeviceToDevice, s));
@@ -904,6 +914,10 @@ const float *Engine::snap_fp32(int kk)
 {
     const int64_t n = pb_.nxyz();
     const int nsc = pb_.nshots * pb_.ncomp();
+    if (seg_L_ > 0) {
+        if (kk >= nwritten_) return snapz_.as<float>();
+        return snaps_.as<float>() + (int64_t)(kk - seg_lo_) * nsc * n;
+    }
     if (storage_ == STORE_FP32) return snaps_.as<float>() + (int64_t)kk * nsc * n;
     if (kk >= nwritten_) return snapz_.as<float>();
     cudaStream_t s = (cudaStream_t)stream_;
@@ -920,6 +934,40 @@ const float *Engine::snap_fp32(int kk)
     return snaps_.as<float>() + (int64_t)(kk % 3) * nsc * n;
 }
 
+// Forward snapshots of segment j (indices ckpt_index(j) .. min((j+1)L, last))
+// recomputed from its checkpoint on the recomputation levels; the adjoint's
+// own levels are swapped out meanwhile.
+void Engine::recompute_segment(int j)
+{
+    cudaStream_t s = (cudaStream_t)stream_;
+    const int64_t n = pb_.nxyz();
+    const int nsc = pb_.nshots * pb_.ncomp();
+    const int64_t S = (int64_t)nsc * n;
+    const int lo = ckpt_index(j);
+    const int hi = std::min((j + 1) * seg_L_, nwritten_ - 1);
+    std::swap(fields_, rec_fields_);
+    const int rot_save = rot_;
+    rot_ = 0;
+    const float *c = ckpt_.as<float>() + (int64_t)j * 2 * S;
+    CK(cudaMemcpyAsync(level(0), c, sizeof(float) * S, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(level(1), c + S, sizeof(float) * S, cudaMemcpyDeviceToDevice, s));
+    no_extract_ = true;
+    auto keep = [&](int k) {
+        CK(cudaMemcpyAsync(snaps_.as<float>() + (int64_t)(k - lo) * S, level(1), sizeof(float) * S,
+                           cudaMemcpyDeviceToDevice, s));
+    };
+    for (int it = lo * pb_.sub; it < hi * pb_.sub; it++) {
+        if (it % pb_.sub == 0) keep(it / pb_.sub);
+        run(it, 1);
+    }
+    keep(hi);
+    no_extract_ = false;
+    rot_ = rot_save;
+    std::swap(fields_, rec_fields_);
+    seg_cur_ = j;
+    seg_lo_ = lo;
+}
+
 void Engine::forward(const InjTable &inj, int ntrace, const float *src, const ExtTable &ext, float *rcv, bool store)
 {
     CK(cudaSetDevice(device_));
@@ -931,12 +979,44 @@ void Engine::forward(const InjTable &inj, int ntrace, const float *src, const Ex
     snaps_valid_ = false;
     nwritten_ = 0;
     const bool keep = store && pb_.sub > 0;
+    seg_L_ = 0;
+    seg_cur_ = -1;
     if (keep) {
         nsnap_ = 1 + pb_.nt / pb_.sub;
         // FP16P needs at least three stored snapshots to decode backwards
         const int written = 1 + (pb_.nt - 1) / pb_.sub;
         if (storage_ == STORE_FP16P && written < 3) storage_ = STORE_FP32;
-        if (storage_ == STORE_FP32) {
+        const int64_t S = (int64_t)sizeof(float) * nsc * n;  // one snapshot of the batch
+        const int64_t full = storage_ == STORE_FP32 ? nsnap_ * S : nsnap_ * S / 2 + 8 * S;
+        if (budget_ > 0 && full > budget_) {
+            // segments of L snapshots: nseg FP32 checkpoints (2 levels), an
+            // (L+2)-snapshot buffer, recomputation levels and a zero snapshot
+            int bestL = 0;
+            int64_t best = 0;
+            for (int L = 2; L <= written; L++) {
+                const int ns = (written + L - 1) / L;
+                const int64_t mem = (2 * (int64_t)ns + L + 2 + 3 + 1) * S;
+                if (bestL == 0 || mem < best) {
+                    best = mem;
+                    bestL = L;
+                }
+            }
+            if (best > budget_)
+                throw FwiError(FWI_ERR_OOM, "snapshot budget of " + std::to_string(budget_) +
+                                                " bytes is below the checkpointing minimum of " + std::to_string(best));
+            seg_L_ = bestL;
+            nseg_ = (written + bestL - 1) / bestL;
+            snapq_.alloc(0);
+            snaps_scale_.alloc(0);
+            enc_.alloc(0);
+            ckpt_.alloc((size_t)nseg_ * 2 * S);
+            rec_fields_.alloc(3 * (size_t)S);
+            snaps_.alloc((size_t)(seg_L_ + 2) * S);
+            snapz_.alloc((size_t)S);
+            snapz_.zero(s);
+        } else if (storage_ == STORE_FP32) {
+            ckpt_.alloc(0);
+            rec_fields_.alloc(0);
             snapq_.alloc(0);
             snaps_scale_.alloc(0);
             enc_.alloc(0);
@@ -944,6 +1024,8 @@ void Engine::forward(const InjTable &inj, int ntrace, const float *src, const Ex
             snaps_.alloc(sizeof(float) * (size_t)nsnap_ * nsc * n);
             snaps_.zero(s);
         } else {
+            ckpt_.alloc(0);
+            rec_fields_.alloc(0);
             snaps_.alloc(sizeof(float) * 3 * (size_t)nsc * n);
             snapq_.alloc(sizeof(__half) * (size_t)nsnap_ * nsc * n);
             snaps_scale_.alloc(sizeof(float) * (size_t)nsnap_ * nsc);
@@ -960,7 +1042,7 @@ void Engine::forward(const InjTable &inj, int ntrace, const float *src, const Ex
         run(it, 1);
     }
     if (keep && (pb_.nt - 1) % pb_.sub == 0) snap_store((pb_.nt - 1) / pb_.sub);
-    if (keep && storage_ == STORE_FP16P) {
+    if (keep && seg_L_ == 0 && storage_ == STORE_FP16P) {
         // decoder starts from the encoder's final state (e_K, e_{K-1})
         const int K = nwritten_ - 1;
         const double *e = enc_.as<double>();
@@ -991,6 +1073,10 @@ void Engine::image(int itl, const float *curr, const float *prevl)
     a.itl = itl;
     a.last = pb_.nt / pb_.sub;
     for (int k = 0; k < pb_.nmodels; k++) a.m[k] = model_.as<float>() + k * n;
+    if (seg_L_ > 0) {
+        const int j = std::min(itl / seg_L_, nseg_ - 1);
+        if (j != seg_cur_) recompute_segment(j);
+    }
     const float *lev[3];
     for (int l = 0; l < 3; l++) {
         const int k = itl - 1 + l;
@@ -1043,7 +1129,8 @@ void Engine::adjoint(const InjTable &inj, int ntrace, const float *adj_src, floa
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(grad, gf.p, gf.bytes, cudaMemcpyDeviceToHost, s));
     sync();
-    snaps_valid_ = storage_ == STORE_FP32;  // the FP16P decoder state is consumed
+    snaps_valid_ = seg_L_ > 0 || storage_ == STORE_FP32;  // the FP16P decoder state is consumed
+    seg_cur_ = -1;
 }
 
 // ---------------------------------------------------------------------------

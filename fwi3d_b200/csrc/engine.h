@@ -92,13 +92,19 @@ public:
     // Snapshot storage of the forward wavefield for the imaging condition.
     enum Storage { STORE_FP32 = 0, STORE_FP16P = 1 };
     void set_storage(int mode) { storage_ = mode; }
+    // HBM budget of the forward-wavefield storage of the gradient path (bytes,
+    // 0: unlimited).  When full storage exceeds it, the forward keeps FP32
+    // checkpoints every L snapshots and the adjoint recomputes one segment of
+    // snapshots at a time from them (one extra forward propagation).
+    void set_snapshot_budget(int64_t bytes) { budget_ = bytes; }
+    int checkpoint_segment() const { return seg_L_; }  // 0: full storage
     // forward: full time loop; keeps snapshots when store && sub > 0.  Tables of
     // all shots (as set_sources/set_receivers); rcv [nshots][ncomp][nr][nt].
     void forward(const InjTable &inj, int ntrace, const float *src, const ExtTable &ext, float *rcv, bool store);
     // adjoint + imaging of every shot of the batch; grad out: [min(3,nm)][nxyz]
     // float, summed over the shots in FP64 (before H quadrature and chain rule)
     void adjoint(const InjTable &inj, int ntrace, const float *adj_src, float *grad);
-    int64_t snapshot_bytes() const { return snaps_.bytes + snapq_.bytes + enc_.bytes + snapz_.bytes; }
+    int64_t snapshot_bytes() const { return snaps_.bytes + snapq_.bytes + enc_.bytes + snapz_.bytes + ckpt_.bytes + rec_fields_.bytes; }
 
     // Diagnostic timing of the step's main kernel (the fused interior kernel,
     // else the per-point step kernel): a pair of CUDA events on the engine
@@ -139,6 +145,16 @@ private:
     int nwritten_ = 0;             // snapshots 0..nwritten_-1 hold forward states, the rest are zero
     int dec_lo_ = 0;               // FP16P decoder: state holds snapshots dec_lo_, dec_lo_+1
     void snap_store(int k);
+    int64_t budget_ = 0;
+    int seg_L_ = 0;                // checkpointing: snapshots per segment (0: full storage)
+    int nseg_ = 0;
+    int seg_cur_ = -1;             // segment held in snaps_ (snapshots seg_lo_ .. seg_lo_ + L + 1)
+    int seg_lo_ = 0;
+    DevBuf ckpt_;                  // [nseg][2][nshots][ncomp][nxyz] (prev, curr) at each segment start
+    DevBuf rec_fields_;            // time levels of the recomputation
+    bool no_extract_ = false;
+    int ckpt_index(int j) const { return j == 0 ? 0 : j * seg_L_ - 1; }
+    void recompute_segment(int j);
     const float *snap_fp32(int kk);  // FP32 view of snapshot kk (decoding as needed)
     bool snaps_valid_ = false;
     DevBuf grad_;                  // [3][nxyz] double

@@ -79,6 +79,7 @@ def to_cparam(p: Param) -> _lib.CParam:
     c.gammamin, c.gammamax = p.gammamin, p.gammamax
     c.soft_clip, c.verbose = int(bool(p.soft_clip)), p.verbose
     c.snapshot_storage = int(getattr(p, "snapshot_storage", 0))
+    c.snapshot_budget_gb = float(getattr(p, "snapshot_budget_gb", 0.0))
     return c
 
 

@@ -92,6 +92,9 @@ class Param:
     # gradient snapshot storage (no reference counterpart): 0 FP32, 1 FP16
     # second-difference residuals with per-snapshot scales
     snapshot_storage: int = 0
+    # HBM budget of that storage in GB (0: unlimited); above it, checkpoints
+    # and segment recomputation
+    snapshot_budget_gb: float = 0.0
 
     def copy(self) -> "Param":
         return copy.deepcopy(self)

@@ -73,6 +73,8 @@ typedef struct fwi_param {
     int verbose;
     int snapshot_storage;     /* gradient snapshots: 0 FP32 (as the reference), 1 FP16 second-difference
                                  residuals with per-snapshot scales (half the memory); no reference counterpart */
+    float snapshot_budget_gb; /* HBM budget of the gradient's forward-wavefield storage (0: unlimited); above it
+                                 FP32 checkpoints + segment recomputation replace full storage */
 } fwi_param;
 
 void fwi_param_default(fwi_param *p);
