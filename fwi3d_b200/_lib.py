@@ -11,7 +11,8 @@ import os
 from typing import Optional
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libfwi3d_b200.so")
+# FWI3D_B200_LIB points at another build of the library (e.g. an instrumented one)
+LIB_PATH = os.environ.get("FWI3D_B200_LIB") or os.path.join(HERE, "libfwi3d_b200.so")
 
 FWI_OK = 0
 FWI_ERR_ARG = -1

@@ -125,6 +125,30 @@ __global__ void k_elastic_step(StepArgs a)
     b.next[2][i] = v2;
 }
 
+template <int PH, bool F>
+__device__ __forceinline__ void fused_march(FusedCtx &c, int tid, int ya, int yb)
+{
+    FusedThread th;
+#pragma unroll
+    for (int k = 0; k < 5; k++) th.qmu[k] = th.qeps[k] = th.q66[k] = th.qT[k] = th.qX1[k] = th.qZ1[k] = 0.f;
+    fz_prologue<PH>(c, tid, ya);
+    __syncthreads();
+    for (int y = ya - 4; y < yb; y++) {
+        fz_slots(c, y);
+        fz_load_u(c, tid, y + 4, c.sl[6]);
+        if (y >= ya) fz_load_mat<PH>(c, tid, y);
+        __syncthreads();
+        fz_column<PH, F>(c, th, tid, y + 2);
+        if (y >= ya) fz_derived<PH, F>(c, tid, y);
+        __syncthreads();
+        if (y >= ya) {
+            if (F) fz_output_fast<PH>(c, th, tid, y);
+            else fz_output<PH>(c, th, tid, y);
+        }
+        __syncthreads();
+    }
+}
+
 // Fused elastic step over planes [ylo, yhi) (see fused.cuh).  grid: (z tiles,
 // x tiles, y chunks x shots), block (TZ, TX).
 template <int PH, int MINB>
@@ -144,22 +168,11 @@ __global__ void __launch_bounds__(fz::NT, MINB) k_elastic_fused(const __grid_con
     const int ya = a.y0 + (int)((int64_t)len * ch / nchunks);
     const int yb = a.y0 + (int)((int64_t)len * (ch + 1) / nchunks);
     if (ya >= yb) return;
-    FusedThread th;
-#pragma unroll
-    for (int k = 0; k < 5; k++) th.qmu[k] = th.qeps[k] = th.q66[k] = th.qT[k] = th.qX1[k] = th.qZ1[k] = 0.f;
-    fz_prologue<PH>(c, tid, ya);
-    __syncthreads();
-    for (int y = ya - 4; y < yb; y++) {
-        fz_slots(c, y);
-        fz_load_u(c, tid, y + 4, c.sl[6]);
-        if (y >= ya) fz_load_mat<PH>(c, tid, y);
-        __syncthreads();
-        fz_column<PH>(c, th, tid, y + 2);
-        if (y >= ya) fz_derived<PH>(c, tid, y);
-        __syncthreads();
-        if (y >= ya) fz_output<PH>(c, th, tid, y);
-        __syncthreads();
-    }
+    // tiles whose outputs and derived halo are interior in x and z take the
+    // closure-free code (block-uniform branch)
+    const bool fast = c.x0 >= 6 && c.x0 + fz::TX <= a.g.nx - 6 && c.z0 >= 6 && c.z0 + fz::TZ <= a.g.nz - 6;
+    if (fast) fused_march<PH, true>(c, tid, ya, yb);
+    else fused_march<PH, false>(c, tid, ya, yb);
 }
 
 // Marching elastic step over every plane (see march.cuh).  grid: (z tiles,
@@ -413,7 +426,8 @@ void Engine::sync() { CK(cudaStreamSynchronize((cudaStream_t)stream_)); }
 int64_t Engine::device_bytes() const
 {
     return model_.bytes + fields_.bytes + aux_.bytes + snaps_.bytes + grad_.bytes + sdiv_.bytes + taper_.bytes +
-           src_dev_.bytes + rcv_dev_.bytes;
+           src_dev_.bytes + rcv_dev_.bytes + snapq_.bytes + snaps_scale_.bytes + enc_.bytes + amax_.bytes +
+           snapz_.bytes + ckpt_.bytes + rec_fields_.bytes;
 }
 
 float *Engine::level(int l) const

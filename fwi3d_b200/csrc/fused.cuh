@@ -158,11 +158,12 @@ FWI_HD float d1_sg(const S &s, int i, int n)
 
 // First derivatives of displacement component k at (ix, q, iz) along x, y, z
 // from the ring (with the 1/h).  ixw/izw: smem coordinates in the ring window.
+template <bool F = false>
 FWI_HD float fz_dx(const FusedCtx &c, int k, int slot, int ix, int izw)
 {
     const float *p = &c.sm->u[slot][k][0][izw];
     const int j = ix - (c.x0 - fz::HW);
-    if (ix >= 4 && ix < c.a->g.nx - 4) {
+    if (F || (ix >= 4 && ix < c.a->g.nx - 4)) {
         const SbpTables &t = sbp();
         return (t.d1c0 * (p[(j + 1) * fz::ZW] - p[(j - 1) * fz::ZW]) + t.d1c1 * (p[(j + 2) * fz::ZW] - p[(j - 2) * fz::ZW])) *
                c.a->idx;
@@ -170,11 +171,12 @@ FWI_HD float fz_dx(const FusedCtx &c, int k, int slot, int ix, int izw)
     const SXc s{p, c.x0 - fz::HW, fz::ZW, fz::XW};
     return d1_row(s, ix, c.a->g.nx) * c.a->idx;
 }
+template <bool F = false>
 FWI_HD float fz_dz(const FusedCtx &c, int k, int slot, int ixw, int iz)
 {
     const float *p = &c.sm->u[slot][k][ixw][0];
     const int j = iz - (c.z0 - fz::HW);
-    if (iz >= 4 && iz < c.a->g.nz - 4) {
+    if (F || (iz >= 4 && iz < c.a->g.nz - 4)) {
         const SbpTables &t = sbp();
         return (t.d1c0 * (p[j + 1] - p[j - 1]) + t.d1c1 * (p[j + 2] - p[j - 2])) * c.a->idz;
     }
@@ -194,7 +196,7 @@ FWI_HD float fz_dy(const FusedCtx &c, int k, const int *sn, int ixw, int izw)
 // ---------------------------------------------------------------------------
 // Phase B1: derived quantities of plane y over the derived region.
 // ---------------------------------------------------------------------------
-template <int PH>
+template <int PH, bool F = false>
 FWI_HD void fz_derived(FusedCtx &c, int tid, int y)
 {
     const Dims &g = c.a->g;
@@ -203,20 +205,20 @@ FWI_HD void fz_derived(FusedCtx &c, int tid, int y)
         const int ix = c.x0 - fz::HD + xh, iz = c.z0 - fz::HD + zh;
         float *dv0 = &c.sm->dv[0][xh][zh];
         const int stride = fz::XH * fz::ZH;
-        if (ix < 0 || ix >= g.nx || iz < 0 || iz >= g.nz) {
+        if (!F && (ix < 0 || ix >= g.nx || iz < 0 || iz >= g.nz)) {
             for (int k = 0; k < NDV; k++) dv0[k * stride] = 0.f;
             continue;
         }
         const int ixw = xh + (fz::HW - fz::HD), izw = zh + (fz::HW - fz::HD);
         const int s0 = c.sl[2];
         const int sn[4] = {c.sl[0], c.sl[1], c.sl[3], c.sl[4]};
-        const float ux0 = fz_dx(c, 0, s0, ix, izw);
+        const float ux0 = fz_dx<F>(c, 0, s0, ix, izw);
         const float uy1 = fz_dy(c, 1, sn, ixw, izw);
-        const float uz2 = fz_dz(c, 2, s0, ixw, iz);
+        const float uz2 = fz_dz<F>(c, 2, s0, ixw, iz);
         const float mu = c.sm->mp[MP_MU][xh][zh], lam = c.sm->mp[MP_LAM][xh][zh];
         const float uy0 = fz_dy(c, 0, sn, ixw, izw);
-        const float uz0 = fz_dz(c, 0, s0, ixw, iz);
-        const float ux2 = fz_dx(c, 2, s0, ix, izw);
+        const float uz0 = fz_dz<F>(c, 0, s0, ixw, iz);
+        const float ux2 = fz_dx<F>(c, 2, s0, ix, izw);
         const float uy2 = fz_dy(c, 2, sn, ixw, izw);
         if (PH == ELASTIC) {
             const float T = lam * (ux0 + uy1 + uz2);
@@ -239,7 +241,7 @@ FWI_HD void fz_derived(FusedCtx &c, int tid, int y)
 }
 
 // Phase B2: own-column quantities of plane q = y+2 pushed into the y queues.
-template <int PH>
+template <int PH, bool F = false>
 FWI_HD void fz_column(FusedCtx &c, FusedThread &th, int tid, int q)
 {
     const Dims &g = c.a->g;
@@ -264,11 +266,11 @@ FWI_HD void fz_column(FusedCtx &c, FusedThread &th, int tid, int q)
     // plane q = y+2 sits in slot sl[4]; its neighbours q-2..q+2 in sl[2..6]
     const int s0 = c.sl[4];
     const int sn[4] = {c.sl[2], c.sl[3], c.sl[5], c.sl[6]};
-    const float ux0 = fz_dx(c, 0, s0, ix, izw);
+    const float ux0 = fz_dx<F>(c, 0, s0, ix, izw);
     const float uy1 = fz_dy(c, 1, sn, ixw, izw);
-    const float uz2 = fz_dz(c, 2, s0, ixw, iz);
-    const float ux1 = fz_dx(c, 1, s0, ix, izw);
-    const float uz1 = fz_dz(c, 1, s0, ixw, iz);
+    const float uz2 = fz_dz<F>(c, 2, s0, ixw, iz);
+    const float ux1 = fz_dx<F>(c, 1, s0, ix, izw);
+    const float uz1 = fz_dz<F>(c, 1, s0, ixw, iz);
     if (PH == ELASTIC) {
         th.qT[4] = lam * (ux0 + uy1 + uz2);
         th.qX1[4] = ux1;
@@ -470,6 +472,96 @@ FWI_HD void fz_output(FusedCtx &c, const FusedThread &th, int tid, int y)
         const float pe = (a.taper_prev && tz) ? taper(a, p, ix, y, iz) : p;
         v = dt2 * v * irho + 2.f * s.u[r0][k][ixw][izw] - pe;
         if (face) v = boundary_scale(a, v, k, ix, y, iz);
+        if (tz) v = taper(a, v, ix, y, iz);
+        a.next[k][c.so + i] = v;
+    }
+}
+
+// Output phase of a tile whose outputs and derived halo are all interior in x
+// and z (every stencil is the interior one): same terms as fz_output, taps
+// read at constant offsets from per-point base pointers.
+template <int PH>
+FWI_HD void fz_output_fast(FusedCtx &c, const FusedThread &th, int tid, int y)
+{
+    const StepArgs &a = *c.a;
+    const Dims &g = a.g;
+    const int lz = tid % fz::TZ, lx = tid / fz::TZ;
+    const int ix = c.x0 + lx, iz = c.z0 + lz;
+    if (ix >= c.xend || iz >= c.zend) return;
+    const int64_t i = g.idx(ix, y, iz);
+    const int ixw = lx + fz::HW, izw = lz + fz::HW;
+    const int xh = lx + fz::HD, zh = lz + fz::HD;
+    FusedSmem &s = *c.sm;
+    constexpr int UX = fz::ZW, UC = fz::XW * fz::ZW, US = 3 * fz::XW * fz::ZW, DX = fz::ZH;
+    const float *ub = &s.u[0][0][ixw][izw];
+    const int r0 = c.sl[2] * US, rm1 = c.sl[1] * US, rm2 = c.sl[0] * US, rp1 = c.sl[3] * US, rp2 = c.sl[4] * US;
+    const float *mu = &s.mp[MP_MU][xh][zh];
+    const float idx2 = a.ad1[0], idy2 = a.ad1[1];
+    float acc[3];
+    const W5 wxm = d2w(mu[-2 * DX], mu[-DX], mu[0], mu[DX], mu[2 * DX]);
+    const W5 wz = d2w(mu[-2], mu[-1], mu[0], mu[1], mu[2]);
+    const W5 wym = d2w(th.qmu[0], th.qmu[1], th.qmu[2], th.qmu[3], th.qmu[4]);
+    if (PH == ELASTIC) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const float adx = k == 0 ? a.ad2[0] : a.ad1[0];
+            const float ady = k == 1 ? a.ad2[1] : a.ad1[1];
+            const float adz = k == 2 ? a.ad2[2] : a.ad1[2];
+            const float *u = ub + k * UC + r0;
+            const float *uc = ub + k * UC;
+            float v = d2apply(wxm, adx, u[-2 * UX], u[-UX], u[0], u[UX], u[2 * UX]);
+            v += d2apply(wym, ady, uc[rm2], uc[rm1], u[0], uc[rp1], uc[rp2]);
+            v += d2apply(wz, adz, u[-2], u[-1], u[0], u[1], u[2]);
+            acc[k] = v;
+        }
+    } else {
+        const float *ep = &s.mp[MP_EPS][xh][zh], *c6 = &s.mp[MP_C66][xh][zh];
+        auto c11b = [&](int o) { return 2.f * (1.f + 2.f * ep[o]) * mu[o]; };
+        const W5 wxb = d2w(c11b(-2 * DX), c11b(-DX), c11b(0), c11b(DX), c11b(2 * DX));
+        const W5 wx6 = d2w(c6[-2 * DX], c6[-DX], c6[0], c6[DX], c6[2 * DX]);
+        float qb[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++) qb[k] = 2.f * (1.f + 2.f * th.qeps[k]) * th.qmu[k];
+        const W5 wyb = d2w(qb[0], qb[1], qb[2], qb[3], qb[4]);
+        const W5 wy6 = d2w(th.q66[0], th.q66[1], th.q66[2], th.q66[3], th.q66[4]);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const W5 &wx = k == 0 ? wxb : (k == 1 ? wx6 : wxm);
+            const W5 &wy = k == 0 ? wy6 : (k == 1 ? wyb : wym);
+            const float adz = k == 2 ? a.ad2[2] : a.ad1[2];
+            const float *u = ub + k * UC + r0;
+            const float *uc = ub + k * UC;
+            float v = d2apply(wx, idx2, u[-2 * UX], u[-UX], u[0], u[UX], u[2 * UX]);
+            v += d2apply(wy, idy2, uc[rm2], uc[rm1], u[0], uc[rp1], uc[rp2]);
+            v += d2apply(wz, adz, u[-2], u[-1], u[0], u[1], u[2]);
+            acc[k] = v;
+        }
+    }
+    // D1 of the stress combinations and the mixed terms (we_op.cpp:661-688, 1312-1349)
+    const float *P = (PH == VTI) ? &s.mp[MP_C66][xh][zh] : mu;
+    const float *qP = (PH == VTI) ? th.q66 : th.qmu;
+    const float *t0 = &s.dv[DV_T0][xh][zh], *t2 = &s.dv[DV_T2][xh][zh];
+    const float *x2 = &s.dv[DV_X2][xh][zh], *y0 = &s.dv[DV_Y0][xh][zh];
+    const float *y2 = &s.dv[DV_Y2][xh][zh], *z0 = &s.dv[DV_Z0][xh][zh];
+    acc[0] += d1i(t0[-2 * DX], t0[-DX], t0[DX], t0[2 * DX]) * a.idx;
+    acc[0] += d1m(th.qX1[0], qP[0], th.qX1[1], qP[1], th.qX1[3], qP[3], th.qX1[4], qP[4]) * a.idy;
+    acc[0] += d1m(x2[-2], mu[-2], x2[-1], mu[-1], x2[1], mu[1], x2[2], mu[2]) * a.idy;  // dy as the reference
+    acc[1] += d1i(th.qT[0], th.qT[1], th.qT[3], th.qT[4]) * a.idy;
+    acc[1] += d1m(y0[-2 * DX], P[-2 * DX], y0[-DX], P[-DX], y0[DX], P[DX], y0[2 * DX], P[2 * DX]) * a.idx;
+    acc[1] += d1m(y2[-2], mu[-2], y2[-1], mu[-1], y2[1], mu[1], y2[2], mu[2]) * a.idz;
+    acc[2] += d1i(t2[-2], t2[-1], t2[1], t2[2]) * a.idz;
+    acc[2] += d1m(z0[-2 * DX], mu[-2 * DX], z0[-DX], mu[-DX], z0[DX], mu[DX], z0[2 * DX], mu[2 * DX]) * a.idx;
+    acc[2] += d1m(th.qZ1[0], th.qmu[0], th.qZ1[1], th.qmu[1], th.qZ1[3], th.qmu[3], th.qZ1[4], th.qmu[4]) * a.idy;
+
+    // update, taper (no boundary face in a fast tile; SAT is added by the face kernel)
+    const float dt2 = a.dt * a.dt;
+    const float irho = 1.0f / a.m[2][i];
+    const bool tz = in_taper(a, ix, y, iz);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float p = a.prev[k][c.so + i];
+        const float pe = (a.taper_prev && tz) ? taper(a, p, ix, y, iz) : p;
+        float v = dt2 * acc[k] * irho + 2.f * ub[k * UC + r0] - pe;
         if (tz) v = taper(a, v, ix, y, iz);
         a.next[k][c.so + i] = v;
     }
