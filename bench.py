@@ -299,6 +299,126 @@ def run_ours(args, rank, world, local):
     return 0
 
 
+def gradient_survey(n, nsteps, nside):
+    """Elastic FWI problem of the gradient workload: layered background with
+    three +-8 % Gaussian anomalies (true model), smoothed initial model,
+    nside x nside shots, 2-point receiver stride, seeded."""
+    from fwi3d_b200 import synth
+
+    sv = synth.elastic_anomaly(n=n, nsteps=nsteps, nshots_side=nside, rec_stride=2)
+    sv.par.sub = -1
+    return sv
+
+
+def run_gradient(args):
+    """FWI gradients/hour: the per-shot operator path with FP32 snapshots (the
+    drop-in form of the reference's loop) against the device objective with
+    shots batched in lockstep and FP16 second-difference snapshots."""
+    import torch
+
+    from fwi3d_b200 import ops, synth
+
+    n, nsteps, nside = args.n_grad, args.steps_grad, args.shots_side
+    sv = gradient_survey(n, nsteps, nside)
+    ns = len(sv.par.sxyz)
+    true = synth.Survey(sv.name, 3, sv.nx, sv.ny, sv.nz, sv.dx, sv.dy, sv.dz, sv.extra["true_model"], sv.wavelet,
+                        sv.dt_data, sv.par.copy())
+    obs = ops.forward_batch(true)
+    model = np.ascontiguousarray(sv.model, dtype=np.float32)
+    dt = sv.dt_data
+    dnorm = float(np.sum(obs.astype(np.float64) ** 2)) * dt
+
+    def ht(r):
+        a = (r * np.float32(dt)).astype(np.float32)
+        a[..., 0] = (r[..., 0].astype(np.float64) * 0.5 * dt).astype(np.float32)
+        a[..., -1] = (r[..., -1].astype(np.float64) * 0.5 * dt).astype(np.float32)
+        return a
+
+    def plain():
+        g = np.zeros((3,) + model.shape[1:], dtype=np.float64)
+        f = 0.0
+        for s in range(ns):
+            op = ops.from_survey(sv, s)
+            r = op.forward(False, model) - obs[s]
+            rr = r.astype(np.float64)
+            f += np.sum(rr ** 2) - 0.5 * np.sum(rr[..., 0] ** 2 + rr[..., -1] ** 2)
+            g += op.jacobianT(False, None, model, ht(r))
+            op.close()
+        return 0.5 * dt * f / dnorm, g / dnorm
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    f_plain, g_plain = plain()
+    t_plain = time.perf_counter() - t0
+
+    sv.par.snapshot_storage = 1
+    obj = ops.FwiObjective(sv, obs, batch=args.grad_batch)
+    obj.evaluate(model)  # warm-up (engine creation, allocation)
+    t0 = time.perf_counter()
+    f_b, g_b = obj.evaluate(model)
+    t_b = time.perf_counter() - t0
+    diff = float(np.linalg.norm(g_b - g_plain) / np.linalg.norm(g_plain))
+
+    cpu = None
+    if not args.no_cpu:
+        from oracle import refpy
+
+        k = 12  # the reference divides by nt/10 in its time loop (we_op.cpp:621, 838): nt must be >= 10
+        svc = gradient_survey(n, k, nside)
+        rng = np.random.default_rng(0)
+        d, _ = refpy.modeling(svc, shot=0, precision="fp32", nthreads=os.cpu_count() or 1)
+        adj = (rng.standard_normal(d.shape) * np.abs(d).max()).astype(np.float32)
+        t0 = time.perf_counter()
+        refpy.forward_jacobianT(svc, adj, shot=0, precision="fp32", nthreads=os.cpu_count() or 1)
+        tc = time.perf_counter() - t0
+        sec_per_grad = tc * (nsteps / k) * ns
+        cpu = {"value": 3600.0 / sec_per_grad, "unit": "gradients/h", "cores": os.cpu_count() or 1,
+               "kind": "reference",
+               "sample": f"reference CPU build, 1 shot forward+jacobianT on the {n}^3 grid over a {k}-step time "
+                         f"axis ({tc:.1f} s), scaled by {nsteps}/{k} steps x {ns} shots"}
+    line = {
+        "metric": "FWI gradients/hour", "value": 3600.0 / t_b, "unit": "gradients/h", "n_gpus": 1, "steps": 1,
+        "warmup": 1, "ms_per_step": t_b * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 stencils, FP16 snapshots, FP64 sums", "data": "synthetic (seeded layered model + 3 anomalies)",
+        "config": {"workload": f"elastic FWI gradient {n}^3, 10 m, dt 1 ms, {nsteps} steps, {ns} shots "
+                               f"({nside}x{nside}), 2-point receiver stride, sub 1",
+                   "batch": args.grad_batch, "storage": "FP16 second-difference residuals"},
+        "plain": {"value": 3600.0 / t_plain, "unit": "gradients/h", "seconds": t_plain,
+                  "form": "per-shot operator (forward + jacobianT), FP32 snapshots"},
+        "speedup_vs_plain": t_plain / t_b,
+        "misfit": f_b, "misfit_plain": f_plain,
+        "gradient_rel_l2_vs_plain": diff,
+        "cpu_baseline": cpu,
+        "device_bytes": obj.device_bytes(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serving(args):
+    """Serving mix: Poisson arrivals of modeling and gradient shots on six
+    models (acoustic, elastic, VTI at uneven grids); throughput and p50/p99
+    latency of the continuous-batching loop."""
+    from fwi3d_b200 import servemix, serving
+
+    models, reqs = servemix.make_mix(nreq=args.requests, rate=args.rate, seed=5)
+    srv = serving.Server(models, chunk=50, max_batch=8, gradient_workers=2)
+    rep = srv.run(reqs)
+    s = rep.summary()
+    line = {
+        "metric": "serving grid-pt updates/s", "value": s["gpt_per_s"] * 1e9, "unit": "pt/s", "n_gpus": 1,
+        "steps": 1, "warmup": 0, "ms_per_step": s["seconds"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded request mix)",
+        "config": {"workload": f"{args.requests} requests, Poisson {args.rate}/s, acoustic/elastic/VTI x 2 models, "
+                               "grids 64^3..128x112x96, 200-400 steps, 8-15 Hz, 16^2-24^2 receivers, 25 % gradients",
+                   "admission": "device bytes vs 90 % of free HBM", "chunk_steps": 50, "max_batch": 8},
+        "requests_per_s": s["requests_per_s"], "p50_s": s["p50_s"], "p99_s": s["p99_s"],
+        "latency_unit": "s", "makespan_s": s["seconds"],
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -311,6 +431,13 @@ def main():
     ap.add_argument("--ref-cap", type=int, default=40, help="max time steps of the CPU reference window")
     ap.add_argument("--n", type=int, default=256, help="grid points per axis (profiling runs use smaller grids)")
     ap.add_argument("--shots", type=int, default=8)
+    ap.add_argument("--workload", default="modeling", choices=["modeling", "gradient", "serving"])
+    ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--rate", type=float, default=20.0)
+    ap.add_argument("--n-grad", type=int, default=200)
+    ap.add_argument("--steps-grad", type=int, default=500)
+    ap.add_argument("--shots-side", type=int, default=4)
+    ap.add_argument("--grad-batch", type=int, default=4)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -319,6 +446,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "gradient":
+        return run_gradient(args)
+    if args.workload == "serving":
+        return run_serving(args)
     if world > 1:
         import datetime
 
