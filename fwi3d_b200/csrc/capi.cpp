@@ -115,6 +115,20 @@ struct fwi_op {
         for (int r = 0; r < nr; r++) l[r] = Loc{rxyz[5 * r], rxyz[5 * r + 1], rxyz[5 * r + 2]};
         return l;
     }
+    bool das() const { return nmodels != 2 && par.gl > 0; }
+    std::vector<Loc5> fibres() const
+    {
+        std::vector<Loc5> l(nr);
+        for (int r = 0; r < nr; r++)
+            l[r] = Loc5{rxyz[5 * r], rxyz[5 * r + 1], rxyz[5 * r + 2], rxyz[5 * r + 3], rxyz[5 * r + 4]};
+        return l;
+    }
+    std::vector<float> rcv_angle(int k) const
+    {
+        std::vector<float> v(nr);
+        for (int r = 0; r < nr; r++) v[r] = rxyz[5 * r + k];
+        return v;
+    }
 };
 
 struct fwi_batch {
@@ -199,7 +213,6 @@ int fwi_op_create(fwi_op **out, int device, const fwi_grid *grid, int nmodels, c
         return fail(FWI_ERR_ARG, "each grid axis needs at least 12 points");
     if (nt_data < 2 || !(dt_data > 0)) return fail(FWI_ERR_ARG, "the wavelet needs at least 2 samples and dt > 0");
     if (nr < 1) return fail(FWI_ERR_ARG, "at least one receiver is required");
-    if (par->gl > 0) return fail(FWI_ERR_UNSUPPORTED, "DAS receivers (gl > 0) are not implemented on the GPU path");
     return guarded([&] {
         std::unique_ptr<fwi_op> op(new fwi_op());
         op->device = device;
@@ -209,8 +222,9 @@ int fwi_op_create(fwi_op **out, int device, const fwi_grid *grid, int nmodels, c
         if (nmodels == 2) op->par.mt = 0;
         op->nt_data = nt_data;
         op->dt_data = dt_data;
+        if (nmodels == 2) op->par.gl = 0.f;  // analyzeGeometry, we_op.cpp:11-14
         op->nscomp = nmodels == 2 ? 1 : (op->par.mt ? 6 : 3);
-        op->nrcomp = nmodels == 2 ? 1 : 3;
+        op->nrcomp = nmodels == 2 ? 1 : (op->par.gl > 0 ? 1 : 3);
         op->wavelet = expand_wavelet(wavelet, wavelet_ncomp, nt_data, nmodels, op->par);
         std::memcpy(op->sxyz, sxyz, sizeof(op->sxyz));
         op->nr = nr;
@@ -225,9 +239,15 @@ int fwi_op_create(fwi_op **out, int device, const fwi_grid *grid, int nmodels, c
         };
         if (!inside(sxyz[0], sxyz[1], sxyz[2]))
             throw FwiError(FWI_ERR_ARG, "Shot falls outside subsurface model boundaries");
-        for (int r = 0; r < nr; r++)
+        for (int r = 0; r < nr; r++) {
             if (!inside(rxyz[5 * r], rxyz[5 * r + 1], rxyz[5 * r + 2]))
                 throw FwiError(FWI_ERR_ARG, "Receiver " + std::to_string(r) + " falls outside subsurface model boundaries");
+            if (op->das() && !dipole_inside(Loc5{rxyz[5 * r], rxyz[5 * r + 1], rxyz[5 * r + 2], rxyz[5 * r + 3],
+                                                 rxyz[5 * r + 4]},
+                                            op->par.gl, g.nx, g.ny, g.nz, g.dx, g.dy, g.dz, g.ox, g.oy, g.oz))
+                throw FwiError(FWI_ERR_ARG, "DAS channel " + std::to_string(r) +
+                                                " has its gauge length falling outside subsurface model boundaries");
+        }
         *out = op.release();
     });
 }
@@ -247,15 +267,28 @@ int fwi_op_forward(fwi_op *op, int add, const float *model, float *data)
                          pb.dt, op->nscomp);
         PointOp inj = make_delta(pb.nx, pb.ny, pb.nz, pb.dx, pb.dy, pb.dz, op->grid.ox, op->grid.oy, op->grid.oz,
                                  {Loc{op->sxyz[0], op->sxyz[1], op->sxyz[2]}}, op->par.mt != 0);
-        PointOp ext = make_delta(pb.nx, pb.ny, pb.nz, pb.dx, pb.dy, pb.dz, op->grid.ox, op->grid.oy, op->grid.oz,
-                                 op->receivers(), false);
         const InjTable it = injection_table(inj, pb.nx, pb.ny, pb.nz, op->ncomp());
-        const ExtTable et = extraction_table(ext, pb.nx, pb.ny, pb.nz);
+        ExtTable et;
+        if (op->das()) {
+            et = dipole_extraction_table(make_dipole(pb.nx, pb.ny, pb.nz, pb.dx, pb.dy, pb.dz, op->grid.ox, op->grid.oy,
+                                                     op->grid.oz, op->fibres(), op->par.gl),
+                                         pb.nx, pb.ny, pb.nz);
+        } else {
+            PointOp ext = make_delta(pb.nx, pb.ny, pb.nz, pb.dx, pb.dy, pb.dz, op->grid.ox, op->grid.oy, op->grid.oz,
+                                     op->receivers(), false);
+            et = extraction_table(ext, pb.nx, pb.ny, pb.nz);
+        }
         const int ncr = op->ncomp();
-        const int ntr = ncr * op->nr;
-        std::vector<float> rcv((size_t)ntr * nt);
+        std::vector<float> rcv((size_t)ncr * op->nr * nt);
         op->eng->forward(it, op->nscomp, src.data(), et, rcv.data(), pb.sub > 0);
         if (!finite_all(rcv.data(), (int64_t)rcv.size())) throw FwiError(FWI_ERR_NAN, "non-finite values in the traces");
+        if (op->das()) {
+            // strain along the fibre (we_op.cpp:929)
+            const std::vector<float> dip = op->rcv_angle(3), az = op->rcv_angle(4);
+            dipole_to_strain(false, rcv.data(), dip.data(), az.data(), op->nr, nt, op->par.gl);
+            rcv.resize((size_t)op->nr * nt);
+        }
+        const int ntr = op->nrcomp * op->nr;
         if (op->par.seismotype == 1) {
             // particle velocity (we_op.cpp:932-938)
             std::vector<float> v(rcv.size());
@@ -301,9 +334,11 @@ int fwi_op_jacobianT(fwi_op *op, int add, float *grad, const float *model0, cons
         std::vector<float> temp;
         if (add) temp.assign(grad, grad + nm * n);
         else std::fill(grad, grad + nm * n, 0.f);
-        // data -> propagation sampling, Ht^-1, time reversal, -alpha (we_op.cpp:994-1003)
-        std::vector<float> rcv((size_t)ntr * nt);
-        resample_forward(sinc, op->par.sinc_half_length, data, op->nt_data, op->dt_data, rcv.data(), nt, pb.dt, ntr);
+        // data -> propagation sampling, Ht^-1, time reversal, -alpha (we_op.cpp:994-1003);
+        // DAS data fill component 0 of the three
+        std::vector<float> rcv((size_t)ntr * nt, 0.f);
+        resample_forward(sinc, op->par.sinc_half_length, data, op->nt_data, op->dt_data, rcv.data(), nt, pb.dt,
+                         op->nrcomp * op->nr);
         apply_ht(true, rcv.data(), rcv.data(), ntr, nt, pb.dt);
         for (int tr = 0; tr < ntr; tr++) std::reverse(rcv.begin() + (size_t)tr * nt, rcv.begin() + (size_t)(tr + 1) * nt);
         const float alpha = pb.dt / op->dt_data;
@@ -313,9 +348,19 @@ int fwi_op_jacobianT(fwi_op *op, int add, float *grad, const float *model0, cons
             apply_dt(true, rcv.data(), v.data(), ntr, nt, pb.dt);
             rcv.swap(v);
         }
-        PointOp inj = make_delta(pb.nx, pb.ny, pb.nz, pb.dx, pb.dy, pb.dz, op->grid.ox, op->grid.oy, op->grid.oz,
-                                 op->receivers(), false);
-        const InjTable it = injection_table(inj, pb.nx, pb.ny, pb.nz, ncr);
+        InjTable it;
+        if (op->das()) {
+            // strain back to the dipole components (we_op.cpp:1015), dipole injection
+            const std::vector<float> dip = op->rcv_angle(3), az = op->rcv_angle(4);
+            dipole_to_strain(true, rcv.data(), dip.data(), az.data(), op->nr, nt, op->par.gl);
+            it = dipole_injection_table(make_dipole(pb.nx, pb.ny, pb.nz, pb.dx, pb.dy, pb.dz, op->grid.ox, op->grid.oy,
+                                                    op->grid.oz, op->fibres(), op->par.gl),
+                                        pb.nx, pb.ny, pb.nz, ncr);
+        } else {
+            PointOp inj = make_delta(pb.nx, pb.ny, pb.nz, pb.dx, pb.dy, pb.dz, op->grid.ox, op->grid.oy, op->grid.oz,
+                                     op->receivers(), false);
+            it = injection_table(inj, pb.nx, pb.ny, pb.nz, ncr);
+        }
         std::vector<float> g((size_t)nm * n);
         op->eng->adjoint(it, ntr, rcv.data(), g.data());
         // The reference accumulates the imaging sums into pmod itself, so with
@@ -354,7 +399,9 @@ int fwi_batch_create(fwi_batch **out, int device, const fwi_grid *grid, int nmod
     *out = nullptr;
     if (nmodels != 2 && nmodels != 3 && nmodels != 6)
         return fail(FWI_ERR_ARG, "The model must contain 2, 3, or 6 parameters");
-    if (par->gl > 0) return fail(FWI_ERR_UNSUPPORTED, "DAS receivers (gl > 0) are not implemented on the GPU path");
+    if (par->gl > 0 && nmodels != 2)
+        return fail(FWI_ERR_UNSUPPORTED, "DAS receivers (gl > 0) are taken by the operator path (fwi_op_*); "
+                                         "batches and the objective take point receivers");
     return guarded([&] {
         std::unique_ptr<fwi_batch> b(new fwi_batch());
         b->device = device;
@@ -543,7 +590,9 @@ int fwi_objective_create(fwi_objective **out, int device, const fwi_grid *grid, 
         return fail(FWI_ERR_ARG, "The model must contain 2, 3, or 6 parameters");
     if (grid->nx < 12 || grid->ny < 12 || grid->nz < 12) return fail(FWI_ERR_ARG, "each grid axis needs at least 12 points");
     if (nt_data < 2 || !(dt_data > 0)) return fail(FWI_ERR_ARG, "the wavelet needs at least 2 samples and dt > 0");
-    if (par->gl > 0) return fail(FWI_ERR_UNSUPPORTED, "DAS receivers (gl > 0) are not implemented on the GPU path");
+    if (par->gl > 0 && nmodels != 2)
+        return fail(FWI_ERR_UNSUPPORTED, "DAS receivers (gl > 0) are taken by the operator path (fwi_op_*); "
+                                         "batches and the objective take point receivers");
     return guarded([&] {
         std::unique_ptr<fwi_objective> o(new fwi_objective());
         o->device = device;

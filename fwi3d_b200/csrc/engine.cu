@@ -322,16 +322,29 @@ __global__ void k_scale0(float *prev, int64_t sst, const float *coef, int64_t n,
 
 // Receivers: rcv[s][c][r][it] = sum_k w_k u_c(g_k) (injector.cpp:118-140).
 __global__ void k_extract(const float *u, int64_t sst, int64_t nxyz, int ncomp, const int64_t *gidx, const float *w,
-                          int nrec, int nr, float *rcv, int nt, int it)
+                          int nrec, int nr, float *rcv, int nt, int it, int ntap)
 {
     const int row = blockIdx.x * blockDim.x + threadIdx.x;
     const int c = blockIdx.y;
     if (row >= nrec) return;
     const int sh = row / nr, r = row - sh * nr;
     const float *uc = u + sh * sst + c * nxyz;
+    const int64_t b = (int64_t)ntap * row;
     float acc = 0.f;
+    if (ntap == 27) {
 #pragma unroll
-    for (int k = 0; k < 27; k++) acc += w[27 * row + k] * uc[gidx[27 * row + k] - (int64_t)sh * nxyz];
+        for (int k = 0; k < 27; k++) acc += w[b + k] * uc[gidx[b + k] - (int64_t)sh * nxyz];
+    } else {
+        // dipole rows: taps in (end b, end a) pairs; each pair's difference is
+        // formed, rounded, then accumulated, without contraction, as
+        // dipole_m3::extract does (injector.cpp:487-489): the two ends nearly
+        // cancel, so the rounding order matters
+        for (int k = 0; k < ntap; k += 2) {
+            const float pb = __fmul_rn(w[b + k], uc[gidx[b + k] - (int64_t)sh * nxyz]);
+            const float pa = __fmul_rn(w[b + k + 1], uc[gidx[b + k + 1] - (int64_t)sh * nxyz]);
+            acc = __fadd_rn(acc, __fadd_rn(pb, pa));
+        }
+    }
     rcv[(((int64_t)sh * ncomp + c) * nr + r) * nt + it] = acc;
 }
 
@@ -706,7 +719,7 @@ void Engine::extract(const DevExt &ext, const float *curr, float *rcv_dev, int i
     const int64_t n = pb_.nxyz();
     const dim3 grd((ext.nrec + 127) / 128, nc);
     k_extract<<<grd, 128, 0, s>>>(curr, (int64_t)nc * n, n, nc, ext.gidx.as<int64_t>(), ext.w.as<float>(), ext.nrec,
-                                  ext.nr, rcv_dev, pb_.nt, it);
+                                  ext.nr, rcv_dev, pb_.nt, it, ext.ntap);
     CK(cudaGetLastError());
 }
 
@@ -775,6 +788,7 @@ void Engine::set_receivers(const ExtTable &ext, int nr)
     cudaStream_t s = (cudaStream_t)stream_;
     ext_.nrec = ext.nrec;
     ext_.nr = nr;
+    ext_.ntap = ext.ntap;
     ext_.gidx.alloc(sizeof(int64_t) * ext.gidx.size());
     ext_.w.alloc(sizeof(float) * ext.w.size());
     if (ext.nrec) {

@@ -63,6 +63,7 @@ struct DevInj {
 struct DevExt {
     int nrec = 0;   // total rows over the batch
     int nr = 0;     // receivers per shot
+    int ntap = 27;  // weights per row
     DevBuf gidx, w;
 };
 

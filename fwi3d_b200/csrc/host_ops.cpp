@@ -414,6 +414,120 @@ ExtTable extraction_table(const PointOp &op, int nx, int ny, int nz)
     return t;
 }
 
+Dipole make_dipole(int nx, int ny, int nz, float dx, float dy, float dz, float ox, float oy, float oz,
+                   const std::vector<Loc5> &loc, float gl)
+{
+    // dipole_m3::findIndicesWeights (injector.cpp:313-431): the offsets of
+    // the two ends are evaluated in double (cos/sin of float angles), the
+    // sub-cell positions stored as float, weights as for delta_m3.
+    Dipole d;
+    const int npts = (int)loc.size();
+    for (PointOp *op : {&d.a, &d.b}) {
+        op->npts = npts;
+        op->derivative = false;
+        op->xind.assign(3 * npts, 0);
+        op->yind.assign(3 * npts, 0);
+        op->zind.assign(3 * npts, 0);
+        op->xw.assign((size_t)6 * npts, 0.f);
+        op->yw.assign((size_t)6 * npts, 0.f);
+        op->zw.assign((size_t)6 * npts, 0.f);
+    }
+    auto axis = [&](double pos, float o, float h, int n, int *ind, float *w) {
+        int piv = (int)std::round((pos - o) / h);
+        if (piv == 0) piv = 1;
+        if (piv == n - 1) piv = n - 2;
+        ind[0] = piv - 1;
+        ind[1] = piv;
+        ind[2] = piv + 1;
+        const float a = (float)((pos - o) / h - piv);
+        const double a2 = std::pow((double)a, 2);
+        float *wi = w, *we = w + 3;
+        wi[0] = (float)((a2 - a) / (2 * h * hcoef(n, ind[0])));
+        wi[1] = (float)((-a2 + 1) / (h * hcoef(n, ind[1])));
+        wi[2] = (float)((a2 + a) / (2 * h * hcoef(n, ind[2])));
+        we[0] = (float)((a2 - a) / 2);
+        we[1] = (float)(-a2 + 1);
+        we[2] = (float)((a2 + a) / 2);
+    };
+    for (int r = 0; r < npts; r++) {
+        const Loc5 &l = loc[r];
+        const double hx = gl / 2 * std::cos((double)l.dip) * std::cos((double)l.az);
+        const double hy = gl / 2 * std::cos((double)l.dip) * std::sin((double)l.az);
+        const double hz = gl / 2 * std::sin((double)l.dip);
+        axis(l.x - hx, ox, dx, nx, &d.a.xind[3 * r], &d.a.xw[(size_t)6 * r]);
+        axis(l.x + hx, ox, dx, nx, &d.b.xind[3 * r], &d.b.xw[(size_t)6 * r]);
+        axis(l.y - hy, oy, dy, ny, &d.a.yind[3 * r], &d.a.yw[(size_t)6 * r]);
+        axis(l.y + hy, oy, dy, ny, &d.b.yind[3 * r], &d.b.yw[(size_t)6 * r]);
+        axis(l.z - hz, oz, dz, nz, &d.a.zind[3 * r], &d.a.zw[(size_t)6 * r]);
+        axis(l.z + hz, oz, dz, nz, &d.b.zind[3 * r], &d.b.zw[(size_t)6 * r]);
+    }
+    return d;
+}
+
+ExtTable dipole_extraction_table(const Dipole &d, int nx, int ny, int nz)
+{
+    // dipole_m3::extract (injector.cpp:467-493): sum of (b weights) u(b) - (a weights) u(a)
+    const ExtTable ta = extraction_table(d.a, nx, ny, nz), tb = extraction_table(d.b, nx, ny, nz);
+    ExtTable t;
+    t.nrec = ta.nrec;
+    t.ntap = 54;
+    t.gidx.resize((size_t)54 * t.nrec);
+    t.w.resize((size_t)54 * t.nrec);
+    for (int r = 0; r < t.nrec; r++)
+        for (int k = 0; k < 27; k++) {
+            t.gidx[(size_t)54 * r + 2 * k] = tb.gidx[(size_t)27 * r + k];
+            t.w[(size_t)54 * r + 2 * k] = tb.w[(size_t)27 * r + k];
+            t.gidx[(size_t)54 * r + 2 * k + 1] = ta.gidx[(size_t)27 * r + k];
+            t.w[(size_t)54 * r + 2 * k + 1] = -ta.w[(size_t)27 * r + k];
+        }
+    return t;
+}
+
+InjTable dipole_injection_table(const Dipole &d, int nx, int ny, int nz, int ncomp_field)
+{
+    // dipole_m3::inject (injector.cpp:433-465): end a gets -w s, end b +w s
+    InjTable ta = injection_table(d.a, nx, ny, nz, ncomp_field), tb = injection_table(d.b, nx, ny, nz, ncomp_field);
+    for (int c = 0; c < ncomp_field; c++) {
+        for (auto &w : ta.w[c]) w = -w;
+        ta.gidx[c].insert(ta.gidx[c].end(), tb.gidx[c].begin(), tb.gidx[c].end());
+        ta.trace[c].insert(ta.trace[c].end(), tb.trace[c].begin(), tb.trace[c].end());
+        ta.w[c].insert(ta.w[c].end(), tb.w[c].begin(), tb.w[c].end());
+    }
+    return ta;
+}
+
+void dipole_to_strain(bool adj, float *p, const float *dip, const float *az, int nr, int nt, float gl)
+{
+    float *p0 = p, *p1 = p + (size_t)nr * nt, *p2 = p + 2 * (size_t)nr * nt;
+    for (int ix = 0; ix < nr; ix++) {
+        const float cd = (float)std::cos((double)dip[ix]), sd = (float)std::sin((double)dip[ix]);
+        const float ca = (float)std::cos((double)az[ix]), sa = (float)std::sin((double)az[ix]);
+        const size_t o = (size_t)ix * nt;
+        for (int it = 0; it < nt; it++) {
+            if (!adj) {
+                p0[o + it] = (cd * ca * p0[o + it] + cd * sa * p1[o + it] + sd * p2[o + it]) / gl;
+                p1[o + it] = 0.f;
+                p2[o + it] = 0.f;
+            } else {
+                p2[o + it] = sd * p0[o + it] / gl;
+                p1[o + it] = cd * sa * p0[o + it] / gl;
+                p0[o + it] *= cd * ca / gl;
+            }
+        }
+    }
+}
+
+bool dipole_inside(const Loc5 &l, float gl, int nx, int ny, int nz, float dx, float dy, float dz, float ox, float oy,
+                   float oz)
+{
+    const double hx = gl / 2 * std::cos((double)l.dip) * std::cos((double)l.az);
+    const double hy = gl / 2 * std::cos((double)l.dip) * std::sin((double)l.az);
+    const double hz = gl / 2 * std::sin((double)l.dip);
+    auto in = [](double v, float o, float d, int n) { return !(v < o || v > o + (n - 1) * d); };
+    return in(l.x - hx, ox, dx, nx) && in(l.x + hx, ox, dx, nx) && in(l.y - hy, oy, dy, ny) &&
+           in(l.y + hy, oy, dy, ny) && in(l.z - hz, oz, dz, nz) && in(l.z + hz, oz, dz, nz);
+}
+
 void apply_h3(float *g, int nx, int ny, int nz, float dx, float dy, float dz)
 {
     // applyHx, applyHy, applyHz in that order (we_op.cpp:1033-1038; spatial_operators.cpp:11-177)

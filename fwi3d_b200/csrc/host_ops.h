@@ -69,10 +69,32 @@ struct InjTable {
 InjTable injection_table(const PointOp &op, int nx, int ny, int nz, int ncomp_field);
 struct ExtTable {
     int nrec = 0;
-    std::vector<int64_t> gidx;  // [nrec][27]
-    std::vector<float> w;       // [nrec][27]
+    int ntap = 27;              // 27 (point receiver) or 54 (dipole: both ends)
+    std::vector<int64_t> gidx;  // [nrec][ntap]
+    std::vector<float> w;       // [nrec][ntap]
 };
 ExtTable extraction_table(const PointOp &op, int nx, int ny, int nz);
+
+// DAS receivers (dipole_m3, injector.cpp:313-493): two delta points half a
+// gauge length `gl` before (a) and after (b) the receiver along the fibre
+// direction (dip, azimuth); the recorded value is b - a.
+struct Loc5 {
+    float x, y, z, dip, az;
+};
+struct Dipole {
+    PointOp a, b;
+};
+Dipole make_dipole(int nx, int ny, int nz, float dx, float dy, float dz, float ox, float oy, float oz,
+                   const std::vector<Loc5> &loc, float gl);
+ExtTable dipole_extraction_table(const Dipole &d, int nx, int ny, int nz);
+InjTable dipole_injection_table(const Dipole &d, int nx, int ny, int nz, int ncomp_field);
+// dipole_to_strain (misc.cpp:11-42) on [3][nr][nt]: forward projects the
+// three components on the fibre (into component 0, zeroing 1 and 2) and
+// divides by gl; adjoint spreads component 0 back.
+void dipole_to_strain(bool adj, float *p, const float *dip, const float *az, int nr, int nt, float gl);
+// Fibre endpoints inside the model (analyzeGeometry, we_op.cpp:105-125).
+bool dipole_inside(const Loc5 &l, float gl, int nx, int ny, int nz, float dx, float dy, float dz, float ox, float oy,
+                   float oz);
 
 // H quadrature on a 3-D array along x, y, z (spatial_operators.cpp:11-177).
 void apply_h3(float *g, int nx, int ny, int nz, float dx, float dy, float dz);

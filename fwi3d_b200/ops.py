@@ -117,7 +117,8 @@ class nl_we_op:
     # -- shapes ----------------------------------------------------------
     @property
     def nrcomp(self) -> int:
-        return 1 if self.nmodels == 2 else 3
+        # DAS channels (gl > 0) record one strain component (analyzeGeometry, we_op.cpp:23)
+        return 1 if self.nmodels == 2 or self._par.gl > 0 else 3
 
     @property
     def domain_shape(self):

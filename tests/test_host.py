@@ -70,8 +70,13 @@ def test_create_validates_geometry_and_options():
     assert rc == _lib.FWI_ERR_ARG and "outside" in msg
     rc, msg = _create(sv, rxyz=[[[0.05, 0.05, 9.0, 0, 0]]])
     assert rc == _lib.FWI_ERR_ARG and "Receiver 0" in msg
-    rc, msg = _create(sv, gl=0.01)
-    assert rc == _lib.FWI_ERR_UNSUPPORTED
+    # acoustic operators ignore the gauge length (analyzeGeometry sets it to 0)
+    assert _create(sv, gl=0.01)[0] == _lib.FWI_OK
+    # an elastic DAS channel whose fibre leaves the model is rejected
+    ev = synth.elastic_layered(n=16, nsteps=10, taper=2, rec_stride=4, nshots=1)
+    rc, msg = _create(ev, gl=0.05, rxyz=[[[0.01, 0.06, 0.06, 0.0, 0.0]]])
+    assert rc == _lib.FWI_ERR_ARG and "gauge length" in msg
+    assert _create(ev, gl=0.02, rxyz=[[[0.06, 0.06, 0.06, 0.3, 1.0]]])[0] == _lib.FWI_OK
     del bad
 
 
