@@ -187,7 +187,7 @@ __device__ __forceinline__ void march_tile(const MarchCtx &c, int ya, int yb, in
 }
 
 template <int PH>
-__global__ void __launch_bounds__(f3::NT, 1) k_elastic_march(const __grid_constant__ StepArgs a, int nchunks)
+__global__ void __launch_bounds__(f3::NT, 1) k_elastic_march(const __grid_constant__ StepArgs a, int nchunks, int slab)
 {
     extern __shared__ __align__(16) unsigned char m3_smem[];
     MarchCtx c;
@@ -200,7 +200,13 @@ __global__ void __launch_bounds__(f3::NT, 1) k_elastic_march(const __grid_consta
     tile_range(blockIdx.x, a.g.nz, f3::TZ, c.z0, c.zend);
     tile_range(blockIdx.y, a.g.nx, f3::TX, c.x0, c.xend);
     int ya, yb;
-    m3_chunk(a.g.ny, ch, nchunks, ya, yb);
+    if (slab > 0) {
+        // the two y-wall slabs [0, slab) and [ny - slab, ny) of the fused path
+        ya = ch == 0 ? 0 : a.g.ny - slab;
+        yb = ch == 0 ? slab : a.g.ny;
+    } else {
+        m3_chunk(a.g.ny, ch, nchunks, ya, yb);
+    }
     if (ya >= yb) return;
     const bool xf = m3_fast(c.x0, a.g.nx, f3::TX), zf = m3_fast(c.z0, a.g.nz, f3::TZ);
     if (xf && zf) march_tile<PH, true, true>(c, ya, yb, tid);
@@ -396,9 +402,16 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     const char *menv = std::getenv("FWI_MARCH");
     march_ = pb.nmodels != 2 && (menv && menv[0] == '1') && pb.nx >= f3::TX + 6 && pb.nz >= f3::TZ + 6 &&
              pb.ny >= 12;
-    if (pb.nmodels != 2 && !march_)
+    {
+        const char *fe = std::getenv("FWI_FUSED");
+        const char *se = std::getenv("FWI_SLAB_MARCH");
+        const bool fused = !march_ && pb.nmodels != 2 && !(fe && fe[0] == '0') && pb.nx >= fz::TX + 6 &&
+                           pb.nz >= fz::TZ + 6 && pb.ny > 2 * fz::YPAD;
+        slab_march_ = fused && !(se && se[0] == '0');
+    }
+    if (pb.nmodels != 2 && !march_ && !slab_march_)
         aux_.alloc(sizeof(float) * (size_t)pb.nshots * (pb.nmodels == 6 ? 9 : 7) * n);
-    if (march_) {
+    if (march_ || slab_march_) {
         CK(cudaFuncSetAttribute(k_elastic_march<ELASTIC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(MarchSmem)));
         CK(cudaFuncSetAttribute(k_elastic_march<VTI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -603,8 +616,8 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         nch = std::max(1, std::min(nch, (pb_.ny - 12) / 24));
         const dim3 grd(kz, kx, nch * pb_.nshots), mblk(f3::TZ, f3::TX);
         kmark(true, "k_elastic_march", n * pb_.nshots);
-        if (pb_.nmodels == 3) k_elastic_march<ELASTIC><<<grd, mblk, sizeof(MarchSmem), s>>>(a, nch);
-        else k_elastic_march<VTI><<<grd, mblk, sizeof(MarchSmem), s>>>(a, nch);
+        if (pb_.nmodels == 3) k_elastic_march<ELASTIC><<<grd, mblk, sizeof(MarchSmem), s>>>(a, nch, 0);
+        else k_elastic_march<VTI><<<grd, mblk, sizeof(MarchSmem), s>>>(a, nch, 0);
         kmark(false, nullptr, 0);
         // SAT of every face point
         const int64_t nf = 2 * (int64_t)pb_.nx * pb_.ny + 2 * (int64_t)(pb_.nz - 2) * pb_.ny +
@@ -657,15 +670,23 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         step_range(0, pb_.ny);
         kmark(false, nullptr, 0);
     } else {
-        // planes near the y walls: per-point kernels (derivative scratch two planes deeper)
-        if (pb_.ny < 2 * (P + 2)) {
-            aux_range(0, pb_.ny);
+        if (slab_march_) {
+            // planes near the y walls: the marching kernel (y closures), two chunks per tile column
+            const int kz3 = (pb_.nz + f3::TZ - 1) / f3::TZ, kx3 = (pb_.nx + f3::TX - 1) / f3::TX;
+            const dim3 grd3(kz3, kx3, 2 * pb_.nshots), mblk(f3::TZ, f3::TX);
+            if (pb_.nmodels == 3) k_elastic_march<ELASTIC><<<grd3, mblk, sizeof(MarchSmem), s>>>(a, 2, P);
+            else k_elastic_march<VTI><<<grd3, mblk, sizeof(MarchSmem), s>>>(a, 2, P);
         } else {
-            aux_range(0, P + 2);
-            aux_range(pb_.ny - P - 2, pb_.ny);
+            // planes near the y walls: per-point kernels (derivative scratch two planes deeper)
+            if (pb_.ny < 2 * (P + 2)) {
+                aux_range(0, pb_.ny);
+            } else {
+                aux_range(0, P + 2);
+                aux_range(pb_.ny - P - 2, pb_.ny);
+            }
+            step_range(0, P);
+            step_range(pb_.ny - P, pb_.ny);
         }
-        step_range(0, P);
-        step_range(pb_.ny - P, pb_.ny);
         // interior planes: fused kernel
         StepArgs f = a;
         f.y0 = P;
@@ -686,12 +707,19 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
             else k_elastic_fused<VTI, 1><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch);
         }
         kmark(false, nullptr, 0);
-        // SAT of the x/z faces of the fused planes
-        const int64_t ly = f.y1 - f.y0;
-        const int64_t nf = 2 * (int64_t)pb_.nx * ly + 2 * (int64_t)(pb_.nz - 2) * ly;
+        // SAT of the x/z faces of the fused planes (and, with the marching
+        // slabs, of every face of the grid)
+        StepArgs sat = f;
+        if (slab_march_) {
+            sat.y0 = 0;
+            sat.y1 = pb_.ny;
+        }
+        const int64_t ly = sat.y1 - sat.y0;
+        int64_t nf = 2 * (int64_t)pb_.nx * ly + 2 * (int64_t)(pb_.nz - 2) * ly;
+        if (slab_march_) nf += 2 * (int64_t)(pb_.nx - 2) * (pb_.nz - 2);
         const dim3 sgrd((unsigned)((nf + 127) / 128), pb_.nshots);
-        if (pb_.nmodels == 3) k_elastic_face_sat<ELASTIC><<<sgrd, 128, 0, s>>>(f, nf);
-        else k_elastic_face_sat<VTI><<<sgrd, 128, 0, s>>>(f, nf);
+        if (pb_.nmodels == 3) k_elastic_face_sat<ELASTIC><<<sgrd, 128, 0, s>>>(sat, nf);
+        else k_elastic_face_sat<VTI><<<sgrd, 128, 0, s>>>(sat, nf);
     }
     CK(cudaGetLastError());
 }
@@ -768,7 +796,8 @@ double Engine::main_kernel_ms(int *launches, int64_t *points, const char **name)
 
 int Engine::launches_per_step() const
 {
-    int k = (pb_.nmodels == 2 ? 1 : (march_ ? 2 : (fused_ ? (pb_.ny < 2 * (fz::YPAD + 2) ? 5 : 6) : 2)));
+    int k = (pb_.nmodels == 2 ? 1
+                              : (march_ ? 2 : (fused_ ? (slab_march_ ? 3 : (pb_.ny < 2 * (fz::YPAD + 2) ? 5 : 6)) : 2)));
     if (ext_.nrec) k += 1;
     for (int c = 0; c < 3; c++) k += inj_.n[c] ? 1 : 0;
     return k;
