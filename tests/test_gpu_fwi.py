@@ -163,3 +163,22 @@ def test_checkpointed_gradient_matches_full_storage():
     sv.par.snapshot_budget_gb = 0.001  # below the checkpointing minimum: a clear error
     with pytest.raises(Exception, match="snapshot budget"):
         ops.FwiObjective(sv, obs, batch=4).evaluate(sv.model)
+
+
+def test_sharded_objective_matches_single_process():
+    """Shots split over two ranks (rank-strided) and summed as the all-reduce
+    does: same misfit and gradient as one objective over all shots."""
+    from fwi3d_b200 import distributed
+
+    sv, obs = _problem()
+    f, g = ops.FwiObjective(sv, obs, normalize=True, batch=4).evaluate(sv.model)
+    one = distributed.ShardedObjective(sv, obs, rank=0, world=1, batch=4)
+    f1, g1 = one.evaluate(sv.model)
+    assert f1 == pytest.approx(f, rel=1e-9) and rel(g1, g) < 1e-7
+    parts = [distributed.ShardedObjective(sv, obs, rank=r, world=2, batch=2) for r in range(2)]
+    fs, gs, dns = 0.0, 0.0, 0.0
+    for p in parts:
+        fl, gl = p.obj.evaluate(sv.model)
+        fs, gs, dns = fs + fl, gs + gl.astype(np.float64), dns + p.dn_local
+    assert fs / dns == pytest.approx(f, rel=1e-6)
+    assert rel(gs / dns, g) < 1e-6
