@@ -134,10 +134,18 @@ __device__ __forceinline__ void fused_march(FusedCtx &c, int tid, int ya, int yb
     fz_prologue<PH>(c, tid, ya);
     __syncthreads();
     for (int y = ya - 4; y < yb; y++) {
-        fz_slots(c, y);
-        fz_load_u(c, tid, y + 4, c.sl[6]);
+        fz_slots<PH>(c, y);
+        // the elastic kernel copies plane y+4 in during the previous iteration
+        if (PH == VTI || y == ya - 4) fz_load_u(c, tid, y + 4, c.sl[6]);
+        else cpa_wait();
         if (y >= ya) fz_load_mat<PH>(c, tid, y);
         __syncthreads();
+        if (PH == ELASTIC) {
+            // plane y+5 (< ny - 3 for every chunk of [8, ny-8)) into the slot of
+            // plane y-3, which no phase of this iteration reads
+            fz_load_u<true>(c, tid, y + 5, ring<PH>(y + 5));
+            cpa_commit();
+        }
         fz_column<PH, F>(c, th, tid, y + 2);
         if (y >= ya) fz_derived<PH, F>(c, tid, y);
         __syncthreads();
@@ -147,6 +155,7 @@ __device__ __forceinline__ void fused_march(FusedCtx &c, int tid, int ya, int yb
         }
         __syncthreads();
     }
+    cpa_wait();
 }
 
 // Fused elastic step over planes [ylo, yhi) (see fused.cuh).  grid: (z tiles,

@@ -29,20 +29,65 @@ constexpr int HW = 4;                          // halo of the displacement ring
 constexpr int ZW = TZ + 2 * HW, XW = TX + 2 * HW;
 constexpr int HD = 2;                          // halo of the derived planes
 constexpr int ZH = TZ + 2 * HD, XH = TX + 2 * HD;
-constexpr int NRING = 7;
 constexpr int YPAD = 8;                        // y planes per side left to the per-point kernels
 }  // namespace fz
 
-// Derived-plane slots.
-enum { DV_T0 = 0, DV_T2 = 1, DV_Y0 = 2, DV_Z0 = 3, DV_X2 = 4, DV_Y2 = 5, NDV = 6 };
-// Material planes over the derived region: mu, lambda, (VTI) c13, eps, c66.
-enum { MP_MU = 0, MP_LAM = 1, MP_C13 = 2, MP_EPS = 3, MP_C66 = 4, NMP = 5 };
+// Derived-plane slots: T0, Y0, Z0, X2, Y2 in dv; T2 (VTI only; the isotropic
+// T2 equals T0) in the overlay below.
+enum { DV_T0 = 0, DV_Y0 = 1, DV_Z0 = 2, DV_X2 = 3, DV_Y2 = 4, NDVC = 5, DV_T2 = 5, NDV = 6 };
+// Material planes over the derived region: mu, lambda in mp; (VTI) c13, eps,
+// c66 in the overlay.
+enum { MP_MU = 0, MP_LAM = 1, NMPC = 2, MP_C13 = 2, MP_EPS = 3, MP_C66 = 4, NMP = 5 };
 
+// Ring slot 7: the elastic kernel's eighth displacement plane (the one
+// copied in while the others are in use); the VTI kernel keeps a 7-slot ring
+// and stores its four extra planes (T2, c13, eps, c66) there instead.
 struct FusedSmem {
-    float u[fz::NRING][3][fz::XW][fz::ZW];
-    float dv[NDV][fz::XH][fz::ZH];
-    float mp[NMP][fz::XH][fz::ZH];
+    float u[8][3][fz::XW][fz::ZW];
+    float dv[NDVC][fz::XH][fz::ZH];
+    float mp[NMPC][fz::XH][fz::ZH];
 };
+static_assert(4 * fz::XH * fz::ZH <= 3 * fz::XW * fz::ZW, "VTI overlay must fit one ring slot");
+using ZRow = float[fz::ZH];
+FWI_HD ZRow *fz_dvp(const FusedSmem *s, int d)
+{
+    if (d < NDVC) return const_cast<ZRow *>(s->dv[d]);
+    return reinterpret_cast<ZRow *>(const_cast<float *>(&s->u[7][0][0][0]));
+}
+FWI_HD ZRow *fz_mpp(const FusedSmem *s, int m)
+{
+    if (m < NMPC) return const_cast<ZRow *>(s->mp[m]);
+    return reinterpret_cast<ZRow *>(const_cast<float *>(&s->u[7][0][0][0]) + (m - NMPC + 1) * fz::XH * fz::ZH);
+}
+
+// One 4-byte global->shared copy: asynchronous on the GPU (cp.async; zero
+// fill when `valid` is false, `src` then only has to be a mapped address),
+// a plain copy on the host.
+template <bool ASYNC>
+FWI_HD void cpa4(float *dst, const float *src, bool valid)
+{
+#if defined(__CUDA_ARCH__)
+    if (ASYNC) {
+        const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 4 : 0)
+                     : "memory");
+        return;
+    }
+#endif
+    *dst = valid ? *src : 0.f;
+}
+FWI_HD void cpa_commit()
+{
+#if defined(__CUDA_ARCH__)
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+#endif
+}
+FWI_HD void cpa_wait()
+{
+#if defined(__CUDA_ARCH__)
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+#endif
+}
 
 // Per-thread state carried along the march (registers on the GPU).
 struct FusedThread {
@@ -97,21 +142,27 @@ struct SXc {
     }
 };
 
-FWI_HD int ring(int q) { return ((q % fz::NRING) + fz::NRING) % fz::NRING; }
+// Ring depth: 8 slots for the elastic kernel (one plane in flight), 7 for VTI.
+template <int PH>
+FWI_HD constexpr int fz_nring() { return PH == ELASTIC ? 8 : 7; }
+template <int PH>
+FWI_HD int ring(int q) { return ((q % fz_nring<PH>()) + fz_nring<PH>()) % fz_nring<PH>(); }
 
 // Ring slots of planes y-2 .. y+4.
+template <int PH>
 FWI_HD void fz_slots(FusedCtx &c, int y)
 {
-    int s = ring(y - 2);
+    int s = ring<PH>(y - 2);
     for (int k = 0; k < 7; k++) {
         c.sl[k] = s;
-        s = s + 1 == fz::NRING ? 0 : s + 1;
+        s = s + 1 == fz_nring<PH>() ? 0 : s + 1;
     }
 }
 
 // ---------------------------------------------------------------------------
 // Phase A: load displacement plane q (tile + 4 halo) into its ring slot.
 // ---------------------------------------------------------------------------
+template <bool ASYNC = false>
 FWI_HD void fz_load_u(FusedCtx &c, int tid, int q, int slot)
 {
     const Dims &g = c.a->g;
@@ -119,8 +170,8 @@ FWI_HD void fz_load_u(FusedCtx &c, int tid, int q, int slot)
         const int xw = p / fz::ZW, zw = p - xw * fz::ZW;
         const int ix = c.x0 - fz::HW + xw, iz = c.z0 - fz::HW + zw;
         const bool in = ix >= 0 && ix < g.nx && iz >= 0 && iz < g.nz;
-        const int64_t i = in ? g.idx(ix, q, iz) : 0;
-        for (int k = 0; k < 3; k++) c.sm->u[slot][k][xw][zw] = in ? c.a->curr[k][c.so + i] : 0.f;
+        const int64_t i = c.so + (in ? g.idx(ix, q, iz) : 0);
+        for (int k = 0; k < 3; k++) cpa4<ASYNC>(&c.sm->u[slot][k][xw][zw], c.a->curr[k] + i, in);
     }
 }
 
@@ -134,12 +185,12 @@ FWI_HD void fz_load_mat(FusedCtx &c, int tid, int y)
         const int ix = c.x0 - fz::HD + xh, iz = c.z0 - fz::HD + zh;
         const bool in = ix >= 0 && ix < g.nx && iz >= 0 && iz < g.nz;
         const int64_t i = in ? g.idx(ix, y, iz) : 0;
-        c.sm->mp[MP_MU][xh][zh] = in ? c.a->m[1][i] : 0.f;
-        c.sm->mp[MP_LAM][xh][zh] = in ? c.a->m[0][i] : 0.f;
+        fz_mpp(c.sm, MP_MU)[xh][zh] = in ? c.a->m[1][i] : 0.f;
+        fz_mpp(c.sm, MP_LAM)[xh][zh] = in ? c.a->m[0][i] : 0.f;
         if (PH == VTI) {
-            c.sm->mp[MP_C13][xh][zh] = in ? c.a->m[3][i] : 0.f;
-            c.sm->mp[MP_EPS][xh][zh] = in ? c.a->m[4][i] : 0.f;
-            c.sm->mp[MP_C66][xh][zh] = in ? c.a->m[5][i] : 0.f;
+            fz_mpp(c.sm, MP_C13)[xh][zh] = in ? c.a->m[3][i] : 0.f;
+            fz_mpp(c.sm, MP_EPS)[xh][zh] = in ? c.a->m[4][i] : 0.f;
+            fz_mpp(c.sm, MP_C66)[xh][zh] = in ? c.a->m[5][i] : 0.f;
         }
     }
 }
@@ -203,10 +254,9 @@ FWI_HD void fz_derived(FusedCtx &c, int tid, int y)
     for (int p = tid; p < fz::XH * fz::ZH; p += fz::NT) {
         const int xh = p / fz::ZH, zh = p - xh * fz::ZH;
         const int ix = c.x0 - fz::HD + xh, iz = c.z0 - fz::HD + zh;
-        float *dv0 = &c.sm->dv[0][xh][zh];
-        const int stride = fz::XH * fz::ZH;
+        auto dv = [&](int d) -> float & { return fz_dvp(c.sm, d)[xh][zh]; };
         if (!F && (ix < 0 || ix >= g.nx || iz < 0 || iz >= g.nz)) {
-            for (int k = 0; k < NDV; k++) dv0[k * stride] = 0.f;
+            for (int k = 0; k < (PH == ELASTIC ? NDVC : NDV); k++) dv(k) = 0.f;
             continue;
         }
         const int ixw = xh + (fz::HW - fz::HD), izw = zh + (fz::HW - fz::HD);
@@ -215,28 +265,26 @@ FWI_HD void fz_derived(FusedCtx &c, int tid, int y)
         const float ux0 = fz_dx<F>(c, 0, s0, ix, izw);
         const float uy1 = fz_dy(c, 1, sn, ixw, izw);
         const float uz2 = fz_dz<F>(c, 2, s0, ixw, iz);
-        const float mu = c.sm->mp[MP_MU][xh][zh], lam = c.sm->mp[MP_LAM][xh][zh];
+        const float mu = fz_mpp(c.sm, MP_MU)[xh][zh], lam = fz_mpp(c.sm, MP_LAM)[xh][zh];
         const float uy0 = fz_dy(c, 0, sn, ixw, izw);
         const float uz0 = fz_dz<F>(c, 0, s0, ixw, iz);
         const float ux2 = fz_dx<F>(c, 2, s0, ix, izw);
         const float uy2 = fz_dy(c, 2, sn, ixw, izw);
         if (PH == ELASTIC) {
-            const float T = lam * (ux0 + uy1 + uz2);
-            dv0[DV_T0 * stride] = T;
-            dv0[DV_T2 * stride] = T;
-            dv0[DV_Y0 * stride] = uy0;  // multiplied by the coefficient at the tap (mult_D)
+            dv(DV_T0) = lam * (ux0 + uy1 + uz2);  // also the z-differentiated T2
+            dv(DV_Y0) = uy0;  // multiplied by the coefficient at the tap (mult_D)
         } else {
-            const float c13 = c.sm->mp[MP_C13][xh][zh], eps = c.sm->mp[MP_EPS][xh][zh];
-            const float c66 = c.sm->mp[MP_C66][xh][zh];
+            const float c13 = fz_mpp(c.sm, MP_C13)[xh][zh], eps = fz_mpp(c.sm, MP_EPS)[xh][zh];
+            const float c66 = fz_mpp(c.sm, MP_C66)[xh][zh];
             const float c11c = (1.f + 2.f * eps) * lam;
             const float c12 = (1.f + 2.f * eps) * (lam + 2.f * mu) - 2.f * c66;
-            dv0[DV_T0 * stride] = c11c * ux0 + c12 * uy1 + c13 * uz2;
-            dv0[DV_T2 * stride] = c13 * (ux0 + uy1) + lam * uz2;
-            dv0[DV_Y0 * stride] = uy0;
+            dv(DV_T0) = c11c * ux0 + c12 * uy1 + c13 * uz2;
+            dv(DV_T2) = c13 * (ux0 + uy1) + lam * uz2;
+            dv(DV_Y0) = uy0;
         }
-        dv0[DV_Z0 * stride] = uz0;
-        dv0[DV_X2 * stride] = ux2;
-        dv0[DV_Y2 * stride] = uy2;
+        dv(DV_Z0) = uz0;
+        dv(DV_X2) = ux2;
+        dv(DV_Y2) = uy2;
     }
 }
 
@@ -354,10 +402,10 @@ FWI_HD float d2closure_apply(const W8 &w, const U &u, int i, int n, float ad2)
 // Smem accessors of the output phase.
 FWI_HD SX ux_line(const FusedCtx &c, int slot, int k, int izw) { return SX{&c.sm->u[slot][k][0][izw], c.x0 - fz::HW, fz::ZW}; }
 FWI_HD SZ uz_line(const FusedCtx &c, int slot, int k, int ixw) { return SZ{&c.sm->u[slot][k][ixw][0], c.z0 - fz::HW}; }
-FWI_HD SX mx_line(const FusedCtx &c, int m, int zh) { return SX{&c.sm->mp[m][0][zh], c.x0 - fz::HD, fz::ZH}; }
-FWI_HD SZ mz_line(const FusedCtx &c, int m, int xh) { return SZ{&c.sm->mp[m][xh][0], c.z0 - fz::HD}; }
-FWI_HD SX dx_line(const FusedCtx &c, int d, int zh) { return SX{&c.sm->dv[d][0][zh], c.x0 - fz::HD, fz::ZH}; }
-FWI_HD SZ dz_line(const FusedCtx &c, int d, int xh) { return SZ{&c.sm->dv[d][xh][0], c.z0 - fz::HD}; }
+FWI_HD SX mx_line(const FusedCtx &c, int m, int zh) { return SX{&fz_mpp(c.sm, m)[0][zh], c.x0 - fz::HD, fz::ZH}; }
+FWI_HD SZ mz_line(const FusedCtx &c, int m, int xh) { return SZ{&fz_mpp(c.sm, m)[xh][0], c.z0 - fz::HD}; }
+FWI_HD SX dx_line(const FusedCtx &c, int d, int zh) { return SX{&fz_dvp(c.sm, d)[0][zh], c.x0 - fz::HD, fz::ZH}; }
+FWI_HD SZ dz_line(const FusedCtx &c, int d, int xh) { return SZ{&fz_dvp(c.sm, d)[xh][0], c.z0 - fz::HD}; }
 template <class E, class M>
 struct C11bS {
     E eps;
@@ -456,7 +504,7 @@ FWI_HD void fz_output(FusedCtx &c, const FusedThread &th, int tid, int y)
     acc[1] += d1_prod_row(dx_line(c, DV_Y0, zh), Px, ix, g.nx) * a.idx;
     acc[1] += d1_prod_row(dz_line(c, DV_Y2, xh), muz, iz, g.nz) * a.idz;
     // comp 2: Dz(T2)/dz + Dx(mu u_z0)/dx + Dy(mu u_z1)/dy
-    acc[2] += d1_row(dz_line(c, DV_T2, xh), iz, g.nz) * a.idz;
+    acc[2] += d1_row(dz_line(c, PH == ELASTIC ? DV_T0 : DV_T2, xh), iz, g.nz) * a.idz;
     acc[2] += d1_prod_row(dx_line(c, DV_Z0, zh), mux, ix, g.nx) * a.idx;
     acc[2] += d1m(th.qZ1[0], th.qmu[0], th.qZ1[1], th.qmu[1], th.qZ1[3], th.qmu[3], th.qZ1[4], th.qmu[4]) * a.idy;
 
@@ -495,7 +543,7 @@ FWI_HD void fz_output_fast(FusedCtx &c, const FusedThread &th, int tid, int y)
     constexpr int UX = fz::ZW, UC = fz::XW * fz::ZW, US = 3 * fz::XW * fz::ZW, DX = fz::ZH;
     const float *ub = &s.u[0][0][ixw][izw];
     const int r0 = c.sl[2] * US, rm1 = c.sl[1] * US, rm2 = c.sl[0] * US, rp1 = c.sl[3] * US, rp2 = c.sl[4] * US;
-    const float *mu = &s.mp[MP_MU][xh][zh];
+    const float *mu = &fz_mpp(&s, MP_MU)[xh][zh];
     const float idx2 = a.ad1[0], idy2 = a.ad1[1];
     float acc[3];
     const W5 wxm = d2w(mu[-2 * DX], mu[-DX], mu[0], mu[DX], mu[2 * DX]);
@@ -515,7 +563,7 @@ FWI_HD void fz_output_fast(FusedCtx &c, const FusedThread &th, int tid, int y)
             acc[k] = v;
         }
     } else {
-        const float *ep = &s.mp[MP_EPS][xh][zh], *c6 = &s.mp[MP_C66][xh][zh];
+        const float *ep = &fz_mpp(&s, MP_EPS)[xh][zh], *c6 = &fz_mpp(&s, MP_C66)[xh][zh];
         auto c11b = [&](int o) { return 2.f * (1.f + 2.f * ep[o]) * mu[o]; };
         const W5 wxb = d2w(c11b(-2 * DX), c11b(-DX), c11b(0), c11b(DX), c11b(2 * DX));
         const W5 wx6 = d2w(c6[-2 * DX], c6[-DX], c6[0], c6[DX], c6[2 * DX]);
@@ -538,11 +586,11 @@ FWI_HD void fz_output_fast(FusedCtx &c, const FusedThread &th, int tid, int y)
         }
     }
     // D1 of the stress combinations and the mixed terms (we_op.cpp:661-688, 1312-1349)
-    const float *P = (PH == VTI) ? &s.mp[MP_C66][xh][zh] : mu;
+    const float *P = (PH == VTI) ? &fz_mpp(&s, MP_C66)[xh][zh] : mu;
     const float *qP = (PH == VTI) ? th.q66 : th.qmu;
-    const float *t0 = &s.dv[DV_T0][xh][zh], *t2 = &s.dv[DV_T2][xh][zh];
-    const float *x2 = &s.dv[DV_X2][xh][zh], *y0 = &s.dv[DV_Y0][xh][zh];
-    const float *y2 = &s.dv[DV_Y2][xh][zh], *z0 = &s.dv[DV_Z0][xh][zh];
+    const float *t0 = &fz_dvp(&s, DV_T0)[xh][zh], *t2 = &fz_dvp(&s, PH == ELASTIC ? DV_T0 : DV_T2)[xh][zh];
+    const float *x2 = &fz_dvp(&s, DV_X2)[xh][zh], *y0 = &fz_dvp(&s, DV_Y0)[xh][zh];
+    const float *y2 = &fz_dvp(&s, DV_Y2)[xh][zh], *z0 = &fz_dvp(&s, DV_Z0)[xh][zh];
     acc[0] += d1i(t0[-2 * DX], t0[-DX], t0[DX], t0[2 * DX]) * a.idx;
     acc[0] += d1m(th.qX1[0], qP[0], th.qX1[1], qP[1], th.qX1[3], qP[3], th.qX1[4], qP[4]) * a.idy;
     acc[0] += d1m(x2[-2], mu[-2], x2[-1], mu[-1], x2[1], mu[1], x2[2], mu[2]) * a.idy;  // dy as the reference
@@ -588,7 +636,7 @@ FWI_HD void tile_range(int k, int n, int T, int &origin, int &end)
 template <int PH>
 FWI_HD void fz_prologue(FusedCtx &c, int tid, int ya)
 {
-    for (int q = ya - 4; q < ya; q++) fz_load_u(c, tid, q, ring(q));
+    for (int q = ya - 4; q < ya; q++) fz_load_u(c, tid, q, ring<PH>(q));
 }
 
 }  // namespace fwi

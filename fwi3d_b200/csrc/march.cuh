@@ -63,35 +63,6 @@ struct MarchCtx {
     MarchSmem *sm;
 };
 
-// One 4-byte global->shared copy: asynchronous on the GPU (cp.async, zero
-// fill when `valid` is false; `src` then only has to be a mapped address),
-// a plain copy on the host.
-template <bool ASYNC>
-FWI_HD void m3_cp4(float *dst, const float *src, bool valid)
-{
-#if defined(__CUDA_ARCH__)
-    if (ASYNC) {
-        const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 4 : 0)
-                     : "memory");
-        return;
-    }
-#endif
-    *dst = valid ? *src : 0.f;
-}
-FWI_HD void m3_cp_commit()
-{
-#if defined(__CUDA_ARCH__)
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-#endif
-}
-FWI_HD void m3_cp_wait()
-{
-#if defined(__CUDA_ARCH__)
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-#endif
-}
-
 // Ring accessors along y (own column), indexed by global plane.
 struct URing {
     const float *p;  // &u[0][k][xu][zu]
@@ -116,7 +87,7 @@ FWI_HD void m3_load_u(const MarchCtx &c, int tid, int q)
         const bool in = INSIDE || (ix >= 0 && ix < g.nx && iz >= 0 && iz < g.nz);
         const int64_t i = c.so + (in ? g.idx(ix, q, iz) : 0);
 #pragma unroll
-        for (int k = 0; k < 3; k++) m3_cp4<ASYNC>(&c.sm->u[slot][k][xu][zu], c.a->curr[k] + i, in);
+        for (int k = 0; k < 3; k++) cpa4<ASYNC>(&c.sm->u[slot][k][xu][zu], c.a->curr[k] + i, in);
     }
 }
 
@@ -129,12 +100,12 @@ FWI_HD void m3_load_mat(const MarchCtx &c, int tid, int b, int y)
         const int ix = c.x0 - f3::HD + xd, iz = c.z0 - f3::HD + zd;
         const bool in = INSIDE || (ix >= 0 && ix < g.nx && iz >= 0 && iz < g.nz);
         const int64_t i = in ? g.idx(ix, y, iz) : 0;
-        m3_cp4<ASYNC>(&c.sm->mp[b][MP_MU][xd][zd], c.a->m[1] + i, in);
-        m3_cp4<ASYNC>(&c.sm->mp[b][MP_LAM][xd][zd], c.a->m[0] + i, in);
+        cpa4<ASYNC>(&c.sm->mp[b][MP_MU][xd][zd], c.a->m[1] + i, in);
+        cpa4<ASYNC>(&c.sm->mp[b][MP_LAM][xd][zd], c.a->m[0] + i, in);
         if (PH == VTI) {
-            m3_cp4<ASYNC>(&c.sm->mp[b][MP_C13][xd][zd], c.a->m[3] + i, in);
-            m3_cp4<ASYNC>(&c.sm->mp[b][MP_EPS][xd][zd], c.a->m[4] + i, in);
-            m3_cp4<ASYNC>(&c.sm->mp[b][MP_C66][xd][zd], c.a->m[5] + i, in);
+            cpa4<ASYNC>(&c.sm->mp[b][MP_C13][xd][zd], c.a->m[3] + i, in);
+            cpa4<ASYNC>(&c.sm->mp[b][MP_EPS][xd][zd], c.a->m[4] + i, in);
+            cpa4<ASYNC>(&c.sm->mp[b][MP_C66][xd][zd], c.a->m[5] + i, in);
         }
     }
 }
@@ -488,7 +459,7 @@ FWI_HD void m3_march(MarchCtx c, int ya, int yb, Par &&par)
         loaded = need > loaded ? need : loaded;
         const bool have_mp = nout && mp_plane == out[0];
         par([&](int tid) {
-            m3_cp_wait();
+            cpa_wait();
             for (int p = lo; p <= need; p++) m3_load_u<IN, false>(c, tid, p);
             if (nout && !have_mp) m3_load_mat<PH, IN, false>(c, tid, mb, out[0]);
         });
@@ -506,7 +477,7 @@ FWI_HD void m3_march(MarchCtx c, int ya, int yb, Par &&par)
         par([&](int tid) {
             for (int p = pf_lo; p <= pf_hi; p++) m3_load_u<IN, true>(c, tid, p);
             if (pf_mp) m3_load_mat<PH, IN, true>(c, tid, nmb, nout1[0]);
-            m3_cp_commit();
+            cpa_commit();
             m3_column<PH, XF, ZF>(c, tid, q);
             if (nout) m3_derived<PH, XF, ZF>(c, tid, out[0]);
         });
@@ -522,7 +493,7 @@ FWI_HD void m3_march(MarchCtx c, int ya, int yb, Par &&par)
         mb = nmb;
         mp_plane = pf_mp ? nout1[0] : -1;
     }
-    par([&](int) { m3_cp_wait(); });
+    par([&](int) { cpa_wait(); });
 }
 
 // Chunk of planes [ya, yb) of chunk ch of nch along ny: interior boundaries
