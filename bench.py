@@ -37,19 +37,33 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BYTES_PER_UPDATE = 48  # algorithmic FP32 traffic of one elastic point update (lambda, mu, rho, prev x3, curr x3, next x3)
+# per physics: algorithmic bytes per update (acoustic: K, 1/rho, prev, curr read, next written; VTI: six
+# model arrays + nine wavefield values) and the modeling configuration of the benchmark
+PHYSICS = {
+    "elastic": {"bytes": 48, "shots": 8, "n": 256},
+    "acoustic": {"bytes": 20, "shots": 1, "n": 101},
+    "vti": {"bytes": 60, "shots": 24, "n": 0},  # 320 x 320 x 200 (n > 0: a cube of n for profiling)
+}
 
 
 _CACHE = {}
 
 
-def workload(n=256, nshots=8, nsteps=3000):
+def workload(n=256, nshots=8, nsteps=3000, physics="elastic"):
     """The seeded survey; the model is generated once per grid size and the
     wavelet cut to ``nsteps`` + 1 samples."""
     from fwi3d_b200 import synth
 
-    if n not in _CACHE:
-        _CACHE[n] = synth.elastic_layered(n=n, nsteps=4000, nshots=8)
-    base = _CACHE[n]
+    key = (physics, n)
+    if key not in _CACHE:
+        if physics == "elastic":
+            _CACHE[key] = synth.elastic_layered(n=n, nsteps=4000, nshots=8)
+        elif physics == "acoustic":
+            _CACHE[key] = synth.acoustic_linear(n=n, nsteps=4000)
+        else:
+            dims = dict(nx=n, ny=n, nz=n) if n > 0 else {}
+            _CACHE[key] = synth.vti_layered(nsteps=4000, nshots=24, **dims)
+    base = _CACHE[key]
     sv = base.shot(0) if nshots == 1 else base
     sv = synth.Survey(sv.name, sv.nmodels, sv.nx, sv.ny, sv.nz, sv.dx, sv.dy, sv.dz, sv.model,
                       np.ascontiguousarray(base.wavelet[:nsteps + 1]), sv.dt_data, sv.par.copy())
@@ -146,34 +160,53 @@ def max_over_ranks(value, world, device=None):
     return float(t.item())
 
 
-def cpu_reference(n_steps, threads, n=256):
+def cpu_reference(n_steps, threads, n=256, physics="elastic"):
     """Reference CPU code (oracle/_ref, built from the reference sources): one
     shot of the workload over an n_steps window; returns pt-updates/s."""
     from oracle import refpy
 
-    sv = workload(n=n, nshots=1, nsteps=n_steps)
+    sv = workload(n=n, nshots=1, nsteps=n_steps, physics=physics)
     t0 = time.perf_counter()
     refpy.modeling(sv, shot=0, precision="fp32", nthreads=threads)
     dt = time.perf_counter() - t0
     return sv.nxyz * n_steps / dt, dt
 
 
+def grid_label(sv):
+    return f"{sv.nx}^3" if sv.nx == sv.ny == sv.nz else f"{sv.nx}x{sv.ny}x{sv.nz}"
+
+
+def workload_label(physics, sv, ns, nr):
+    g = grid_label(sv)
+    d = sv.dx * 1000
+    if physics == "elastic":
+        return (f"elastic iso modeling {g}, {d:g} m, dt {sv.dt_data * 1e3:g} ms, {ns} moment-tensor shots batched on "
+                f"the shared model, {nr} 3-C receivers per shot")
+    if physics == "acoustic":
+        return (f"acoustic VD modeling {g}, {d:g} m, dt {sv.dt_data * 1e3:g} ms, {ns} shot, {nr} pressure receivers, "
+                f"20-point tapers, free-surface top")
+    return (f"elastic VTI modeling {g}, {d:g} m, dt {sv.dt_data * 1e3:g} ms, {ns} vertical-force shots batched on "
+            f"the shared model, {nr} 3-C receivers per shot")
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    k = min(args.steps, args.ref_cap)
+    k = max(10, min(args.steps, args.ref_cap))  # the reference needs nt >= 10 (we_op.cpp:621, 838)
     if args.warmup > 0:
-        cpu_reference(min(args.warmup, 3), threads)
-    value, secs = cpu_reference(k, threads)
-    sample = (f"1 shot of the 256^3 elastic workload, {k}-step window, whole apply_forward call "
+        cpu_reference(10, threads, n=args.n, physics=args.physics)
+    value, secs = cpu_reference(k, threads, n=args.n, physics=args.physics)
+    sv = workload(n=args.n, nshots=1, nsteps=k, physics=args.physics)
+    sample = (f"1 shot of the {grid_label(sv)} {args.physics} workload, {k}-step window, whole apply_forward call "
               f"(model analysis and setup included), OMP threads={threads}")
     line = {
         "impl": "reference", "metric": "grid-pt updates/s", "value": value, "unit": "pt/s", "n_gpus": args.gpus,
         "steps": k, "warmup": args.warmup, "ms_per_step": secs * 1e3 / k, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "elastic iso modeling 256^3, 8 shots (CPU: 1-shot bounded window)",
-                   "grid": [256, 256, 256], "shots": 8, "parallelism": "cpu"},
+        "config": {"workload": workload_label(args.physics, sv, PHYSICS[args.physics]["shots"], len(sv.par.rxyz[0]))
+                   + " (CPU: 1-shot bounded window)",
+                   "grid": [sv.nx, sv.ny, sv.nz], "shots": PHYSICS[args.physics]["shots"], "parallelism": "cpu"},
         "cpu_baseline": {"value": value, "unit": "pt/s", "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "pt/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -190,9 +223,11 @@ def run_ours(args, rank, world, local):
 
     torch.cuda.set_device(local)
     lib = _lib.load()
-    sv = workload(n=args.n, nshots=args.shots, nsteps=max(args.steps + args.warmup + 1, 301))
+    sv = workload(n=args.n, nshots=args.shots, nsteps=max(args.steps + args.warmup + 1, 301), physics=args.physics)
     ns = len(sv.par.sxyz)
-    dom = ops.Domain(sv.nx, sv.ny, sv.nz, sv.dx, sv.dy, sv.dz, 3)
+    dom = ops.Domain(sv.nx, sv.ny, sv.nz, sv.dx, sv.dy, sv.dz, sv.nmodels)
+    bpu = PHYSICS[args.physics]["bytes"]
+    nrcomp = 1 if sv.nmodels == 2 else 3
     nr = len(sv.par.rxyz[0])
     w = np.ascontiguousarray(sv.wavelet, dtype=np.float32)
     sx = np.ascontiguousarray(np.asarray(sv.par.sxyz, dtype=np.float32))
@@ -201,7 +236,7 @@ def run_ours(args, rank, world, local):
     cp = ops.to_cparam(sv.par)
 
     h = C.c_void_p()
-    _lib.check(lib.fwi_batch_create(C.byref(h), local, C.byref(dom.grid()), 3, C.byref(cp), _lib.fptr(model),
+    _lib.check(lib.fwi_batch_create(C.byref(h), local, C.byref(dom.grid()), sv.nmodels, C.byref(cp), _lib.fptr(model),
                                     _lib.fptr(w), 1, w.shape[-1], sv.dt_data, ns, _lib.fptr(sx), nr, _lib.fptr(rx)))
     sp = C.c_void_p()
     _lib.check(lib.fwi_batch_stream(h, C.byref(sp)))
@@ -241,20 +276,20 @@ def run_ours(args, rank, world, local):
     peak, peak_kind = peaks()
     launch_ms = k_ms.value / max(1, k_n.value)
     kernel = (k_name.value or b"").decode()
-    achieved = BYTES_PER_UPDATE * k_pts.value / (launch_ms * 1e-3) / 1e9 if k_n.value else None
-    step_gbs = BYTES_PER_UPDATE * units_per_step / (ms_step / 1e3) / 1e9
+    achieved = bpu * k_pts.value / (launch_ms * 1e-3) / 1e9 if k_n.value else None
+    step_gbs = bpu * units_per_step / (ms_step / 1e3) / 1e9
     tpu, tkernel = traffic_per_update()
 
     # e2e through the public C-ABI call, host buffers, 300-step time axis
     e2e = None
     if not args.no_e2e:
-        sv_e = workload(n=args.n, nshots=args.shots, nsteps=300)
+        sv_e = workload(n=args.n, nshots=args.shots, nsteps=300, physics=args.physics)
         we = np.ascontiguousarray(sv_e.wavelet, dtype=np.float32)
-        out = np.zeros((ns, 3, nr, we.shape[-1]), dtype=np.float32)
+        out = np.zeros((ns, nrcomp, nr, we.shape[-1]), dtype=np.float32)
         if world > 1:
             torch.distributed.barrier()
         t0 = time.perf_counter()
-        _lib.check(lib.fwi_forward_batch(local, C.byref(dom.grid()), 3, C.byref(cp), _lib.fptr(model), _lib.fptr(we),
+        _lib.check(lib.fwi_forward_batch(local, C.byref(dom.grid()), sv.nmodels, C.byref(cp), _lib.fptr(model), _lib.fptr(we),
                                          1, we.shape[-1], sv_e.dt_data, ns, _lib.fptr(sx), nr, _lib.fptr(rx),
                                          _lib.fptr(out)))
         te = time.perf_counter() - t0
@@ -268,28 +303,27 @@ def run_ours(args, rank, world, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        v, secs = cpu_reference(args.cpu_steps, threads)
+        v, secs = cpu_reference(args.cpu_steps, threads, n=args.n, physics=args.physics)
         cpu = {"value": v, "unit": "pt/s", "cores": threads, "kind": "reference",
-               "sample": f"reference CPU build, 1 shot of the 256^3 elastic workload, {args.cpu_steps}-step window "
-                         f"({secs:.1f} s, setup included), OMP threads={threads}"}
+               "sample": f"reference CPU build, 1 shot of the {grid_label(sv)} {args.physics} workload, "
+                         f"{args.cpu_steps}-step window ({secs:.1f} s, setup included), OMP threads={threads}"}
 
     if rank == 0:
         line = {
             "metric": "grid-pt updates/s", "value": value, "unit": "pt/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered model, Ricker sources)",
-            "config": {"workload": f"elastic iso modeling {args.n}^3, 8 m, dt 0.6 ms, {ns} moment-tensor shots "
-                                   f"batched on the shared model, {nr} 3-C receivers per shot",
-                       "grid": [args.n] * 3, "shots_per_gpu": ns, "receivers_per_shot": nr,
+            "config": {"workload": workload_label(args.physics, sv, ns, nr),
+                       "grid": [sv.nx, sv.ny, sv.nz], "shots_per_gpu": ns, "receivers_per_shot": nr,
                        "parallelism": f"shots x{world} (weak)", "l2": "working set >> L2 (no flush needed)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak if achieved else None), "peak_kind": peak_kind,
                          "traffic": (tpu * k_pts.value if tpu and tkernel == kernel else None),
                          "kernel": kernel, "launch_ms": launch_ms, "launches": k_n.value,
                          "updates_per_launch": k_pts.value,
-                         "algorithmic_bytes_per_update": BYTES_PER_UPDATE,
+                         "algorithmic_bytes_per_update": bpu,
                          "step_achieved_gbs": step_gbs,
-                         "note": "achieved = 48 B x updates per launch / mean CUDA-event time of the main kernel's "
+                         "note": f"achieved = {bpu} B x updates per launch / mean CUDA-event time of the main kernel's "
                                  "launches in the timed region; traffic = ncu DRAM bytes per update of that kernel "
                                  "(profiles/ncu_traffic.txt) x updates per launch; step_achieved_gbs covers every "
                                  "kernel of the step"},
@@ -429,8 +463,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=16)
     ap.add_argument("--ref-cap", type=int, default=40, help="max time steps of the CPU reference window")
-    ap.add_argument("--n", type=int, default=256, help="grid points per axis (profiling runs use smaller grids)")
-    ap.add_argument("--shots", type=int, default=8)
+    ap.add_argument("--physics", default="elastic", choices=sorted(PHYSICS),
+                    help="modeling workload: elastic 256^3 x 8 shots (default), acoustic 101^3 x 1, "
+                         "vti 320x320x200 x 24")
+    ap.add_argument("--n", type=int, default=None, help="grid points per axis (profiling runs use smaller grids)")
+    ap.add_argument("--shots", type=int, default=None)
     ap.add_argument("--workload", default="modeling", choices=["modeling", "gradient", "serving"])
     ap.add_argument("--requests", type=int, default=48)
     ap.add_argument("--rate", type=float, default=20.0)
@@ -441,6 +478,10 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.n is None:
+        args.n = PHYSICS[args.physics]["n"]
+    if args.shots is None:
+        args.shots = PHYSICS[args.physics]["shots"]
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

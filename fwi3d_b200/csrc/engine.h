@@ -165,6 +165,7 @@ private:
     const float *taper_ptr_[6] = {};
     int scale_ = 0;
     bool march_ = false;           // marching elastic kernel over all planes
+    bool afused_ = false;          // acoustic marching kernel (else the per-point kernel)
     bool slab_march_ = false;      // fused path: y-wall slabs by the marching kernel (else per-point kernels)
     bool fused_ = false;           // fused elastic kernel for the interior planes
     int fused_minb_ = 2;           // resident CTAs per SM the fused kernel is compiled for

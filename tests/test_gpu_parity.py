@@ -221,3 +221,23 @@ def test_das_gradient(oracle_fp32):
     sv = _das(n=26, steps=120)
     tol, _, _ = _das_tol(oracle_fp32, sv)
     _grad_case(oracle_fp32, sv, 1, trace_tol=tol)
+
+
+@pytest.mark.parametrize("bc", [(1, 2, 2, 2, 2, 2), (2, 1, 3, 2, 1, 2)])
+def test_acoustic_fused_traces(oracle_fp32, bc, monkeypatch):
+    """The acoustic marching kernel (grids with nz >= 38, nx >= 22) against the
+    oracle and against the per-point kernel (FWI_FUSED=0)."""
+    sv = synth.acoustic_linear(n=44, nsteps=150, taper=6, rec_stride=3)
+    sv.par.set_bc(*bc)
+    monkeypatch.setenv("FWI_FUSED", "1")  # the marching kernel also below its size threshold
+    d = ops.from_survey(sv).forward(False, sv.model)
+    ref, _ = oracle_fp32.modeling(sv, precision="fp32")
+    assert rel(d, ref) < TRACE_TOL
+    monkeypatch.setenv("FWI_FUSED", "0")
+    d0 = ops.from_survey(sv).forward(False, sv.model)
+    assert rel(d, d0) < 2e-6
+
+
+def test_acoustic_fused_gradient(oracle_fp32, monkeypatch):
+    monkeypatch.setenv("FWI_FUSED", "1")
+    _grad_case(oracle_fp32, synth.acoustic_linear(n=40, nsteps=120, taper=5, rec_stride=3), 1)
