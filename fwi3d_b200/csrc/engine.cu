@@ -6,7 +6,7 @@
 //   aux       first-derivative scratch (elastic/VTI)        k_elastic_aux
 //   step      D2var + D1 terms + SAT + update + scale + taper, fused   k_*_step
 //   inject    sources (receivers' residual in the adjoint)  k_inject
-// and, every `sub` steps of the adjoint, the imaging condition k_*_image.
+// and, every `sub` steps of the adjoint, the imaging condition k_image_batch.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -389,19 +389,33 @@ __global__ void k_extract(const float *u, int64_t sst, int64_t nxyz, int ncomp, 
     rcv[(((int64_t)sh * ncomp + c) * nr + r) * nt + it] = acc;
 }
 
-__global__ void k_acoustic_image(ImageArgs a)
-{
-    int ix, iy, iz, s;
-    if (!point_of(a.g, (a.g.ny + BY - 1) / BY, ix, iy, iz, s)) return;
-    acoustic_image_point(a, ix, iy, iz);
-}
-
+// Imaging of every shot of a batch at once: the increments of the shots
+// (fields at offsets s * sst) are summed in FP64 per point, then added to the
+// gradient once.
 template <int PH>
-__global__ void k_elastic_image(ImageArgs a)
+__global__ void k_image_batch(ImageArgs a, int nshots, int64_t sst)
 {
     int ix, iy, iz, s;
     if (!point_of(a.g, (a.g.ny + BY - 1) / BY, ix, iy, iz, s)) return;
-    elastic_image_point<PH>(a, ix, iy, iz);
+    const int64_t i = a.g.idx(ix, iy, iz);
+    double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+    for (int sh = 0; sh < nshots; sh++) {
+        if (PH == ACOUSTIC) {
+            double k, b;
+            acoustic_image_inc(a, sh * sst, ix, iy, iz, k, b);
+            g0 -= k;
+            g1 += b;
+        } else {
+            double i0, i1, i2;
+            elastic_image_inc<PH>(a, sh * sst, ix, iy, iz, i0, i1, i2);
+            g0 += i0;
+            g1 += i1;
+            g2 += i2;
+        }
+    }
+    a.grad[0][i] += g0;
+    a.grad[1][i] += g1;
+    if (PH != ACOUSTIC) a.grad[2][i] += g2;
 }
 
 __global__ void k_d2f(const double *in, float *out, int64_t n)
@@ -1192,20 +1206,18 @@ void Engine::image(int itl, const float *curr, const float *prevl)
         lev[l] = snap_fp32(std::min(std::max(k, 0), nsnap_ - 1));
     }
     const dim3 blk(BZ, BX, BY), grd = grid_of(a.g, 1);
-    for (int sh = 0; sh < pb_.nshots; sh++) {
-        const int64_t so = (int64_t)sh * nc * n;
-        for (int l = 0; l < 3; l++)
-            for (int c = 0; c < 3; c++) a.fwd[l][c] = lev[l] + so + (int64_t)(c < nc ? c : 0) * n;
-        for (int c = 0; c < 3; c++) {
-            const int cc = c < nc ? c : 0;
-            a.adj[c] = curr + so + cc * n;
-            a.lag[c] = prevl + so + cc * n;
-            a.grad[c] = grad_.as<double>() + (int64_t)(c < (pb_.nmodels == 2 ? 2 : 3) ? c : 0) * n;
-        }
-        if (pb_.nmodels == 2) k_acoustic_image<<<grd, blk, 0, s>>>(a);
-        else if (pb_.nmodels == 3) k_elastic_image<ELASTIC><<<grd, blk, 0, s>>>(a);
-        else k_elastic_image<VTI><<<grd, blk, 0, s>>>(a);
+    for (int l = 0; l < 3; l++)
+        for (int c = 0; c < 3; c++) a.fwd[l][c] = lev[l] + (int64_t)(c < nc ? c : 0) * n;
+    for (int c = 0; c < 3; c++) {
+        const int cc = c < nc ? c : 0;
+        a.adj[c] = curr + cc * n;
+        a.lag[c] = prevl + cc * n;
+        a.grad[c] = grad_.as<double>() + (int64_t)(c < (pb_.nmodels == 2 ? 2 : 3) ? c : 0) * n;
     }
+    const int64_t sst = (int64_t)nc * n;
+    if (pb_.nmodels == 2) k_image_batch<ACOUSTIC><<<grd, blk, 0, s>>>(a, pb_.nshots, sst);
+    else if (pb_.nmodels == 3) k_image_batch<ELASTIC><<<grd, blk, 0, s>>>(a, pb_.nshots, sst);
+    else k_image_batch<VTI><<<grd, blk, 0, s>>>(a, pb_.nshots, sst);
     CK(cudaGetLastError());
 }
 

@@ -30,29 +30,32 @@ FWI_HD float dx1(const Dims &g, const float *p, int ix, int iy, int iz, float d)
 FWI_HD float dy1(const Dims &g, const float *p, int ix, int iy, int iz, float d) { return d1_row(g.ly(p, ix, iz), iy, g.ny) / d; }
 FWI_HD float dz1(const Dims &g, const float *p, int ix, int iy, int iz, float d) { return d1_row(g.lz(p, ix, iy), iz, g.nz) / d; }
 
+// Increments of the three gradients at one point for the shot whose fields
+// start at offset `so` (batches: shot s at s * shot stride).
 template <int PH>
-FWI_HD void elastic_image_point(const ImageArgs &a, int ix, int iy, int iz)
+FWI_HD void elastic_image_inc(const ImageArgs &a, int64_t so, int ix, int iy, int iz, double &inc0, double &inc1,
+                              double &inc2)
 {
     const Dims &g = a.g;
     const int64_t i = g.idx(ix, iy, iz);
-    const float *const *fn = a.fwd[1];
+    const float *const fn[3] = {a.fwd[1][0] + so, a.fwd[1][1] + so, a.fwd[1][2] + so};
+    const float *const lag[3] = {a.lag[0] + so, a.lag[1] + so, a.lag[2] + so};
     // forward strains at the imaging time (we_op.cpp:510-518)
     const float t0 = dx1(g, fn[0], ix, iy, iz, a.dx), t1 = dy1(g, fn[1], ix, iy, iz, a.dy), t2 = dz1(g, fn[2], ix, iy, iz, a.dz);
     const float t3 = dx1(g, fn[2], ix, iy, iz, a.dx), t4 = dz1(g, fn[0], ix, iy, iz, a.dz);
     const float t5 = dx1(g, fn[1], ix, iy, iz, a.dx), t6 = dy1(g, fn[0], ix, iy, iz, a.dy);
     const float t7 = dy1(g, fn[2], ix, iy, iz, a.dy), t8 = dz1(g, fn[1], ix, iy, iz, a.dz);
     // adjoint strains (of the previous adjoint step)
-    const float ax0 = dx1(g, a.lag[0], ix, iy, iz, a.dx), ax1 = dx1(g, a.lag[1], ix, iy, iz, a.dx),
-                ax2 = dx1(g, a.lag[2], ix, iy, iz, a.dx);
-    const float ay0 = dy1(g, a.lag[0], ix, iy, iz, a.dy), ay1 = dy1(g, a.lag[1], ix, iy, iz, a.dy),
-                ay2 = dy1(g, a.lag[2], ix, iy, iz, a.dy);
-    const float az0 = dz1(g, a.lag[0], ix, iy, iz, a.dz), az1 = dz1(g, a.lag[1], ix, iy, iz, a.dz),
-                az2 = dz1(g, a.lag[2], ix, iy, iz, a.dz);
+    const float ax0 = dx1(g, lag[0], ix, iy, iz, a.dx), ax1 = dx1(g, lag[1], ix, iy, iz, a.dx),
+                ax2 = dx1(g, lag[2], ix, iy, iz, a.dx);
+    const float ay0 = dy1(g, lag[0], ix, iy, iz, a.dy), ay1 = dy1(g, lag[1], ix, iy, iz, a.dy),
+                ay2 = dy1(g, lag[2], ix, iy, iz, a.dy);
+    const float az0 = dz1(g, lag[0], ix, iy, iz, a.dz), az1 = dz1(g, lag[1], ix, iy, iz, a.dz),
+                az2 = dz1(g, lag[2], ix, iy, iz, a.dz);
     const float dt = a.dtimg;
     const bool first = a.itl == 0;
     const bool mid = a.itl > 0 && a.itl < a.last;
     float glam, gmu;
-    double inc0, inc1;
     if (PH == ELASTIC) {
         // dt (div adj) (div fwd): the reference multiplies dt into the first factor
         const float A = ax0 + ay1 + az2, B = t0 + t1 + t2;
@@ -75,40 +78,56 @@ FWI_HD void elastic_image_point(const ImageArgs &a, int ix, int iy, int iz)
     inc1 = first ? 0.5 * dt * gmu : (double)(dt * gmu);
     float s = 0.f;
     for (int c = 0; c < 3; c++) {
-        const float fp = a.fwd[2][c][i], f0 = a.fwd[1][c][i];
+        const float fp = a.fwd[2][c][so + i], f0 = a.fwd[1][c][so + i];
         float tt;
-        if (mid) tt = fp - 2 * f0 + a.fwd[0][c][i];
+        if (mid) tt = fp - 2 * f0 + a.fwd[0][c][so + i];
         else if (first) tt = fp - f0;
-        else tt = -f0 + a.fwd[0][c][i];
-        s = (c == 0) ? a.adj[c][i] * tt : s + a.adj[c][i] * tt;
+        else tt = -f0 + a.fwd[0][c][so + i];
+        s = (c == 0) ? a.adj[c][so + i] * tt : s + a.adj[c][so + i] * tt;
     }
-    const double inc2 = 1.0 / dt * s;
+    inc2 = 1.0 / dt * s;
+}
+
+template <int PH>
+FWI_HD void elastic_image_point(const ImageArgs &a, int ix, int iy, int iz)
+{
+    const int64_t i = a.g.idx(ix, iy, iz);
+    double inc0, inc1, inc2;
+    elastic_image_inc<PH>(a, 0, ix, iy, iz, inc0, inc1, inc2);
     a.grad[0][i] += inc0;
     a.grad[1][i] += inc1;
     a.grad[2][i] += inc2;
 }
 
-FWI_HD void acoustic_image_point(const ImageArgs &a, int ix, int iy, int iz)
+FWI_HD void acoustic_image_inc(const ImageArgs &a, int64_t so, int ix, int iy, int iz, double &inck, double &incb)
 {
     const Dims &g = a.g;
     const int64_t i = g.idx(ix, iy, iz);
-    const float *fn = a.fwd[1][0];
+    const float *fn = a.fwd[1][0] + so;
     const float t0 = dx1(g, fn, ix, iy, iz, a.dx), t1 = dy1(g, fn, ix, iy, iz, a.dy), t2 = dz1(g, fn, ix, iy, iz, a.dz);
-    const float *ad = a.adj[0];
+    const float *ad = a.adj[0] + so;
     const float t3 = dx1(g, ad, ix, iy, iz, a.dx), t4 = dy1(g, ad, ix, iy, iz, a.dy), t5 = dz1(g, ad, ix, iy, iz, a.dz);
     const float dt = a.dtimg;
     const float K = a.m[0][i];
     const bool first = a.itl == 0;
     const bool mid = a.itl > 0 && a.itl < a.last;
-    const float fp = a.fwd[2][0][i], f0 = a.fwd[1][0][i];
+    const float fp = a.fwd[2][0][so + i], f0 = a.fwd[1][0][so + i];
     float tt;
-    if (mid) tt = fp - 2 * f0 + a.fwd[0][0][i];
+    if (mid) tt = fp - 2 * f0 + a.fwd[0][0][so + i];
     else if (first) tt = fp - f0;
-    else tt = -2 * f0 + a.fwd[0][0][i];  // the reference's last-sample form (we_op.cpp:1601)
+    else tt = -2 * f0 + a.fwd[0][0][so + i];  // the reference's last-sample form (we_op.cpp:1601)
     const float q = t3 * t0 + t4 * t1 + t5 * t2;
-    const double inck = 1.0 / (double)(dt * K * K) * (double)ad[i] * (double)tt;
+    inck = 1.0 / (double)(dt * K * K) * (double)ad[i] * (double)tt;
+    incb = first ? 0.5 * dt * q : (double)(dt * q);
+}
+
+FWI_HD void acoustic_image_point(const ImageArgs &a, int ix, int iy, int iz)
+{
+    const int64_t i = a.g.idx(ix, iy, iz);
+    double inck, incb;
+    acoustic_image_inc(a, 0, ix, iy, iz, inck, incb);
     a.grad[0][i] -= inck;
-    a.grad[1][i] += first ? 0.5 * dt * q : (double)(dt * q);
+    a.grad[1][i] += incb;
 }
 
 }  // namespace fwi
