@@ -175,13 +175,32 @@ FWI_HD void fz_load_u(FusedCtx &c, int tid, int q, int slot)
     }
 }
 
+// Position p of the derived region (XH x ZH = 20 x 36): the 32 columns
+// zh = 2..33 row by row first, so that a warp covers one row of the tile
+// (no shared-memory bank conflicts), then the four halo columns.
+FWI_HD void fz_dpos(int p, int &xh, int &zh)
+{
+    constexpr int MAIN = fz::XH * fz::TZ;  // 640
+    static_assert(fz::TZ == 32 && fz::ZH == fz::TZ + 4, "warp-row mapping assumes 32 + 2 x 2 columns");
+    if (p < MAIN) {
+        xh = p >> 5;
+        zh = fz::HD + (p & 31);
+    } else {
+        const int h = p - MAIN;
+        xh = h >> 2;
+        const int zc = h & 3;
+        zh = zc < 2 ? zc : fz::TZ + zc;
+    }
+}
+
 // Material planes at y over the derived region.
 template <int PH>
 FWI_HD void fz_load_mat(FusedCtx &c, int tid, int y)
 {
     const Dims &g = c.a->g;
     for (int p = tid; p < fz::XH * fz::ZH; p += fz::NT) {
-        const int xh = p / fz::ZH, zh = p - xh * fz::ZH;
+        int xh, zh;
+        fz_dpos(p, xh, zh);
         const int ix = c.x0 - fz::HD + xh, iz = c.z0 - fz::HD + zh;
         const bool in = ix >= 0 && ix < g.nx && iz >= 0 && iz < g.nz;
         const int64_t i = in ? g.idx(ix, y, iz) : 0;
@@ -252,7 +271,8 @@ FWI_HD void fz_derived(FusedCtx &c, int tid, int y)
 {
     const Dims &g = c.a->g;
     for (int p = tid; p < fz::XH * fz::ZH; p += fz::NT) {
-        const int xh = p / fz::ZH, zh = p - xh * fz::ZH;
+        int xh, zh;
+        fz_dpos(p, xh, zh);
         const int ix = c.x0 - fz::HD + xh, iz = c.z0 - fz::HD + zh;
         auto dv = [&](int d) -> float & { return fz_dvp(c.sm, d)[xh][zh]; };
         if (!F && (ix < 0 || ix >= g.nx || iz < 0 || iz >= g.nz)) {
