@@ -126,7 +126,7 @@ __global__ void k_elastic_step(StepArgs a)
     b.next[2][i] = v2;
 }
 
-template <int PH, bool F>
+template <int PH, bool XF, bool ZF>
 __device__ __forceinline__ void fused_march(FusedCtx &c, int tid, int ya, int yb)
 {
     FusedThread th;
@@ -147,12 +147,12 @@ __device__ __forceinline__ void fused_march(FusedCtx &c, int tid, int ya, int yb
             fz_load_u<true>(c, tid, y + 5, ring<PH>(y + 5));
             cpa_commit();
         }
-        fz_column<PH, F>(c, th, tid, y + 2);
-        if (y >= ya) fz_derived<PH, F>(c, tid, y);
+        fz_column<PH, XF, ZF>(c, th, tid, y + 2);
+        if (y >= ya) fz_derived<PH, XF, ZF>(c, tid, y);
         __syncthreads();
         if (y >= ya) {
-            if (F) fz_output_fast<PH>(c, th, tid, y);
-            else fz_output<PH>(c, th, tid, y);
+            if (PH == ELASTIC && !(XF && ZF)) fz_output<PH>(c, th, tid, y);
+            else fz_output_t<PH, XF, ZF>(c, th, tid, y);
         }
         __syncthreads();
     }
@@ -180,9 +180,14 @@ __global__ void __launch_bounds__(fz::NT, MINB) k_elastic_fused(const __grid_con
     if (ya >= yb) return;
     // tiles whose outputs and derived halo are interior in x and z take the
     // closure-free code (block-uniform branch)
-    const bool fast = c.x0 >= 6 && c.x0 + fz::TX <= a.g.nx - 6 && c.z0 >= 6 && c.z0 + fz::TZ <= a.g.nz - 6;
-    if (fast) fused_march<PH, true>(c, tid, ya, yb);
-    else fused_march<PH, false>(c, tid, ya, yb);
+    // interior tiles take the closure-free code on both axes; edge tiles of
+    // the VTI kernel keep it on their interior axis, those of the isotropic
+    // kernel (which measured faster so under the 64-register bound) do not
+    const bool xf = c.x0 >= 6 && c.x0 + fz::TX <= a.g.nx - 6, zf = c.z0 >= 6 && c.z0 + fz::TZ <= a.g.nz - 6;
+    if (xf && zf) fused_march<PH, true, true>(c, tid, ya, yb);
+    else if (PH == VTI && xf) fused_march<PH, true, false>(c, tid, ya, yb);
+    else if (PH == VTI && zf) fused_march<PH, false, true>(c, tid, ya, yb);
+    else fused_march<PH, false, false>(c, tid, ya, yb);
 }
 
 // Acoustic marching step (see acoustic.cuh).  grid: (z tiles, x tiles,

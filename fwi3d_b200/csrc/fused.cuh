@@ -266,7 +266,7 @@ FWI_HD float fz_dy(const FusedCtx &c, int k, const int *sn, int ixw, int izw)
 // ---------------------------------------------------------------------------
 // Phase B1: derived quantities of plane y over the derived region.
 // ---------------------------------------------------------------------------
-template <int PH, bool F = false>
+template <int PH, bool XF = false, bool ZF = false>
 FWI_HD void fz_derived(FusedCtx &c, int tid, int y)
 {
     const Dims &g = c.a->g;
@@ -275,20 +275,20 @@ FWI_HD void fz_derived(FusedCtx &c, int tid, int y)
         fz_dpos(p, xh, zh);
         const int ix = c.x0 - fz::HD + xh, iz = c.z0 - fz::HD + zh;
         auto dv = [&](int d) -> float & { return fz_dvp(c.sm, d)[xh][zh]; };
-        if (!F && (ix < 0 || ix >= g.nx || iz < 0 || iz >= g.nz)) {
+        if (!(XF && ZF) && (ix < 0 || ix >= g.nx || iz < 0 || iz >= g.nz)) {
             for (int k = 0; k < (PH == ELASTIC ? NDVC : NDV); k++) dv(k) = 0.f;
             continue;
         }
         const int ixw = xh + (fz::HW - fz::HD), izw = zh + (fz::HW - fz::HD);
         const int s0 = c.sl[2];
         const int sn[4] = {c.sl[0], c.sl[1], c.sl[3], c.sl[4]};
-        const float ux0 = fz_dx<F>(c, 0, s0, ix, izw);
+        const float ux0 = fz_dx<XF>(c, 0, s0, ix, izw);
         const float uy1 = fz_dy(c, 1, sn, ixw, izw);
-        const float uz2 = fz_dz<F>(c, 2, s0, ixw, iz);
+        const float uz2 = fz_dz<ZF>(c, 2, s0, ixw, iz);
         const float mu = fz_mpp(c.sm, MP_MU)[xh][zh], lam = fz_mpp(c.sm, MP_LAM)[xh][zh];
         const float uy0 = fz_dy(c, 0, sn, ixw, izw);
-        const float uz0 = fz_dz<F>(c, 0, s0, ixw, iz);
-        const float ux2 = fz_dx<F>(c, 2, s0, ix, izw);
+        const float uz0 = fz_dz<ZF>(c, 0, s0, ixw, iz);
+        const float ux2 = fz_dx<XF>(c, 2, s0, ix, izw);
         const float uy2 = fz_dy(c, 2, sn, ixw, izw);
         if (PH == ELASTIC) {
             dv(DV_T0) = lam * (ux0 + uy1 + uz2);  // also the z-differentiated T2
@@ -309,7 +309,7 @@ FWI_HD void fz_derived(FusedCtx &c, int tid, int y)
 }
 
 // Phase B2: own-column quantities of plane q = y+2 pushed into the y queues.
-template <int PH, bool F = false>
+template <int PH, bool XF = false, bool ZF = false>
 FWI_HD void fz_column(FusedCtx &c, FusedThread &th, int tid, int q)
 {
     const Dims &g = c.a->g;
@@ -334,11 +334,11 @@ FWI_HD void fz_column(FusedCtx &c, FusedThread &th, int tid, int q)
     // plane q = y+2 sits in slot sl[4]; its neighbours q-2..q+2 in sl[2..6]
     const int s0 = c.sl[4];
     const int sn[4] = {c.sl[2], c.sl[3], c.sl[5], c.sl[6]};
-    const float ux0 = fz_dx<F>(c, 0, s0, ix, izw);
+    const float ux0 = fz_dx<XF>(c, 0, s0, ix, izw);
     const float uy1 = fz_dy(c, 1, sn, ixw, izw);
-    const float uz2 = fz_dz<F>(c, 2, s0, ixw, iz);
-    const float ux1 = fz_dx<F>(c, 1, s0, ix, izw);
-    const float uz1 = fz_dz<F>(c, 1, s0, ixw, iz);
+    const float uz2 = fz_dz<ZF>(c, 2, s0, ixw, iz);
+    const float ux1 = fz_dx<XF>(c, 1, s0, ix, izw);
+    const float uz1 = fz_dz<ZF>(c, 1, s0, ixw, iz);
     if (PH == ELASTIC) {
         th.qT[4] = lam * (ux0 + uy1 + uz2);
         th.qX1[4] = ux1;
@@ -545,11 +545,12 @@ FWI_HD void fz_output(FusedCtx &c, const FusedThread &th, int tid, int y)
     }
 }
 
-// Output phase of a tile whose outputs and derived halo are all interior in x
-// and z (every stencil is the interior one): same terms as fz_output, taps
-// read at constant offsets from per-point base pointers.
-template <int PH>
-FWI_HD void fz_output_fast(FusedCtx &c, const FusedThread &th, int tid, int y)
+// Output phase with the taps read at constant offsets from per-point base
+// pointers.  XF (ZF): every output and derived-halo point of the tile is
+// interior along x (z); otherwise the rows of the SBP closures along that
+// axis take the closure code, the other points the interior code.
+template <int PH, bool XF, bool ZF>
+FWI_HD void fz_output_t(FusedCtx &c, const FusedThread &th, int tid, int y)
 {
     const StepArgs &a = *c.a;
     const Dims &g = a.g;
@@ -559,17 +560,25 @@ FWI_HD void fz_output_fast(FusedCtx &c, const FusedThread &th, int tid, int y)
     const int64_t i = g.idx(ix, y, iz);
     const int ixw = lx + fz::HW, izw = lz + fz::HW;
     const int xh = lx + fz::HD, zh = lz + fz::HD;
+    const bool xin = XF || (ix >= 6 && ix < g.nx - 6);
+    const bool zin = ZF || (iz >= 6 && iz < g.nz - 6);
     FusedSmem &s = *c.sm;
     constexpr int UX = fz::ZW, UC = fz::XW * fz::ZW, US = 3 * fz::XW * fz::ZW, DX = fz::ZH;
     const float *ub = &s.u[0][0][ixw][izw];
     const int r0 = c.sl[2] * US, rm1 = c.sl[1] * US, rm2 = c.sl[0] * US, rp1 = c.sl[3] * US, rp2 = c.sl[4] * US;
     const float *mu = &fz_mpp(&s, MP_MU)[xh][zh];
     const float idx2 = a.ad1[0], idy2 = a.ad1[1];
+    const SX mux = mx_line(c, MP_MU, zh);
+    const SZ muz = mz_line(c, MP_MU, xh);
     float acc[3];
-    const W5 wxm = d2w(mu[-2 * DX], mu[-DX], mu[0], mu[DX], mu[2 * DX]);
-    const W5 wz = d2w(mu[-2], mu[-1], mu[0], mu[1], mu[2]);
     const W5 wym = d2w(th.qmu[0], th.qmu[1], th.qmu[2], th.qmu[3], th.qmu[4]);
     if (PH == ELASTIC) {
+        W5 wx{}, wz{};
+        W8 wxc{}, wzc{};
+        if (xin) wx = d2w(mu[-2 * DX], mu[-DX], mu[0], mu[DX], mu[2 * DX]);
+        else wxc = d2closure_weights(mux, ix, g.nx);
+        if (zin) wz = d2w(mu[-2], mu[-1], mu[0], mu[1], mu[2]);
+        else wzc = d2closure_weights(muz, iz, g.nz);
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             const float adx = k == 0 ? a.ad2[0] : a.ad1[0];
@@ -577,16 +586,25 @@ FWI_HD void fz_output_fast(FusedCtx &c, const FusedThread &th, int tid, int y)
             const float adz = k == 2 ? a.ad2[2] : a.ad1[2];
             const float *u = ub + k * UC + r0;
             const float *uc = ub + k * UC;
-            float v = d2apply(wxm, adx, u[-2 * UX], u[-UX], u[0], u[UX], u[2 * UX]);
+            float v = xin ? d2apply(wx, adx, u[-2 * UX], u[-UX], u[0], u[UX], u[2 * UX])
+                          : d2closure_apply(wxc, ux_line(c, c.sl[2], k, izw), ix, g.nx, adx);
             v += d2apply(wym, ady, uc[rm2], uc[rm1], u[0], uc[rp1], uc[rp2]);
-            v += d2apply(wz, adz, u[-2], u[-1], u[0], u[1], u[2]);
+            v += zin ? d2apply(wz, adz, u[-2], u[-1], u[0], u[1], u[2])
+                     : d2closure_apply(wzc, uz_line(c, c.sl[2], k, ixw), iz, g.nz, adz);
             acc[k] = v;
         }
     } else {
         const float *ep = &fz_mpp(&s, MP_EPS)[xh][zh], *c6 = &fz_mpp(&s, MP_C66)[xh][zh];
+        const C11bS<SX, SX> bx{mx_line(c, MP_EPS, zh), mux};
+        const SX c6x = mx_line(c, MP_C66, zh);
         auto c11b = [&](int o) { return 2.f * (1.f + 2.f * ep[o]) * mu[o]; };
-        const W5 wxb = d2w(c11b(-2 * DX), c11b(-DX), c11b(0), c11b(DX), c11b(2 * DX));
-        const W5 wx6 = d2w(c6[-2 * DX], c6[-DX], c6[0], c6[DX], c6[2 * DX]);
+        W5 wxb{}, wx6{}, wxm{}, wz{};
+        if (xin) {
+            wxb = d2w(c11b(-2 * DX), c11b(-DX), c11b(0), c11b(DX), c11b(2 * DX));
+            wx6 = d2w(c6[-2 * DX], c6[-DX], c6[0], c6[DX], c6[2 * DX]);
+            wxm = d2w(mu[-2 * DX], mu[-DX], mu[0], mu[DX], mu[2 * DX]);
+        }
+        if (zin) wz = d2w(mu[-2], mu[-1], mu[0], mu[1], mu[2]);
         float qb[5];
 #pragma unroll
         for (int k = 0; k < 5; k++) qb[k] = 2.f * (1.f + 2.f * th.qeps[k]) * th.qmu[k];
@@ -599,37 +617,57 @@ FWI_HD void fz_output_fast(FusedCtx &c, const FusedThread &th, int tid, int y)
             const float adz = k == 2 ? a.ad2[2] : a.ad1[2];
             const float *u = ub + k * UC + r0;
             const float *uc = ub + k * UC;
-            float v = d2apply(wx, idx2, u[-2 * UX], u[-UX], u[0], u[UX], u[2 * UX]);
+            float v;
+            if (xin) {
+                v = d2apply(wx, idx2, u[-2 * UX], u[-UX], u[0], u[UX], u[2 * UX]);
+            } else {
+                const SX ul = ux_line(c, c.sl[2], k, izw);
+                v = k == 0 ? d2var_row(ul, bx, ix, g.nx, idx2)
+                           : (k == 1 ? d2var_row(ul, c6x, ix, g.nx, idx2) : d2var_row(ul, mux, ix, g.nx, idx2));
+            }
             v += d2apply(wy, idy2, uc[rm2], uc[rm1], u[0], uc[rp1], uc[rp2]);
-            v += d2apply(wz, adz, u[-2], u[-1], u[0], u[1], u[2]);
+            v += zin ? d2apply(wz, adz, u[-2], u[-1], u[0], u[1], u[2])
+                     : d2var_row(uz_line(c, c.sl[2], k, ixw), muz, iz, g.nz, adz);
             acc[k] = v;
         }
     }
     // D1 of the stress combinations and the mixed terms (we_op.cpp:661-688, 1312-1349)
     const float *P = (PH == VTI) ? &fz_mpp(&s, MP_C66)[xh][zh] : mu;
+    const SX Px = (PH == VTI) ? mx_line(c, MP_C66, zh) : mux;
     const float *qP = (PH == VTI) ? th.q66 : th.qmu;
-    const float *t0 = &fz_dvp(&s, DV_T0)[xh][zh], *t2 = &fz_dvp(&s, PH == ELASTIC ? DV_T0 : DV_T2)[xh][zh];
+    const int DT2 = PH == ELASTIC ? DV_T0 : DV_T2;
+    const float *t0 = &fz_dvp(&s, DV_T0)[xh][zh], *t2 = &fz_dvp(&s, DT2)[xh][zh];
     const float *x2 = &fz_dvp(&s, DV_X2)[xh][zh], *y0 = &fz_dvp(&s, DV_Y0)[xh][zh];
     const float *y2 = &fz_dvp(&s, DV_Y2)[xh][zh], *z0 = &fz_dvp(&s, DV_Z0)[xh][zh];
-    acc[0] += d1i(t0[-2 * DX], t0[-DX], t0[DX], t0[2 * DX]) * a.idx;
+    // each term is added where it is formed, so that few values are live at once
+    // comp 0: Dx(T0)/dx + Dy(P u_x1)/dy + Dz(mu u_x2)/dy (dy as in the reference, we_op.cpp:678)
+    acc[0] += (xin ? d1i(t0[-2 * DX], t0[-DX], t0[DX], t0[2 * DX]) : d1_row(dx_line(c, DV_T0, zh), ix, g.nx)) * a.idx;
     acc[0] += d1m(th.qX1[0], qP[0], th.qX1[1], qP[1], th.qX1[3], qP[3], th.qX1[4], qP[4]) * a.idy;
-    acc[0] += d1m(x2[-2], mu[-2], x2[-1], mu[-1], x2[1], mu[1], x2[2], mu[2]) * a.idy;  // dy as the reference
+    acc[0] += (zin ? d1m(x2[-2], mu[-2], x2[-1], mu[-1], x2[1], mu[1], x2[2], mu[2])
+                   : d1_prod_row(dz_line(c, DV_X2, xh), muz, iz, g.nz)) * a.idy;
+    // comp 1: Dy(T1)/dy + Dx(P u_y0)/dx + Dz(mu u_y2)/dz
     acc[1] += d1i(th.qT[0], th.qT[1], th.qT[3], th.qT[4]) * a.idy;
-    acc[1] += d1m(y0[-2 * DX], P[-2 * DX], y0[-DX], P[-DX], y0[DX], P[DX], y0[2 * DX], P[2 * DX]) * a.idx;
-    acc[1] += d1m(y2[-2], mu[-2], y2[-1], mu[-1], y2[1], mu[1], y2[2], mu[2]) * a.idz;
-    acc[2] += d1i(t2[-2], t2[-1], t2[1], t2[2]) * a.idz;
-    acc[2] += d1m(z0[-2 * DX], mu[-2 * DX], z0[-DX], mu[-DX], z0[DX], mu[DX], z0[2 * DX], mu[2 * DX]) * a.idx;
+    acc[1] += (xin ? d1m(y0[-2 * DX], P[-2 * DX], y0[-DX], P[-DX], y0[DX], P[DX], y0[2 * DX], P[2 * DX])
+                   : d1_prod_row(dx_line(c, DV_Y0, zh), Px, ix, g.nx)) * a.idx;
+    acc[1] += (zin ? d1m(y2[-2], mu[-2], y2[-1], mu[-1], y2[1], mu[1], y2[2], mu[2])
+                   : d1_prod_row(dz_line(c, DV_Y2, xh), muz, iz, g.nz)) * a.idz;
+    // comp 2: Dz(T2)/dz + Dx(mu u_z0)/dx + Dy(mu u_z1)/dy
+    acc[2] += (zin ? d1i(t2[-2], t2[-1], t2[1], t2[2]) : d1_row(dz_line(c, DT2, xh), iz, g.nz)) * a.idz;
+    acc[2] += (xin ? d1m(z0[-2 * DX], mu[-2 * DX], z0[-DX], mu[-DX], z0[DX], mu[DX], z0[2 * DX], mu[2 * DX])
+                   : d1_prod_row(dx_line(c, DV_Z0, zh), mux, ix, g.nx)) * a.idx;
     acc[2] += d1m(th.qZ1[0], th.qmu[0], th.qZ1[1], th.qmu[1], th.qZ1[3], th.qmu[3], th.qZ1[4], th.qmu[4]) * a.idy;
 
-    // update, taper (no boundary face in a fast tile; SAT is added by the face kernel)
+    // update, scaling (x/z faces), taper; SAT is added by the face kernel
     const float dt2 = a.dt * a.dt;
     const float irho = 1.0f / a.m[2][i];
+    const bool face = !(XF && ZF) && (ix == 0 || ix == g.nx - 1 || iz == 0 || iz == g.nz - 1);
     const bool tz = in_taper(a, ix, y, iz);
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         const float p = a.prev[k][c.so + i];
         const float pe = (a.taper_prev && tz) ? taper(a, p, ix, y, iz) : p;
         float v = dt2 * acc[k] * irho + 2.f * ub[k * UC + r0] - pe;
+        if (face) v = boundary_scale(a, v, k, ix, y, iz);
         if (tz) v = taper(a, v, ix, y, iz);
         a.next[k][c.so + i] = v;
     }
