@@ -7,6 +7,8 @@
 //   step      D2var + D1 terms + SAT + update + scale + taper, fused   k_*_step
 //   inject    sources (receivers' residual in the adjoint)  k_inject
 // and, every `sub` steps of the adjoint, the imaging condition k_image_batch.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -126,27 +128,105 @@ __global__ void k_elastic_step(StepArgs a)
     b.next[2][i] = v2;
 }
 
+// Tensor map of one time level for the fused kernel's plane copies: 5-D
+// (z, x, y, component, shot) over the [shot][component][y][x][z] layout, box
+// ZW x XW x 1 x 3 x 1 = one ring slot; out-of-grid positions read as zeros.
+struct FusedTma {
+    CUtensorMap u;
+    int *err;  // set to 1 when a wait for a copy gave up
+    int on;
+};
+
+__device__ __forceinline__ unsigned fz_saddr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void fz_bar_init(FusedCtx &c)
+{
+    for (int k = 0; k < 8; k++)
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(fz_saddr(&c.sm->bar[k])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+
+// One thread: copy plane q (three components, tile window with halo) into
+// ring slot `slot`; completion is signalled on the slot's barrier.
+__device__ __forceinline__ void fz_tma_issue(const FusedCtx &c, int q, int slot)
+{
+    const unsigned bar = fz_saddr(&c.sm->bar[slot]);
+    // order the block's earlier shared-memory accesses of the slot before the copy
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(FZ_PLANE_BYTES)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5, %6}], [%7];\n" ::"r"(fz_saddr(&c.sm->u[slot][0][0][0])),
+        "l"(c.tmap), "r"(c.z0 - fz::HW), "r"(c.x0 - fz::HW), "r"(q), "r"(0), "r"(c.shot), "r"(bar)
+        : "memory");
+}
+
+// Every thread: wait for the copy into `slot`.  The wait gives up after two
+// seconds (the copy takes microseconds), sets the error flag that the host
+// reads at its next synchronisation, and later waits of this thread return
+// at once, so that the kernel always ends.
+__device__ __forceinline__ void fz_tma_wait(FusedCtx &c, int slot)
+{
+    const unsigned bar = fz_saddr(&c.sm->bar[slot]);
+    const unsigned parity = (c.ph >> slot) & 1u;
+    c.ph ^= 1u << slot;
+    if (c.dead) return;
+    unsigned long long t0 = 0;
+    for (;;) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return;
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (t0 == 0) {
+            t0 = t;
+        } else if (t - t0 > 2000000000ull) {
+            atomicOr(c.err, 1);
+            c.dead = true;
+            return;
+        }
+    }
+}
+
 template <int PH, bool XF, bool ZF>
 __device__ __forceinline__ void fused_march(FusedCtx &c, int tid, int ya, int yb)
 {
     FusedThread th;
 #pragma unroll
     for (int k = 0; k < 5; k++) th.qmu[k] = th.qeps[k] = th.q66[k] = th.qT[k] = th.qX1[k] = th.qZ1[k] = 0.f;
+    if (c.tma && tid == 0) fz_bar_init(c);
     fz_prologue<PH>(c, tid, ya);
     __syncthreads();
     for (int y = ya - 4; y < yb; y++) {
         fz_slots<PH>(c, y);
-        // the elastic kernel copies plane y+4 in during the previous iteration
-        if (PH == VTI || y == ya - 4) fz_load_u(c, tid, y + 4, c.sl[6]);
-        else cpa_wait();
+        // plane y+4: copied in here (VTI, first step) or during the previous
+        // iteration (elastic); with bulk-tensor copies it is waited for just
+        // before the column phase, the first to read it
+        if (PH == VTI || y == ya - 4) {
+            if (!c.tma) fz_load_u(c, tid, y + 4, c.sl[6]);
+            else if (tid == 0 && !c.dead) fz_tma_issue(c, y + 4, c.sl[6]);
+        } else if (!c.tma) {
+            cpa_wait();
+        }
         if (y >= ya) fz_load_mat<PH>(c, tid, y);
         __syncthreads();
         if (PH == ELASTIC) {
             // plane y+5 (< ny - 3 for every chunk of [8, ny-8)) into the slot of
             // plane y-3, which no phase of this iteration reads
-            fz_load_u<true>(c, tid, y + 5, ring<PH>(y + 5));
-            cpa_commit();
+            if (!c.tma) {
+                fz_load_u<true>(c, tid, y + 5, ring<PH>(y + 5));
+                cpa_commit();
+            } else if (tid == 0 && !c.dead) {
+                fz_tma_issue(c, y + 5, ring<PH>(y + 5));
+            }
         }
+        if (c.tma) fz_tma_wait(c, c.sl[6]);
         fz_column<PH, XF, ZF>(c, th, tid, y + 2);
         if (y >= ya) fz_derived<PH, XF, ZF>(c, tid, y);
         __syncthreads();
@@ -156,18 +236,23 @@ __device__ __forceinline__ void fused_march(FusedCtx &c, int tid, int ya, int yb
         }
         __syncthreads();
     }
-    cpa_wait();
+    if (!c.tma) cpa_wait();
+    else if (PH == ELASTIC) fz_tma_wait(c, ring<PH>(yb + 4));  // the copy issued in the last iteration
 }
 
 // Fused elastic step over planes [ylo, yhi) (see fused.cuh).  grid: (z tiles,
 // x tiles, y chunks x shots), block (TZ, TX).
 template <int PH, int MINB>
-__global__ void __launch_bounds__(fz::NT, MINB) k_elastic_fused(const __grid_constant__ StepArgs a, int nchunks)
+__global__ void __launch_bounds__(fz::NT, MINB)
+    k_elastic_fused(const __grid_constant__ StepArgs a, int nchunks, const __grid_constant__ FusedTma t)
 {
-    extern __shared__ __align__(16) unsigned char fz_smem[];
+    extern __shared__ __align__(128) unsigned char fz_smem[];
     FusedCtx c;
     c.a = &a;
     c.sm = reinterpret_cast<FusedSmem *>(fz_smem);
+    c.tmap = &t.u;
+    c.err = t.err;
+    c.tma = t.on && (fz_saddr(fz_smem) & 127u) == 0;  // bulk-tensor destinations: 128-byte aligned slots
     const int tid = threadIdx.x + fz::TZ * threadIdx.y;
     c.shot = blockIdx.z / nchunks;
     const int ch = blockIdx.z - c.shot * nchunks;
@@ -434,6 +519,40 @@ __global__ void k_d2f(const double *in, float *out, int64_t n)
 // ---------------------------------------------------------------------------
 // Engine
 // ---------------------------------------------------------------------------
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+// (no link against the driver library); null when unavailable.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+        }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// Tensor map of the three displacement components of every shot at one time
+// level (base = component 0 of shot 0), as FusedTma describes.  Needs the
+// 16-byte strides of nz % 4 == 0 and a 16-byte aligned base.
+static bool encode_level_map(CUtensorMap *m, const float *base, const Problem &pb)
+{
+    const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc || pb.nz % 4 != 0 || ((uintptr_t)base & 15) != 0) return false;
+    const cuuint64_t n = (cuuint64_t)pb.nxyz();
+    const cuuint64_t dims[5] = {(cuuint64_t)pb.nz, (cuuint64_t)pb.nx, (cuuint64_t)pb.ny, 3, (cuuint64_t)pb.nshots};
+    const cuuint64_t strides[4] = {(cuuint64_t)pb.nz * 4, (cuuint64_t)pb.nx * pb.nz * 4, n * 4, 3 * n * 4};
+    const cuuint32_t box[5] = {fz::ZW, fz::XW, 1, 3, 1};
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, const_cast<float *>(base), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
 {
     int ndev = 0;
@@ -487,7 +606,13 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     // (default, the faster on B200) or 1 CTA per SM with up to 128 registers.
     const char *mb = std::getenv("FWI_FUSED_MINB");
     fused_minb_ = (mb && mb[0] == '1') ? 1 : 2;
+    // plane copies of the fused kernel by the tensor memory accelerator
+    // (FWI_TMA=0: per-thread asynchronous copies instead)
+    const char *te = std::getenv("FWI_TMA");
+    tma_ = fused_ && pb.nmodels != 2 && pb.nz % 4 == 0 && !(te && te[0] == '0') && tensor_map_encoder() != nullptr;
     if (fused_) {
+        tma_err_.alloc(sizeof(int));
+        tma_err_.zero(stream_);
         CK(cudaFuncSetAttribute(k_elastic_fused<ELASTIC, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(FusedSmem)));
         CK(cudaFuncSetAttribute(k_elastic_fused<VTI, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -508,7 +633,18 @@ Engine::~Engine()
     for (void *e : kev_) cudaEventDestroy((cudaEvent_t)e);
 }
 
-void Engine::sync() { CK(cudaStreamSynchronize((cudaStream_t)stream_)); }
+void Engine::sync()
+{
+    CK(cudaStreamSynchronize((cudaStream_t)stream_));
+    if (tma_) {
+        int e = 0;
+        CK(cudaMemcpy(&e, tma_err_.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (e) {
+            CK(cudaMemset(tma_err_.p, 0, sizeof(int)));
+            throw FwiError(FWI_ERR_CUDA, "fused kernel: a plane copy did not complete within its wait limit");
+        }
+    }
+}
 
 int64_t Engine::device_bytes() const
 {
@@ -769,13 +905,17 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         int nch = (target + tiles - 1) / tiles;
         nch = std::max(1, std::min(nch, (f.y1 - f.y0) / 16));
         const dim3 grd(kz, kx, nch * pb_.nshots), fblk(fz::TZ, fz::TX);
+        FusedTma tm;
+        std::memset(&tm, 0, sizeof(tm));
+        tm.err = tma_err_.as<int>();
+        tm.on = tma_ && encode_level_map(&tm.u, curr, pb_) ? 1 : 0;
         kmark(true, "k_elastic_fused", (int64_t)(f.y1 - f.y0) * pb_.nx * pb_.nz * pb_.nshots);
         if (fused_minb_ == 2) {
-            if (pb_.nmodels == 3) k_elastic_fused<ELASTIC, 2><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch);
-            else k_elastic_fused<VTI, 2><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch);
+            if (pb_.nmodels == 3) k_elastic_fused<ELASTIC, 2><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch, tm);
+            else k_elastic_fused<VTI, 2><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch, tm);
         } else {
-            if (pb_.nmodels == 3) k_elastic_fused<ELASTIC, 1><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch);
-            else k_elastic_fused<VTI, 1><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch);
+            if (pb_.nmodels == 3) k_elastic_fused<ELASTIC, 1><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch, tm);
+            else k_elastic_fused<VTI, 1><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch, tm);
         }
         kmark(false, nullptr, 0);
         // SAT of the x/z faces of the fused planes (and, with the marching

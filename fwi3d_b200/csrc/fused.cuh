@@ -46,7 +46,11 @@ struct FusedSmem {
     float u[8][3][fz::XW][fz::ZW];
     float dv[NDVC][fz::XH][fz::ZH];
     float mp[NMPC][fz::XH][fz::ZH];
+    unsigned long long bar[8];  // completion barriers of the ring slots' bulk-tensor copies
 };
+// bytes of one displacement plane window (three components) in a ring slot
+constexpr unsigned FZ_PLANE_BYTES = 3u * fz::XW * fz::ZW * sizeof(float);
+static_assert(FZ_PLANE_BYTES % 128 == 0, "ring slots must stay 128-byte aligned for bulk-tensor copies");
 static_assert(4 * fz::XH * fz::ZH <= 3 * fz::XW * fz::ZW, "VTI overlay must fit one ring slot");
 using ZRow = float[fz::ZH];
 FWI_HD ZRow *fz_dvp(const FusedSmem *s, int d)
@@ -107,6 +111,12 @@ struct FusedCtx {
     int xend, zend;    // end of this tile's output rows
     int sl[7];         // ring slots of planes y-2 .. y+4 for the current march step
     FusedSmem *sm;
+    // bulk-tensor plane copies (GPU only): tensor map of the current level,
+    // error flag, per-slot barrier phases of this thread, copies on / given up
+    const void *tmap = nullptr;
+    int *err = nullptr;
+    unsigned ph = 0;
+    bool tma = false, dead = false;
 };
 
 

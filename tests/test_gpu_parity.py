@@ -162,6 +162,26 @@ def test_fused_matches_per_point(monkeypatch):
         assert rel(out[name + "m"], out[name + "p"]) < 2e-6
 
 
+def test_fused_plane_copies(monkeypatch):
+    """The fused kernel's bulk-tensor plane copies (nz % 4 == 0) give the same
+    bits as its per-thread copies (FWI_TMA=0); a grid with nz % 4 != 0 takes
+    the per-thread copies and matches the per-point kernels."""
+    for name, sv in (("e", _elastic_fused()), ("v", _vti_fused())):
+        monkeypatch.setenv("FWI_TMA", "1")
+        t = ops.from_survey(sv).forward(False, sv.model)
+        monkeypatch.setenv("FWI_TMA", "0")
+        a = ops.from_survey(sv).forward(False, sv.model)
+        assert np.array_equal(t, a), name
+    monkeypatch.delenv("FWI_TMA")
+    sv = _elastic_fused()
+    sv.model = np.ascontiguousarray(sv.model[:, :, :, :46])
+    sv.nz = 46
+    f = ops.from_survey(sv).forward(False, sv.model)
+    monkeypatch.setenv("FWI_FUSED", "0")
+    p = ops.from_survey(sv).forward(False, sv.model)
+    assert rel(f, p) < 2e-6
+
+
 def test_march_chunks_and_batch(monkeypatch):
     """Marching kernel with several y chunks per tile column and a batch of
     shots against the per-point kernels."""
