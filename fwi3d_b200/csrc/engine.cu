@@ -201,6 +201,7 @@ __device__ __forceinline__ void fused_march(FusedCtx &c, int tid, int ya, int yb
 #pragma unroll
     for (int k = 0; k < 5; k++) th.qmu[k] = th.qeps[k] = th.q66[k] = th.qT[k] = th.qX1[k] = th.qZ1[k] = 0.f;
     if (c.tma && tid == 0) fz_bar_init(c);
+    fill_smem_rows(c.sm->rows, tid, fz::NT);
     fz_prologue<PH>(c, tid, ya);
     __syncthreads();
     for (int y = ya - 4; y < yb; y++) {
@@ -253,6 +254,7 @@ __global__ void __launch_bounds__(fz::NT, MINB)
     c.tmap = &t.u;
     c.err = t.err;
     c.tma = t.on && (fz_saddr(fz_smem) & 127u) == 0;  // bulk-tensor destinations: 128-byte aligned slots
+    c.rows.p = c.sm->rows;
     const int tid = threadIdx.x + fz::TZ * threadIdx.y;
     c.shot = blockIdx.z / nchunks;
     const int ch = blockIdx.z - c.shot * nchunks;
@@ -318,6 +320,7 @@ __global__ void __launch_bounds__(f3::NT, 1) k_elastic_march(const __grid_consta
     MarchCtx c;
     c.a = &a;
     c.sm = reinterpret_cast<MarchSmem *>(m3_smem);
+    c.rows.p = c.sm->rows;  // filled below; first read after the first phase's barrier
     const int tid = threadIdx.x + f3::TZ * threadIdx.y;
     const int shot = blockIdx.z / nchunks;
     const int ch = blockIdx.z - shot * nchunks;
@@ -333,6 +336,7 @@ __global__ void __launch_bounds__(f3::NT, 1) k_elastic_march(const __grid_consta
         m3_chunk(a.g.ny, ch, nchunks, ya, yb);
     }
     if (ya >= yb) return;
+    fill_smem_rows(c.sm->rows, tid, f3::NT);
     const bool xf = m3_fast(c.x0, a.g.nx, f3::TX), zf = m3_fast(c.z0, a.g.nz, f3::TZ);
     if (xf && zf) march_tile<PH, true, true>(c, ya, yb, tid);
     else if (xf) march_tile<PH, true, false>(c, ya, yb, tid);

@@ -47,6 +47,7 @@ struct FusedSmem {
     float dv[NDVC][fz::XH][fz::ZH];
     float mp[NMPC][fz::XH][fz::ZH];
     unsigned long long bar[8];  // completion barriers of the ring slots' bulk-tensor copies
+    float rows[SR_FLOATS];      // SBP closure rows, padded (SmemRows)
 };
 // bytes of one displacement plane window (three components) in a ring slot
 constexpr unsigned FZ_PLANE_BYTES = 3u * fz::XW * fz::ZW * sizeof(float);
@@ -113,6 +114,7 @@ struct FusedCtx {
     FusedSmem *sm;
     // bulk-tensor plane copies (GPU only): tensor map of the current level,
     // error flag, per-slot barrier phases of this thread, copies on / given up
+    SmemRows rows{nullptr};  // closure rows in shared memory (FusedSmem::rows)
     const void *tmap = nullptr;
     int *err = nullptr;
     unsigned ph = 0;
@@ -224,18 +226,6 @@ FWI_HD void fz_load_mat(FusedCtx &c, int tid, int y)
     }
 }
 
-// D1 row (unscaled) at global index i of a smem line.  Closure rows read
-// samples 0..5 or n-6..n-1, which lie in the window for every position whose
-// value an output row uses; halo positions outside that set are clamped to
-// the window and their (unused) values are meaningless.
-template <class S>
-FWI_HD float d1_sg(const S &s, int i, int n)
-{
-    const SbpTables &t = sbp();
-    if (i < 4 || i >= n - 4) return d1_row(s, i, n);
-    return t.d1c0 * (s(i + 1) - s(i - 1)) + t.d1c1 * (s(i + 2) - s(i - 2));
-}
-
 // First derivatives of displacement component k at (ix, q, iz) along x, y, z
 // from the ring (with the 1/h).  ixw/izw: smem coordinates in the ring window.
 template <bool F = false>
@@ -249,7 +239,7 @@ FWI_HD float fz_dx(const FusedCtx &c, int k, int slot, int ix, int izw)
                c.a->idx;
     }
     const SXc s{p, c.x0 - fz::HW, fz::ZW, fz::XW};
-    return d1_row(s, ix, c.a->g.nx) * c.a->idx;
+    return d1_row(s, ix, c.a->g.nx, c.rows) * c.a->idx;
 }
 template <bool F = false>
 FWI_HD float fz_dz(const FusedCtx &c, int k, int slot, int ixw, int iz)
@@ -261,7 +251,7 @@ FWI_HD float fz_dz(const FusedCtx &c, int k, int slot, int ixw, int iz)
         return (t.d1c0 * (p[j + 1] - p[j - 1]) + t.d1c1 * (p[j + 2] - p[j - 2])) * c.a->idz;
     }
     const SZc s{p, c.z0 - fz::HW, fz::ZW};
-    return d1_row(s, iz, c.a->g.nz) * c.a->idz;
+    return d1_row(s, iz, c.a->g.nz, c.rows) * c.a->idz;
 }
 // Dy at a plane from the ring slots of its four neighbours: interior rows only
 // (the fused launch keeps every differentiated plane in [6, ny-6)).
@@ -404,10 +394,9 @@ FWI_HD float d1m(float am2, float mm2, float am1, float mm1, float ap1, float mp
 struct W8 {
     float w[8];
 };
-template <class F>
-FWI_HD W8 d2closure_weights(const F &f, int i, int n)
+template <class F, class R>
+FWI_HD W8 d2closure_weights(const F &f, int i, int n, const R &b)
 {
-    const SbpTables &t = sbp();
     const bool hi = i >= n - 6;
     const int r = hi ? n - 1 - i : i;
     float fk[8];
@@ -415,7 +404,7 @@ FWI_HD W8 d2closure_weights(const F &f, int i, int n)
     W8 w;
     for (int j = 0; j < 8; j++) {
         float v = 0.f;
-        for (int k = 0; k < 8; k++) v += t.d2b[r][j][k] * fk[k];
+        for (int k = 0; k < 8; k++) v += b.d2(r, j, k) * fk[k];
         w.w[j] = v;
     }
     return w;
@@ -469,9 +458,9 @@ FWI_HD void fz_output(FusedCtx &c, const FusedThread &th, int tid, int y)
         W5 wx{}, wz{};
         W8 wxc{}, wzc{};
         if (xin) wx = d2w(mux(ix - 2), mux(ix - 1), mux(ix), mux(ix + 1), mux(ix + 2));
-        else wxc = d2closure_weights(mux, ix, g.nx);
+        else wxc = d2closure_weights(mux, ix, g.nx, c.rows);
         if (zin) wz = d2w(muz(iz - 2), muz(iz - 1), muz(iz), muz(iz + 1), muz(iz + 2));
-        else wzc = d2closure_weights(muz, iz, g.nz);
+        else wzc = d2closure_weights(muz, iz, g.nz, c.rows);
         const W5 wy = d2w(th.qmu[0], th.qmu[1], th.qmu[2], th.qmu[3], th.qmu[4]);
         for (int k = 0; k < 3; k++) {
             const float adx = k == 0 ? a.ad2[0] : a.ad1[0];
@@ -511,13 +500,13 @@ FWI_HD void fz_output(FusedCtx &c, const FusedThread &th, int tid, int y)
             const SZ uzl = uz_line(c, r0, k, ixw);
             float v;
             if (xin) v = d2apply(wx, idx2, ul(ix - 2), ul(ix - 1), ul(ix), ul(ix + 1), ul(ix + 2));
-            else if (k == 0) v = d2var_row(ul, bx, ix, g.nx, idx2);
-            else if (k == 1) v = d2var_row(ul, c6x, ix, g.nx, idx2);
-            else v = d2var_row(ul, mux, ix, g.nx, idx2);
+            else if (k == 0) v = d2var_row(ul, bx, ix, g.nx, idx2, c.rows);
+            else if (k == 1) v = d2var_row(ul, c6x, ix, g.nx, idx2, c.rows);
+            else v = d2var_row(ul, mux, ix, g.nx, idx2, c.rows);
             v += d2apply(wy, idy2, s.u[rm2][k][ixw][izw], s.u[rm1][k][ixw][izw], s.u[r0][k][ixw][izw],
                          s.u[rp1][k][ixw][izw], s.u[rp2][k][ixw][izw]);
             v += zin ? d2apply(wz, adz, uzl(iz - 2), uzl(iz - 1), uzl(iz), uzl(iz + 1), uzl(iz + 2))
-                     : d2var_row(uzl, muz, iz, g.nz, adz);
+                     : d2var_row(uzl, muz, iz, g.nz, adz, c.rows);
             acc[k] = v;
         }
     }
@@ -526,16 +515,16 @@ FWI_HD void fz_output(FusedCtx &c, const FusedThread &th, int tid, int y)
     const SX Px = (PH == VTI) ? mx_line(c, MP_C66, zh) : mux;
     const float *qP = (PH == VTI) ? th.q66 : th.qmu;
     // comp 0: Dx(T0)/dx + Dy(P u_x1)/dy + Dz(mu u_x2)/dy (dy as in the reference, we_op.cpp:678)
-    acc[0] += d1_row(dx_line(c, DV_T0, zh), ix, g.nx) * a.idx;
+    acc[0] += d1_row(dx_line(c, DV_T0, zh), ix, g.nx, c.rows) * a.idx;
     acc[0] += d1m(th.qX1[0], qP[0], th.qX1[1], qP[1], th.qX1[3], qP[3], th.qX1[4], qP[4]) * a.idy;
-    acc[0] += d1_prod_row(dz_line(c, DV_X2, xh), muz, iz, g.nz) * a.idy;
+    acc[0] += d1_prod_row(dz_line(c, DV_X2, xh), muz, iz, g.nz, c.rows) * a.idy;
     // comp 1: Dy(T1)/dy + Dx(P u_y0)/dx + Dz(mu u_y2)/dz
     acc[1] += d1i(th.qT[0], th.qT[1], th.qT[3], th.qT[4]) * a.idy;
-    acc[1] += d1_prod_row(dx_line(c, DV_Y0, zh), Px, ix, g.nx) * a.idx;
-    acc[1] += d1_prod_row(dz_line(c, DV_Y2, xh), muz, iz, g.nz) * a.idz;
+    acc[1] += d1_prod_row(dx_line(c, DV_Y0, zh), Px, ix, g.nx, c.rows) * a.idx;
+    acc[1] += d1_prod_row(dz_line(c, DV_Y2, xh), muz, iz, g.nz, c.rows) * a.idz;
     // comp 2: Dz(T2)/dz + Dx(mu u_z0)/dx + Dy(mu u_z1)/dy
-    acc[2] += d1_row(dz_line(c, PH == ELASTIC ? DV_T0 : DV_T2, xh), iz, g.nz) * a.idz;
-    acc[2] += d1_prod_row(dx_line(c, DV_Z0, zh), mux, ix, g.nx) * a.idx;
+    acc[2] += d1_row(dz_line(c, PH == ELASTIC ? DV_T0 : DV_T2, xh), iz, g.nz, c.rows) * a.idz;
+    acc[2] += d1_prod_row(dx_line(c, DV_Z0, zh), mux, ix, g.nx, c.rows) * a.idx;
     acc[2] += d1m(th.qZ1[0], th.qmu[0], th.qZ1[1], th.qmu[1], th.qZ1[3], th.qmu[3], th.qZ1[4], th.qmu[4]) * a.idy;
 
     // ---- update, scaling, taper (SAT is added by the face kernel) ----
@@ -586,9 +575,9 @@ FWI_HD void fz_output_t(FusedCtx &c, const FusedThread &th, int tid, int y)
         W5 wx{}, wz{};
         W8 wxc{}, wzc{};
         if (xin) wx = d2w(mu[-2 * DX], mu[-DX], mu[0], mu[DX], mu[2 * DX]);
-        else wxc = d2closure_weights(mux, ix, g.nx);
+        else wxc = d2closure_weights(mux, ix, g.nx, c.rows);
         if (zin) wz = d2w(mu[-2], mu[-1], mu[0], mu[1], mu[2]);
-        else wzc = d2closure_weights(muz, iz, g.nz);
+        else wzc = d2closure_weights(muz, iz, g.nz, c.rows);
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             const float adx = k == 0 ? a.ad2[0] : a.ad1[0];
@@ -632,12 +621,12 @@ FWI_HD void fz_output_t(FusedCtx &c, const FusedThread &th, int tid, int y)
                 v = d2apply(wx, idx2, u[-2 * UX], u[-UX], u[0], u[UX], u[2 * UX]);
             } else {
                 const SX ul = ux_line(c, c.sl[2], k, izw);
-                v = k == 0 ? d2var_row(ul, bx, ix, g.nx, idx2)
-                           : (k == 1 ? d2var_row(ul, c6x, ix, g.nx, idx2) : d2var_row(ul, mux, ix, g.nx, idx2));
+                v = k == 0 ? d2var_row(ul, bx, ix, g.nx, idx2, c.rows)
+                           : (k == 1 ? d2var_row(ul, c6x, ix, g.nx, idx2, c.rows) : d2var_row(ul, mux, ix, g.nx, idx2, c.rows));
             }
             v += d2apply(wy, idy2, uc[rm2], uc[rm1], u[0], uc[rp1], uc[rp2]);
             v += zin ? d2apply(wz, adz, u[-2], u[-1], u[0], u[1], u[2])
-                     : d2var_row(uz_line(c, c.sl[2], k, ixw), muz, iz, g.nz, adz);
+                     : d2var_row(uz_line(c, c.sl[2], k, ixw), muz, iz, g.nz, adz, c.rows);
             acc[k] = v;
         }
     }
@@ -651,20 +640,20 @@ FWI_HD void fz_output_t(FusedCtx &c, const FusedThread &th, int tid, int y)
     const float *y2 = &fz_dvp(&s, DV_Y2)[xh][zh], *z0 = &fz_dvp(&s, DV_Z0)[xh][zh];
     // each term is added where it is formed, so that few values are live at once
     // comp 0: Dx(T0)/dx + Dy(P u_x1)/dy + Dz(mu u_x2)/dy (dy as in the reference, we_op.cpp:678)
-    acc[0] += (xin ? d1i(t0[-2 * DX], t0[-DX], t0[DX], t0[2 * DX]) : d1_row(dx_line(c, DV_T0, zh), ix, g.nx)) * a.idx;
+    acc[0] += (xin ? d1i(t0[-2 * DX], t0[-DX], t0[DX], t0[2 * DX]) : d1_row(dx_line(c, DV_T0, zh), ix, g.nx, c.rows)) * a.idx;
     acc[0] += d1m(th.qX1[0], qP[0], th.qX1[1], qP[1], th.qX1[3], qP[3], th.qX1[4], qP[4]) * a.idy;
     acc[0] += (zin ? d1m(x2[-2], mu[-2], x2[-1], mu[-1], x2[1], mu[1], x2[2], mu[2])
-                   : d1_prod_row(dz_line(c, DV_X2, xh), muz, iz, g.nz)) * a.idy;
+                   : d1_prod_row(dz_line(c, DV_X2, xh), muz, iz, g.nz, c.rows)) * a.idy;
     // comp 1: Dy(T1)/dy + Dx(P u_y0)/dx + Dz(mu u_y2)/dz
     acc[1] += d1i(th.qT[0], th.qT[1], th.qT[3], th.qT[4]) * a.idy;
     acc[1] += (xin ? d1m(y0[-2 * DX], P[-2 * DX], y0[-DX], P[-DX], y0[DX], P[DX], y0[2 * DX], P[2 * DX])
-                   : d1_prod_row(dx_line(c, DV_Y0, zh), Px, ix, g.nx)) * a.idx;
+                   : d1_prod_row(dx_line(c, DV_Y0, zh), Px, ix, g.nx, c.rows)) * a.idx;
     acc[1] += (zin ? d1m(y2[-2], mu[-2], y2[-1], mu[-1], y2[1], mu[1], y2[2], mu[2])
-                   : d1_prod_row(dz_line(c, DV_Y2, xh), muz, iz, g.nz)) * a.idz;
+                   : d1_prod_row(dz_line(c, DV_Y2, xh), muz, iz, g.nz, c.rows)) * a.idz;
     // comp 2: Dz(T2)/dz + Dx(mu u_z0)/dx + Dy(mu u_z1)/dy
-    acc[2] += (zin ? d1i(t2[-2], t2[-1], t2[1], t2[2]) : d1_row(dz_line(c, DT2, xh), iz, g.nz)) * a.idz;
+    acc[2] += (zin ? d1i(t2[-2], t2[-1], t2[1], t2[2]) : d1_row(dz_line(c, DT2, xh), iz, g.nz, c.rows)) * a.idz;
     acc[2] += (xin ? d1m(z0[-2 * DX], mu[-2 * DX], z0[-DX], mu[-DX], z0[DX], mu[DX], z0[2 * DX], mu[2 * DX])
-                   : d1_prod_row(dx_line(c, DV_Z0, zh), mux, ix, g.nx)) * a.idx;
+                   : d1_prod_row(dx_line(c, DV_Z0, zh), mux, ix, g.nx, c.rows)) * a.idx;
     acc[2] += d1m(th.qZ1[0], th.qmu[0], th.qZ1[1], th.qmu[1], th.qZ1[3], th.qmu[3], th.qZ1[4], th.qmu[4]) * a.idy;
 
     // update, scaling (x/z faces), taper; SAT is added by the face kernel

@@ -52,6 +52,7 @@ struct MarchSmem {
     float yd[f3::NY][NYD][f3::TX][f3::TZ];
     float dv[ND3][f3::XD][f3::ZD];
     float mp[2][NMP][f3::XD][f3::ZD];  // double-buffered: the next plane's arrive while this one is used
+    float rows[SR_FLOATS];              // SBP closure rows, padded (SmemRows)
 };
 
 struct MarchCtx {
@@ -61,6 +62,7 @@ struct MarchCtx {
     int xend, zend;  // end of this tile's output rows
     int mb;          // materials buffer of the plane being output
     MarchSmem *sm;
+    SmemRows rows{nullptr};  // closure rows in shared memory (MarchSmem::rows)
 };
 
 // Ring accessors along y (own column), indexed by global plane.
@@ -123,7 +125,7 @@ FWI_HD float m3_dx(const MarchCtx &c, int k, int slot, int xu, int zu)
         return (t.d1c0 * (p[(xu + 1) * f3::ZU] - p[(xu - 1) * f3::ZU]) +
                 t.d1c1 * (p[(xu + 2) * f3::ZU] - p[(xu - 2) * f3::ZU])) * c.a->idx;
     }
-    return d1_row(SXc{p, c.x0 - f3::HU, f3::ZU, f3::XU}, ix, c.a->g.nx) * c.a->idx;
+    return d1_row(SXc{p, c.x0 - f3::HU, f3::ZU, f3::XU}, ix, c.a->g.nx, c.rows) * c.a->idx;
 }
 template <bool ZF>
 FWI_HD float m3_dz(const MarchCtx &c, int k, int slot, int xu, int zu)
@@ -134,7 +136,7 @@ FWI_HD float m3_dz(const MarchCtx &c, int k, int slot, int xu, int zu)
         const SbpTables &t = sbp();
         return (t.d1c0 * (p[zu + 1] - p[zu - 1]) + t.d1c1 * (p[zu + 2] - p[zu - 2])) * c.a->idz;
     }
-    return d1_row(SZc{p, c.z0 - f3::HU, f3::ZU}, iz, c.a->g.nz) * c.a->idz;
+    return d1_row(SZc{p, c.z0 - f3::HU, f3::ZU}, iz, c.a->g.nz, c.rows) * c.a->idz;
 }
 // Dy at plane q: interior taps from the ring, closure rows through the ring
 // accessor (their samples 0..5 or ny-6..ny-1 are resident when used).
@@ -148,7 +150,7 @@ FWI_HD float m3_dy(const MarchCtx &c, int k, int q, int xu, int zu)
         return (t.d1c0 * (p[((q + 1) & R) * f3::USTR] - p[((q - 1) & R) * f3::USTR]) +
                 t.d1c1 * (p[((q + 2) & R) * f3::USTR] - p[((q - 2) & R) * f3::USTR])) * c.a->idy;
     }
-    return d1_row(URing{p}, q, g.ny) * c.a->idy;
+    return d1_row(URing{p}, q, g.ny, c.rows) * c.a->idy;
 }
 
 // ---------------------------------------------------------------------------
@@ -232,16 +234,16 @@ FWI_HD void m3_derived(const MarchCtx &c, int tid, int y)
 // ---------------------------------------------------------------------------
 // In-plane unscaled D1 of a derived line, and of a derived*coefficient line.
 template <bool F, class L>
-FWI_HD float m3_d1(const L &s, int i, int n)
+FWI_HD float m3_d1(const L &s, int i, int n, const SmemRows &rows)
 {
     if (F) return d1i(s(i - 2), s(i - 1), s(i + 1), s(i + 2));
-    return d1_row(s, i, n);
+    return d1_row(s, i, n, rows);
 }
 template <bool F, class L, class M>
-FWI_HD float m3_d1p(const L &s, const M &m, int i, int n)
+FWI_HD float m3_d1p(const L &s, const M &m, int i, int n, const SmemRows &rows)
 {
     if (F) return d1m(s(i - 2), m(i - 2), s(i - 1), m(i - 1), s(i + 1), m(i + 1), s(i + 2), m(i + 2));
-    return d1_prod_row(s, m, i, n);
+    return d1_prod_row(s, m, i, n, rows);
 }
 
 template <int PH, bool XF, bool ZF>
@@ -280,11 +282,11 @@ FWI_HD void m3_output(const MarchCtx &c, int tid, int y)
         W5 wx{}, wz{}, wy{};
         W8 wxc{}, wzc{}, wyc{};
         if (xin) wx = d2w(mux(ix - 2), mux(ix - 1), mux(ix), mux(ix + 1), mux(ix + 2));
-        else wxc = d2closure_weights(mux, ix, g.nx);
+        else wxc = d2closure_weights(mux, ix, g.nx, c.rows);
         if (zin) wz = d2w(muz(iz - 2), muz(iz - 1), muz(iz), muz(iz + 1), muz(iz + 2));
-        else wzc = d2closure_weights(muz, iz, g.nz);
+        else wzc = d2closure_weights(muz, iz, g.nz, c.rows);
         if (yin) wy = d2w(ydv(YD_MU, 0), ydv(YD_MU, 1), ydv(YD_MU, 2), ydv(YD_MU, 3), ydv(YD_MU, 4));
-        else wyc = d2closure_weights(Line{a.m[1], col, ystr}, y, g.ny);
+        else wyc = d2closure_weights(Line{a.m[1], col, ystr}, y, g.ny, c.rows);
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             const float adx = k == 0 ? a.ad2[0] : a.ad1[0];
@@ -328,19 +330,19 @@ FWI_HD void m3_output(const MarchCtx &c, int tid, int y)
             const SZ uzl{&s.u[s0][k][xu][0], c.z0 - f3::HU};
             float v;
             if (xin) v = d2apply(wx, idx2, ul(ix - 2), ul(ix - 1), ul(ix), ul(ix + 1), ul(ix + 2));
-            else if (k == 0) v = d2var_row(ul, bx, ix, g.nx, idx2);
-            else if (k == 1) v = d2var_row(ul, c6x, ix, g.nx, idx2);
-            else v = d2var_row(ul, mux, ix, g.nx, idx2);
+            else if (k == 0) v = d2var_row(ul, bx, ix, g.nx, idx2, c.rows);
+            else if (k == 1) v = d2var_row(ul, c6x, ix, g.nx, idx2, c.rows);
+            else v = d2var_row(ul, mux, ix, g.nx, idx2, c.rows);
             if (yin) {
                 v += d2apply(wy, idy2, uy(k, y - 2), uy(k, y - 1), uy(k, y), uy(k, y + 1), uy(k, y + 2));
             } else {
                 const Line ucol{a.curr[k] + c.so, col, ystr};
-                if (k == 0) v += d2var_row(ucol, c6y, y, g.ny, idy2);
-                else if (k == 1) v += d2var_row(ucol, C11bLine{epsy, muy}, y, g.ny, idy2);
-                else v += d2var_row(ucol, muy, y, g.ny, idy2);
+                if (k == 0) v += d2var_row(ucol, c6y, y, g.ny, idy2, c.rows);
+                else if (k == 1) v += d2var_row(ucol, C11bLine{epsy, muy}, y, g.ny, idy2, c.rows);
+                else v += d2var_row(ucol, muy, y, g.ny, idy2, c.rows);
             }
             v += zin ? d2apply(wz, adz, uzl(iz - 2), uzl(iz - 1), uzl(iz), uzl(iz + 1), uzl(iz + 2))
-                     : d2var_row(uzl, muz, iz, g.nz, adz);
+                     : d2var_row(uzl, muz, iz, g.nz, adz, c.rows);
             acc[k] = v;
         }
     }
@@ -362,21 +364,21 @@ FWI_HD void m3_output(const MarchCtx &c, int tid, int y)
         dyZ1 = d1m(ydv(YD_Z1, 0), ydv(YD_MU, 0), ydv(YD_Z1, 1), ydv(YD_MU, 1), ydv(YD_Z1, 3), ydv(YD_MU, 3),
                    ydv(YD_Z1, 4), ydv(YD_MU, 4));
     } else {
-        dyX1 = d1_prod_row(YRing{ydb + YD_X1 * f3::YF}, YRing{ydb + PY * f3::YF}, y, g.ny);
-        dyT = d1_row(YRing{ydb + YD_T * f3::YF}, y, g.ny);
-        dyZ1 = d1_prod_row(YRing{ydb + YD_Z1 * f3::YF}, YRing{ydb + YD_MU * f3::YF}, y, g.ny);
+        dyX1 = d1_prod_row(YRing{ydb + YD_X1 * f3::YF}, YRing{ydb + PY * f3::YF}, y, g.ny, c.rows);
+        dyT = d1_row(YRing{ydb + YD_T * f3::YF}, y, g.ny, c.rows);
+        dyZ1 = d1_prod_row(YRing{ydb + YD_Z1 * f3::YF}, YRing{ydb + YD_MU * f3::YF}, y, g.ny, c.rows);
     }
     // comp 0: Dx(T0)/dx + Dy(P u_x1)/dy + Dz(mu u_x2)/dy (dy as in the reference, we_op.cpp:678)
-    acc[0] += m3_d1<XF>(dT0x, ix, g.nx) * a.idx;
+    acc[0] += m3_d1<XF>(dT0x, ix, g.nx, c.rows) * a.idx;
     acc[0] += dyX1 * a.idy;
-    acc[0] += m3_d1p<ZF>(dX2z, muz, iz, g.nz) * a.idy;
+    acc[0] += m3_d1p<ZF>(dX2z, muz, iz, g.nz, c.rows) * a.idy;
     // comp 1: Dy(T1)/dy + Dx(P u_y0)/dx + Dz(mu u_y2)/dz
     acc[1] += dyT * a.idy;
-    acc[1] += m3_d1p<XF>(dY0x, Px, ix, g.nx) * a.idx;
-    acc[1] += m3_d1p<ZF>(dY2z, muz, iz, g.nz) * a.idz;
+    acc[1] += m3_d1p<XF>(dY0x, Px, ix, g.nx, c.rows) * a.idx;
+    acc[1] += m3_d1p<ZF>(dY2z, muz, iz, g.nz, c.rows) * a.idz;
     // comp 2: Dz(T2)/dz + Dx(mu u_z0)/dx + Dy(mu u_z1)/dy
-    acc[2] += m3_d1<ZF>(dT2z, iz, g.nz) * a.idz;
-    acc[2] += m3_d1p<XF>(dZ0x, mux, ix, g.nx) * a.idx;
+    acc[2] += m3_d1<ZF>(dT2z, iz, g.nz, c.rows) * a.idz;
+    acc[2] += m3_d1p<XF>(dZ0x, mux, ix, g.nx, c.rows) * a.idx;
     acc[2] += dyZ1 * a.idy;
 
     // ---- update, scaling, taper (SAT is added by the face kernel) ----

@@ -59,46 +59,74 @@ struct Line {
     FWI_HD float operator()(int k) const { return p[base + (int64_t)k * stride]; }
 };
 
+// Closure-row coefficients, read where a kernel keeps them.  ConstRows: the
+// constant-memory tables (a warp whose lanes sit on different closure rows
+// reads them one row at a time).  SmemRows: a shared-memory copy whose rows
+// are padded so that such lanes read different banks in one access
+// (fill_smem_rows writes it).
+struct ConstRows {
+    FWI_HD float d1(int r, int k) const { return sbp().d1b[r][k]; }
+    FWI_HD float d2(int r, int j, int k) const { return sbp().d2b[r][j][k]; }
+};
+constexpr int SR_D2 = 65, SR_D1 = 7;              // padded row strides (floats)
+constexpr int SR_FLOATS = 6 * SR_D2 + 4 * SR_D1;  // 418
+struct SmemRows {
+    const float *p;
+    FWI_HD float d1(int r, int k) const { return p[6 * SR_D2 + r * SR_D1 + k]; }
+    FWI_HD float d2(int r, int j, int k) const { return p[r * SR_D2 + j * 8 + k]; }
+};
+// Thread `tid` of `nt` writes its share of the padded copy.
+FWI_HD void fill_smem_rows(float *p, int tid, int nt)
+{
+    const SbpTables &t = sbp();
+    for (int e = tid; e < 6 * 64 + 4 * 6; e += nt) {
+        if (e < 6 * 64) p[(e >> 6) * SR_D2 + (e & 63)] = (&t.d2b[0][0][0])[e];
+        else p[6 * SR_D2 + ((e - 384) / 6) * SR_D1 + (e - 384) % 6] = t.d1b[(e - 384) / 6][(e - 384) % 6];
+    }
+}
+
 // Unscaled D1 row at index i of an n-sample line (no 1/h).  Boundary rows use
 // the closure (left) or its mirror with a sign flip (right).
-template <class A>
-FWI_HD float d1_row(const A &a, int i, int n)
+template <class A, class R = ConstRows>
+FWI_HD float d1_row(const A &a, int i, int n, const R &b = R())
 {
     const SbpTables &t = sbp();
     if (i < 4) {
-        const float *b = t.d1b[i];
-        return b[0] * a(0) + b[1] * a(1) + b[2] * a(2) + b[3] * a(3) + b[4] * a(4) + b[5] * a(5);
+        const int r = i;
+        return b.d1(r, 0) * a(0) + b.d1(r, 1) * a(1) + b.d1(r, 2) * a(2) + b.d1(r, 3) * a(3) + b.d1(r, 4) * a(4) +
+               b.d1(r, 5) * a(5);
     }
     if (i >= n - 4) {
-        const float *b = t.d1b[n - 1 - i];
-        return -(b[0] * a(n - 1) + b[1] * a(n - 2) + b[2] * a(n - 3) + b[3] * a(n - 4) + b[4] * a(n - 5) +
-                 b[5] * a(n - 6));
+        const int r = n - 1 - i;
+        return -(b.d1(r, 0) * a(n - 1) + b.d1(r, 1) * a(n - 2) + b.d1(r, 2) * a(n - 3) + b.d1(r, 3) * a(n - 4) +
+                 b.d1(r, 4) * a(n - 5) + b.d1(r, 5) * a(n - 6));
     }
     return t.d1c0 * (a(i + 1) - a(i - 1)) + t.d1c1 * (a(i + 2) - a(i - 2));
 }
 
 // D1 row of the product a*m (the reference's mult_D: derivative of par*in).
-template <class A, class M>
-FWI_HD float d1_prod_row(const A &a, const M &m, int i, int n)
+template <class A, class M, class R = ConstRows>
+FWI_HD float d1_prod_row(const A &a, const M &m, int i, int n, const R &b = R())
 {
     const SbpTables &t = sbp();
     if (i < 4) {
-        const float *b = t.d1b[i];
-        return b[0] * a(0) * m(0) + b[1] * a(1) * m(1) + b[2] * a(2) * m(2) + b[3] * a(3) * m(3) +
-               b[4] * a(4) * m(4) + b[5] * a(5) * m(5);
+        const int r = i;
+        return b.d1(r, 0) * a(0) * m(0) + b.d1(r, 1) * a(1) * m(1) + b.d1(r, 2) * a(2) * m(2) +
+               b.d1(r, 3) * a(3) * m(3) + b.d1(r, 4) * a(4) * m(4) + b.d1(r, 5) * a(5) * m(5);
     }
     if (i >= n - 4) {
-        const float *b = t.d1b[n - 1 - i];
-        return -(b[0] * a(n - 1) * m(n - 1) + b[1] * a(n - 2) * m(n - 2) + b[2] * a(n - 3) * m(n - 3) +
-                 b[3] * a(n - 4) * m(n - 4) + b[4] * a(n - 5) * m(n - 5) + b[5] * a(n - 6) * m(n - 6));
+        const int r = n - 1 - i;
+        return -(b.d1(r, 0) * a(n - 1) * m(n - 1) + b.d1(r, 1) * a(n - 2) * m(n - 2) +
+                 b.d1(r, 2) * a(n - 3) * m(n - 3) + b.d1(r, 3) * a(n - 4) * m(n - 4) +
+                 b.d1(r, 4) * a(n - 5) * m(n - 5) + b.d1(r, 5) * a(n - 6) * m(n - 6));
     }
     return t.d1c0 * (a(i + 1) * m(i + 1) - a(i - 1) * m(i - 1)) + t.d1c1 * (a(i + 2) * m(i + 2) - a(i - 2) * m(i - 2));
 }
 
 // Variable-coefficient second derivative (d/dx f d/dx) at index i, times ad2 = a/h^2.
 // u: field line, f: material line (the coefficient function sampled on the same line).
-template <class U, class F>
-FWI_HD float d2var_row(const U &u, const F &f, int i, int n, float ad2)
+template <class U, class F, class R = ConstRows>
+FWI_HD float d2var_row(const U &u, const F &f, int i, int n, float ad2, const R &b = R())
 {
     const SbpTables &t = sbp();
     if (i < 6 || i >= n - 6) {
@@ -112,7 +140,7 @@ FWI_HD float d2var_row(const U &u, const F &f, int i, int n, float ad2)
         for (int j = 0; j < 8; j++) {
             float v = 0.f;
 #pragma unroll
-            for (int k = 0; k < 8; k++) v += t.d2b[r][j][k] * fk[k];
+            for (int k = 0; k < 8; k++) v += b.d2(r, j, k) * fk[k];
             acc += ad2 * v * u(hi ? n - 1 - j : j);
         }
         return acc;
