@@ -396,16 +396,14 @@ __global__ void k_elastic_face_sat(const __grid_constant__ StepArgs a, int64_t n
     int ix, iy, iz;
     if (!face_point(a.g, a.y0, a.y1, k, ix, iy, iz)) return;
     const int64_t so = (int64_t)blockIdx.y * a.sst;
+    const int c = blockIdx.z;  // one component per thread: three independent load chains per point
     const int64_t i = a.g.idx(ix, iy, iz);
-    const float f = a.dt * a.dt / a.m[2][i];
-    for (int c = 0; c < 3; c++) {
-        const float sat = elastic_sat<PH>(a, 0.f, c, ix, iy, iz, so);
-        if (sat == 0.f) continue;
-        float v = f * sat;
-        v = boundary_scale(a, v, c, ix, iy, iz);
-        v = taper(a, v, ix, iy, iz);
-        a.next[c][so + i] += v;
-    }
+    const float sat = elastic_sat<PH>(a, 0.f, c, ix, iy, iz, so);
+    if (sat == 0.f) return;
+    float v = a.dt * a.dt / a.m[2][i] * sat;
+    v = boundary_scale(a, v, c, ix, iy, iz);
+    v = taper(a, v, ix, iy, iz);
+    a.next[c][so + i] += v;
 }
 
 // Post-injection: next += taper(scale(dt^2 (w s)/rho)) (elastic) or dt^2 (w s) K
@@ -836,7 +834,7 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         StepArgs f = a;
         f.y0 = 0;
         f.y1 = pb_.ny;
-        const dim3 sgrd((unsigned)((nf + 127) / 128), pb_.nshots);
+        const dim3 sgrd((unsigned)((nf + 127) / 128), pb_.nshots, 3);
         if (pb_.nmodels == 3) k_elastic_face_sat<ELASTIC><<<sgrd, 128, 0, s>>>(f, nf);
         else k_elastic_face_sat<VTI><<<sgrd, 128, 0, s>>>(f, nf);
         CK(cudaGetLastError());
@@ -932,7 +930,7 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         const int64_t ly = sat.y1 - sat.y0;
         int64_t nf = 2 * (int64_t)pb_.nx * ly + 2 * (int64_t)(pb_.nz - 2) * ly;
         if (slab_march_) nf += 2 * (int64_t)(pb_.nx - 2) * (pb_.nz - 2);
-        const dim3 sgrd((unsigned)((nf + 127) / 128), pb_.nshots);
+        const dim3 sgrd((unsigned)((nf + 127) / 128), pb_.nshots, 3);
         if (pb_.nmodels == 3) k_elastic_face_sat<ELASTIC><<<sgrd, 128, 0, s>>>(sat, nf);
         else k_elastic_face_sat<VTI><<<sgrd, 128, 0, s>>>(sat, nf);
     }

@@ -353,33 +353,35 @@ FWI_HD float elastic_face(const StepArgs &a, float acc, int c, int n, bool hi, i
     // in1/in2 tangential axes and the fields they carry:
     //   n = z: in1 along x, in2 along y ; n = x: in1 along y, in2 along z ; n = y: in1 along x, in2 along z
     // tangential comp c: in(c-slot) = u_n ; normal comp: in1 = u_t1, in2 = u_t2, in3 = u_n
-    float T1 = 0.f, T2 = 0.f, N0 = 0.f, S;
+    // all samples are read unconditionally (valid addresses on every face),
+    // so that their loads issue together; the coefficients select the terms
+    float T1, T2, N0, S;
     if (n == 2) {
         d1 = a.dx; d2 = a.dy; dn = a.dz;
         const float *in1 = (c == 2) ? cu[0] : cu[2];
         const float *in2 = (c == 2) ? cu[1] : cu[2];
-        if (s.f1 != 0.f) T1 = d1_row(g.lx(in1, iy, iz), ix, g.nx);
-        if (s.f2 != 0.f) T2 = d1_row(g.ly(in2, ix, iz), iy, g.ny);
+        T1 = d1_row(g.lx(in1, iy, iz), ix, g.nx);
+        T2 = d1_row(g.ly(in2, ix, iz), iy, g.ny);
         const Line l3 = g.lz(cu[c], ix, iy);
-        if (s.f3 != 0.f) N0 = d1_wall(l3, g.nz, hi);
+        N0 = d1_wall(l3, g.nz, hi);
         S = sbound(l3, g.nz, hi);
     } else if (n == 0) {
         d1 = a.dy; d2 = a.dz; dn = a.dx;
         const float *in1 = (c == 0) ? cu[1] : cu[0];
         const float *in2 = (c == 0) ? cu[2] : cu[0];
-        if (s.f1 != 0.f) T1 = d1_row(g.ly(in1, ix, iz), iy, g.ny);
-        if (s.f2 != 0.f) T2 = d1_row(g.lz(in2, ix, iy), iz, g.nz);
+        T1 = d1_row(g.ly(in1, ix, iz), iy, g.ny);
+        T2 = d1_row(g.lz(in2, ix, iy), iz, g.nz);
         const Line l3 = g.lx(cu[c], iy, iz);
-        if (s.f3 != 0.f) N0 = d1_wall(l3, g.nx, hi);
+        N0 = d1_wall(l3, g.nx, hi);
         S = sbound(l3, g.nx, hi);
     } else {
         d1 = a.dx; d2 = a.dz; dn = a.dy;
         const float *in1 = (c == 1) ? cu[0] : cu[1];
         const float *in2 = (c == 1) ? cu[2] : cu[1];
-        if (s.f1 != 0.f) T1 = d1_row(g.lx(in1, iy, iz), ix, g.nx);
-        if (s.f2 != 0.f) T2 = d1_row(g.lz(in2, ix, iy), iz, g.nz);
+        T1 = d1_row(g.lx(in1, iy, iz), ix, g.nx);
+        T2 = d1_row(g.lz(in2, ix, iy), iz, g.nz);
         const Line l3 = g.ly(cu[c], ix, iz);
-        if (s.f3 != 0.f) N0 = d1_wall(l3, g.ny, hi);
+        N0 = d1_wall(l3, g.ny, hi);
         S = sbound(l3, g.ny, hi);
     }
     const float adh = (float)(1.0 / (double)(dn * h0));
