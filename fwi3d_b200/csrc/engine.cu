@@ -194,7 +194,9 @@ __device__ __forceinline__ void fz_tma_wait(FusedCtx &c, int slot)
     }
 }
 
-template <int PH, bool XF, bool ZF>
+// AX: edge tiles of the isotropic kernel take the per-axis output code (the
+// split launch); otherwise its edge tiles take the per-point code.
+template <int PH, bool XF, bool ZF, bool AX = false>
 __device__ __forceinline__ void fused_march(FusedCtx &c, int tid, int ya, int yb)
 {
     FusedThread th;
@@ -232,7 +234,7 @@ __device__ __forceinline__ void fused_march(FusedCtx &c, int tid, int ya, int yb
         if (y >= ya) fz_derived<PH, XF, ZF>(c, tid, y);
         __syncthreads();
         if (y >= ya) {
-            if (PH == ELASTIC && !(XF && ZF)) fz_output<PH>(c, th, tid, y);
+            if (PH == ELASTIC && !(XF && ZF) && !(AX && (XF || ZF))) fz_output<PH>(c, th, tid, y);
             else fz_output_t<PH, XF, ZF>(c, th, tid, y);
         }
         __syncthreads();
@@ -275,6 +277,45 @@ __global__ void __launch_bounds__(fz::NT, MINB)
     else if (PH == VTI && xf) fused_march<PH, true, false>(c, tid, ya, yb);
     else if (PH == VTI && zf) fused_march<PH, false, true>(c, tid, ya, yb);
     else fused_march<PH, false, false>(c, tid, ya, yb);
+}
+
+// Isotropic fused step split by tiles: MODE 1 runs the interior tiles only
+// (grid tile indices offset by (bz0, bx0)), MODE 2 the edge tiles only (the
+// interior tiles of its full grid return at once).  Separate launches give
+// each its own register allocation: the interior code runs without spills
+// and the edge tiles can keep the closure-free code on their interior axis.
+template <int MODE>
+__global__ void __launch_bounds__(fz::NT, 2)
+    k_elastic_fused_part(const __grid_constant__ StepArgs a, int nchunks, const __grid_constant__ FusedTma t,
+                         int bz0, int bx0)
+{
+    extern __shared__ __align__(128) unsigned char fz_smem[];
+    FusedCtx c;
+    c.a = &a;
+    c.sm = reinterpret_cast<FusedSmem *>(fz_smem);
+    c.tmap = &t.u;
+    c.err = t.err;
+    c.tma = t.on && (fz_saddr(fz_smem) & 127u) == 0;
+    c.rows.p = c.sm->rows;
+    const int tid = threadIdx.x + fz::TZ * threadIdx.y;
+    c.shot = blockIdx.z / nchunks;
+    const int ch = blockIdx.z - c.shot * nchunks;
+    c.so = c.shot * a.sst;
+    tile_range(blockIdx.x + (MODE == 1 ? bz0 : 0), a.g.nz, fz::TZ, c.z0, c.zend);
+    tile_range(blockIdx.y + (MODE == 1 ? bx0 : 0), a.g.nx, fz::TX, c.x0, c.xend);
+    const int len = a.y1 - a.y0;
+    const int ya = a.y0 + (int)((int64_t)len * ch / nchunks);
+    const int yb = a.y0 + (int)((int64_t)len * (ch + 1) / nchunks);
+    if (ya >= yb) return;
+    if (MODE == 1) {
+        fused_march<ELASTIC, true, true, true>(c, tid, ya, yb);
+        return;
+    }
+    const bool xf = fz_interior_tile(c.x0, fz::TX, a.g.nx), zf = fz_interior_tile(c.z0, fz::TZ, a.g.nz);
+    if (xf && zf) return;
+    if (xf) fused_march<ELASTIC, true, false, true>(c, tid, ya, yb);
+    else if (zf) fused_march<ELASTIC, false, true, true>(c, tid, ya, yb);
+    else fused_march<ELASTIC, false, false, true>(c, tid, ya, yb);
 }
 
 // Acoustic marching step (see acoustic.cuh).  grid: (z tiles, x tiles,
@@ -608,6 +649,9 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     // (default, the faster on B200) or 1 CTA per SM with up to 128 registers.
     const char *mb = std::getenv("FWI_FUSED_MINB");
     fused_minb_ = (mb && mb[0] == '1') ? 1 : 2;
+    // isotropic media: interior and edge tiles in two launches (FWI_FUSED_SPLIT=0: one)
+    const char *sp = std::getenv("FWI_FUSED_SPLIT");
+    fused_split_ = !(sp && sp[0] == '0');
     // plane copies of the fused kernel by the tensor memory accelerator
     // (FWI_TMA=0: per-thread asynchronous copies instead)
     const char *te = std::getenv("FWI_TMA");
@@ -622,6 +666,10 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
         CK(cudaFuncSetAttribute(k_elastic_fused<ELASTIC, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(FusedSmem)));
         CK(cudaFuncSetAttribute(k_elastic_fused<VTI, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(FusedSmem)));
+        CK(cudaFuncSetAttribute(k_elastic_fused_part<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(FusedSmem)));
+        CK(cudaFuncSetAttribute(k_elastic_fused_part<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(FusedSmem)));
     }
 }
@@ -902,22 +950,43 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         f.y1 = pb_.ny - P;
         for (int k = 0; k < 9; k++) f.aux[k] = nullptr;
         const int kz = (pb_.nz + fz::TZ - 1) / fz::TZ, kx = (pb_.nx + fz::TX - 1) / fz::TX;
-        const int tiles = kz * kx * pb_.nshots;
-        const int target = 148 * fused_minb_ * 4;  // about four waves of resident CTAs
-        int nch = (target + tiles - 1) / tiles;
-        nch = std::max(1, std::min(nch, (f.y1 - f.y0) / 16));
-        const dim3 grd(kz, kx, nch * pb_.nshots), fblk(fz::TZ, fz::TX);
         FusedTma tm;
         std::memset(&tm, 0, sizeof(tm));
         tm.err = tma_err_.as<int>();
         tm.on = tma_ && encode_level_map(&tm.u, curr, pb_) ? 1 : 0;
+        const dim3 fblk(fz::TZ, fz::TX);
+        const size_t sm = sizeof(FusedSmem);
+        // y chunks per tile column: about four waves of resident CTAs, at
+        // least 16 planes per chunk
+        auto chunks = [&](int64_t tiles, int minb) {
+            const int64_t target = 148 * minb * 4;
+            const int64_t c = (target + tiles - 1) / tiles;
+            return (int)std::max<int64_t>(1, std::min<int64_t>(c, (f.y1 - f.y0) / 16));
+        };
+        // interior tiles form the index box [zl, zh) x [xl, xh)
+        int zl, zh, xl, xh;
+        fz_interior_range(pb_.nz, fz::TZ, zl, zh);
+        fz_interior_range(pb_.nx, fz::TX, xl, xh);
+        const bool el = pb_.nmodels == 3;
+        const bool split = el && fused_split_ && fused_minb_ == 2 && zh > zl && xh > xl;
         kmark(true, "k_elastic_fused", (int64_t)(f.y1 - f.y0) * pb_.nx * pb_.nz * pb_.nshots);
-        if (fused_minb_ == 2) {
-            if (pb_.nmodels == 3) k_elastic_fused<ELASTIC, 2><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch, tm);
-            else k_elastic_fused<VTI, 2><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch, tm);
+        if (split) {
+            const int64_t ti = (int64_t)(zh - zl) * (xh - xl) * pb_.nshots;
+            const int64_t te = (int64_t)kz * kx * pb_.nshots - ti;
+            const int ne = chunks(te, 2), ni = chunks(ti, 2);
+            const dim3 ge(kz, kx, ne * pb_.nshots), gi(zh - zl, xh - xl, ni * pb_.nshots);
+            k_elastic_fused_part<2><<<ge, fblk, sm, s>>>(f, ne, tm, 0, 0);
+            k_elastic_fused_part<1><<<gi, fblk, sm, s>>>(f, ni, tm, zl, xl);
         } else {
-            if (pb_.nmodels == 3) k_elastic_fused<ELASTIC, 1><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch, tm);
-            else k_elastic_fused<VTI, 1><<<grd, fblk, sizeof(FusedSmem), s>>>(f, nch, tm);
+            const int nch = chunks((int64_t)kz * kx * pb_.nshots, fused_minb_);
+            const dim3 grd(kz, kx, nch * pb_.nshots);
+            if (fused_minb_ == 2) {
+                if (el) k_elastic_fused<ELASTIC, 2><<<grd, fblk, sm, s>>>(f, nch, tm);
+                else k_elastic_fused<VTI, 2><<<grd, fblk, sm, s>>>(f, nch, tm);
+            } else {
+                if (el) k_elastic_fused<ELASTIC, 1><<<grd, fblk, sm, s>>>(f, nch, tm);
+                else k_elastic_fused<VTI, 1><<<grd, fblk, sm, s>>>(f, nch, tm);
+            }
         }
         kmark(false, nullptr, 0);
         // SAT of the x/z faces of the fused planes (and, with the marching

@@ -689,6 +689,28 @@ FWI_HD void tile_range(int k, int n, int T, int &origin, int &end)
     }
 }
 
+// A tile (window origin x0, T points) whose outputs and derived halo all lie
+// at least 6 points inside the grid along its axis: no SBP closure row.
+FWI_HD bool fz_interior_tile(int x0, int T, int n) { return x0 >= 6 && x0 + T <= n - 6; }
+
+// Tile indices [lo, hi) of the interior tiles along an axis of n points (the
+// predicate is monotone in the tile origin, so they are contiguous).
+inline void fz_interior_range(int n, int T, int &lo, int &hi)
+{
+    const int K = (n + T - 1) / T;
+    lo = K;
+    hi = K;
+    for (int k = 0; k < K; k++) {
+        int o, e;
+        tile_range(k, n, T, o, e);
+        if (fz_interior_tile(o, T, n)) {
+            if (lo == K) lo = k;
+            hi = k + 1;
+        }
+    }
+    if (lo == K) lo = hi = 0;
+}
+
 // The march of one CTA over output planes [ya, yb) (all inside [8, ny-8)).
 template <int PH>
 FWI_HD void fz_prologue(FusedCtx &c, int tid, int ya)
