@@ -968,7 +968,7 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         fz_interior_range(pb_.nz, fz::TZ, zl, zh);
         fz_interior_range(pb_.nx, fz::TX, xl, xh);
         const bool el = pb_.nmodels == 3;
-        const bool split = el && fused_split_ && fused_minb_ == 2 && zh > zl && xh > xl;
+        const bool split = fused_split_active();
         kmark(true, "k_elastic_fused", (int64_t)(f.y1 - f.y0) * pb_.nx * pb_.nz * pb_.nshots);
         if (split) {
             const int64_t ti = (int64_t)(zh - zl) * (xh - xl) * pb_.nshots;
@@ -1076,10 +1076,19 @@ double Engine::main_kernel_ms(int *launches, int64_t *points, const char **name)
     return ms;
 }
 
+bool Engine::fused_split_active() const
+{
+    int zl, zh, xl, xh;
+    fz_interior_range(pb_.nz, fz::TZ, zl, zh);
+    fz_interior_range(pb_.nx, fz::TX, xl, xh);
+    return pb_.nmodels == 3 && fused_split_ && fused_minb_ == 2 && zh > zl && xh > xl;
+}
+
 int Engine::launches_per_step() const
 {
     int k = (pb_.nmodels == 2 ? 1
                               : (march_ ? 2 : (fused_ ? (slab_march_ ? 3 : (pb_.ny < 2 * (fz::YPAD + 2) ? 5 : 6)) : 2)));
+    if (fused_ && fused_split_active()) k += 1;  // interior and edge tiles launched apart
     if (ext_.nrec) k += 1;
     for (int c = 0; c < 3; c++) k += inj_.n[c] ? 1 : 0;
     return k;

@@ -170,6 +170,7 @@ private:
     bool fused_ = false;           // fused elastic kernel for the interior planes
     int fused_minb_ = 2;           // resident CTAs per SM the fused kernel is compiled for
     bool fused_split_ = true;      // interior and edge tiles of the fused kernel in separate launches
+    bool fused_split_active() const;
     bool tma_ = false;             // fused kernel copies planes with bulk-tensor copies
     DevBuf tma_err_;               // int: a fused-kernel wait for a plane copy gave up
     DevBuf src_dev_, rcv_dev_;
