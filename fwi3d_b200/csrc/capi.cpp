@@ -7,6 +7,8 @@
 // the mutable _zfp_wfld member, we_op.hpp:23).
 #include <algorithm>
 #include <cmath>
+#include <chrono>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -157,6 +159,7 @@ struct fwi_objective {
     Problem pb{};
     std::map<int, std::unique_ptr<Engine>> eng;  // one engine per batch size
     int64_t device_bytes = 0;
+    DeviceResidual dres;  // residual on the device (observed traces, resampling taps)
 };
 
 extern "C" {
@@ -665,7 +668,23 @@ int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, floa
         std::vector<double> gsum((size_t)nm * n, 0.0);
         double fsum = 0.0;
         o->device_bytes = 0;
+        // FWI_OBJ_TIMING=1: per-batch phase times on stderr (host clock)
+        const char *tenv = std::getenv("FWI_OBJ_TIMING");
+        const bool timing = tenv && tenv[0] == '1';
+        auto now = [] { return std::chrono::steady_clock::now(); };
+        auto secs = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+            return std::chrono::duration<double>(b - a).count();
+        };
+        // Residual on the device (sinc resampling, traces that fit in shared
+        // memory; FWI_HOST_RESIDUAL=1 keeps the host path)
+        const char *hre = std::getenv("FWI_HOST_RESIDUAL");
+        const bool on_device = sinc && std::max(nt, ntd) <= kResidualMaxSamples && !(hre && hre[0] == '1');
+        if (on_device) {
+            o->dres.set_observed(o->device, o->observed);
+            o->dres.set_axes(par.sinc_half_length, ntd, o->dt_data, nt, p.dt);
+        }
         for (int s0 = 0; s0 < o->nshots; s0 += o->batch) {
+            const auto t0 = now();
             const int B = std::min(o->batch, o->nshots - s0);
             p.nshots = B;
             auto &eng = o->eng[B];
@@ -707,9 +726,32 @@ int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, floa
                 for (auto gi : e.gidx) ext.gidx.push_back(gi + b * n);
                 ext.w.insert(ext.w.end(), e.w.begin(), e.w.end());
             }
+            const auto t1 = now();
+            if (on_device) {
+                eng->forward(inj, B * o->nscomp, src.data(), ext, nullptr, true);
+                const auto t2 = now();
+                const size_t ntrb = (size_t)B * ntr;
+                fsum += o->dres.run(*eng, (size_t)s0 * ntr * ntd, (int)ntrb, par.seismotype, alpha,
+                                    residual ? residual + (size_t)s0 * ntr * ntd : nullptr);
+                std::vector<float> gb((size_t)nm * n);
+                const auto t3 = now();
+                eng->adjoint_dev(adj, (int)ntrb, o->dres.adjoint_sources(), gb.data());
+                const auto t4 = now();
+                for (size_t i = 0; i < gb.size(); i++) gsum[i] += gb[i];
+                if (timing)
+                    std::fprintf(stderr,
+                                 "objective batch %d: prep %.3f s, forward %.3f s, device residual %.3f s, adjoint %.3f s\n",
+                                 s0 / o->batch, secs(t0, t1), secs(t1, t2), secs(t2, t3), secs(t3, t4));
+                o->device_bytes = std::max(o->device_bytes, eng->device_bytes());
+                o->pb = p;
+                continue;
+            }
             std::vector<float> rcv((size_t)B * ntr * nt);
             eng->forward(inj, B * o->nscomp, src.data(), ext, rcv.data(), true);
+            const auto t2 = now();
             if (!finite_all(rcv.data(), (int64_t)rcv.size())) throw FwiError(FWI_ERR_NAN, "non-finite values in the traces");
+            const auto tr0 = now();
+            double t_ra = 0, t_rf = 0;
             std::vector<float> asrc((size_t)B * ntr * nt);
             std::vector<float> syn((size_t)ntr * ntd), tmp;
             for (int b = 0; b < B; b++) {
@@ -722,7 +764,9 @@ int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, floa
                 }
                 for (size_t i = 0; i < (size_t)ntr * nt; i++) r[i] *= alpha;
                 std::fill(syn.begin(), syn.end(), 0.f);
+                const auto ta0 = now();
                 resample_adjoint(sinc, par.sinc_half_length, syn.data(), ntd, o->dt_data, r, nt, p.dt, ntr);
+                t_ra += secs(ta0, now());
                 // residual and misfit (optimization.cpp:111-115, optimization.hpp:410-424), FP64 sums
                 const float *obs = &o->observed[(size_t)sh * ntr * ntd];
                 for (size_t i = 0; i < syn.size(); i++) syn[i] -= obs[i];
@@ -737,7 +781,9 @@ int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, floa
                 // adjoint sources: Ht(r) (optimization.cpp:118), then jacobianT's data path (we_op.cpp:994-1003)
                 apply_ht(false, syn.data(), syn.data(), ntr, ntd, o->dt_data);
                 float *as = asrc.data() + (size_t)b * ntr * nt;
+                const auto tf0 = now();
                 resample_forward(sinc, par.sinc_half_length, syn.data(), ntd, o->dt_data, as, nt, p.dt, ntr);
+                t_rf += secs(tf0, now());
                 apply_ht(true, as, as, ntr, nt, p.dt);
                 for (int tr = 0; tr < ntr; tr++) std::reverse(as + (size_t)tr * nt, as + (size_t)(tr + 1) * nt);
                 for (size_t i = 0; i < (size_t)ntr * nt; i++) as[i] *= -alpha;
@@ -748,8 +794,16 @@ int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, floa
                 }
             }
             std::vector<float> gb((size_t)nm * n);
+            const auto t3 = now();
             eng->adjoint(adj, B * ntr, asrc.data(), gb.data());
+            const auto t4 = now();
             for (size_t i = 0; i < gb.size(); i++) gsum[i] += gb[i];
+            if (timing)
+                std::fprintf(stderr,
+                             "objective batch %d: prep %.3f s, forward %.3f s, residual %.3f s (check %.3f, "
+                             "resample adj %.3f fwd %.3f; nt %d ntd %d ntr %d), adjoint %.3f s\n",
+                             s0 / o->batch, secs(t0, t1), secs(t1, t2), secs(t2, t3), secs(t2, tr0), t_ra, t_rf, nt,
+                             ntd, ntr, secs(t3, t4));
             o->device_bytes = std::max(o->device_bytes, eng->device_bytes());
             o->pb = p;
         }

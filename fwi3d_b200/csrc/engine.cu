@@ -1402,8 +1402,216 @@ void Engine::forward(const InjTable &inj, int ntrace, const float *src, const Ex
         dec_lo_ = K - 1;
     }
     extract_last();
-    copy_traces(rcv);
+    if (rcv) copy_traces(rcv);
     snaps_valid_ = keep;
+}
+
+// ---------------------------------------------------------------------------
+// Device residual of the FWI objective (ResidualArgs in engine.h).  Each
+// sample is formed with the host path's float / double operations, without
+// contraction, in the same order; only the misfit sum is reassociated (FP64
+// partials per trace, summed in trace order on the host).
+// ---------------------------------------------------------------------------
+namespace {
+__device__ __forceinline__ float rs_tap(float acc, float v, float s, double w)
+{
+    // acc = (float)((double)acc + (double)(v * s) * w)   (operator.cpp:472-520)
+    return __double2float_rn(__dadd_rn((double)acc, __dmul_rn((double)__fmul_rn(v, s), w)));
+}
+
+// Dt of one trace (misc.cpp:70-94), adj as apply_dt
+__device__ void rs_dt(bool adj, const float *in, float *out, int nt, float dt)
+{
+    for (int it = threadIdx.x; it < nt; it += blockDim.x) {
+        float v;
+        if (!adj) {
+            if (it == 0) v = __fdiv_rn(__fsub_rn(in[1], in[0]), dt);
+            else if (it == nt - 1) v = __fdiv_rn(__fsub_rn(in[nt - 1], in[nt - 2]), dt);
+            else v = __fdiv_rn(__fsub_rn(in[it + 1], in[it - 1]), __fmul_rn(2.f, dt));
+        } else {
+            if (it == 0) v = __fdiv_rn(__fadd_rn(in[1], in[0]), dt);
+            else if (it == nt - 1) v = __fdiv_rn(__fsub_rn(-in[nt - 1], in[nt - 2]), dt);
+            else v = __fdiv_rn(__fsub_rn(in[it + 1], in[it - 1]), __fmul_rn(2.f, dt));
+        }
+        out[it] = v;
+    }
+}
+
+__global__ void k_residual(ResidualArgs a)
+{
+    extern __shared__ float rs_sm[];
+    const int nt = a.nt, ntd = a.ntd;
+    float *r = rs_sm, *syn = rs_sm + nt, *as = syn + ntd, *tmp = as + nt;
+    __shared__ double red[32];
+    const int64_t tr = blockIdx.x;
+    const float *src = a.rcv + tr * nt;
+    bool bad = false;
+    for (int it = threadIdx.x; it < nt; it += blockDim.x) {
+        const float v = src[it];
+        bad |= !isfinite(v);
+        r[it] = v;
+    }
+    if (bad) atomicOr(a.bad, 1);
+    __syncthreads();
+    if (a.seismotype == 1) {
+        rs_dt(false, r, tmp, nt, a.dt);
+        __syncthreads();
+        for (int it = threadIdx.x; it < nt; it += blockDim.x) r[it] = tmp[it];
+        __syncthreads();
+    }
+    for (int it = threadIdx.x; it < nt; it += blockDim.x) r[it] = __fmul_rn(r[it], a.alpha);
+    __syncthreads();
+    // adjoint resampling (gather over the propagation samples that reach j,
+    // in increasing order as the host's scatter adds them), minus observed
+    const float *ob = a.obs + tr * ntd;
+    double ss = 0.0;
+    for (int j = threadIdx.x; j < ntd; j += blockDim.x) {
+        float d = 0.f;
+        for (int itd = a.jlo[j]; itd < a.jhi[j]; itd++) {
+            const int k = j - a.first[itd];
+            if (k < 0 || k >= a.count[itd]) continue;
+            const int q = a.off[itd] + k;
+            d = rs_tap(d, r[itd], a.s[q], a.win[q]);
+        }
+        d = __fsub_rn(d, ob[j]);
+        syn[j] = d;
+        if (a.resid) a.resid[tr * ntd + j] = d;
+        ss = __dadd_rn(ss, __dmul_rn((double)d, (double)d));
+    }
+    // block sum of the squares (FP64)
+    for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = ss;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+        const double a0 = syn[0], a1 = syn[ntd - 1];
+        a.part[tr] = t - 0.5 * (a0 * a0 + a1 * a1);
+    }
+    __syncthreads();
+    // Ht on the data axis (misc.cpp:44-68)
+    for (int j = threadIdx.x; j < ntd; j += blockDim.x) {
+        const float v = syn[j];
+        tmp[j] = (j == 0 || j == ntd - 1) ? __double2float_rn(__dmul_rn(__dmul_rn((double)v, 0.5), (double)a.dtd))
+                                           : __fmul_rn(v, a.dtd);
+    }
+    __syncthreads();
+    // forward resampling to the propagation axis, Ht^-1
+    for (int it = threadIdx.x; it < nt; it += blockDim.x) {
+        float acc = 0.f;
+        const int f0 = a.first[it], c0 = a.count[it], q0 = a.off[it];
+        for (int k = 0; k < c0; k++) acc = rs_tap(acc, tmp[f0 + k], a.s[q0 + k], a.win[q0 + k]);
+        as[it] = (it == 0 || it == nt - 1) ? __double2float_rn(__ddiv_rn((double)acc, __dmul_rn(0.5, (double)a.dt)))
+                                           : __fdiv_rn(acc, a.dt);
+    }
+    __syncthreads();
+    // time reversal and -alpha, then Dt^T for velocity data
+    const float na = -a.alpha;
+    for (int it = threadIdx.x; it < nt; it += blockDim.x) r[it] = __fmul_rn(as[nt - 1 - it], na);
+    __syncthreads();
+    const float *fin = r;
+    if (a.seismotype == 1) {
+        rs_dt(true, r, tmp, nt, a.dt);
+        __syncthreads();
+        fin = tmp;
+    }
+    float *dst = a.asrc + tr * nt;
+    for (int it = threadIdx.x; it < nt; it += blockDim.x) dst[it] = fin[it];
+}
+}  // namespace
+
+void DeviceResidual::set_observed(int device, const std::vector<float> &obs)
+{
+    if (device_ == device && obs_.bytes == sizeof(float) * obs.size()) return;
+    CK(cudaSetDevice(device));
+    obs_.alloc(sizeof(float) * obs.size());
+    CK(cudaMemcpy(obs_.p, obs.data(), obs_.bytes, cudaMemcpyHostToDevice));
+    device_ = device;
+}
+
+void DeviceResidual::set_axes(int hl, int ntd, float dtd, int nt, float dt)
+{
+    if (hl == hl_ && ntd == ntd_ && dtd == dtd_ && nt == nt_ && dt == dt_) return;
+    std::vector<int> first, count;
+    std::vector<float> sv;
+    std::vector<double> wv;
+    sinc_resample_taps(hl, ntd, dtd, nt, dt, first, count, sv, wv);
+    std::vector<int> off(nt + 1, 0), jlo(ntd, nt), jhi(ntd, 0);
+    for (int it = 0; it < nt; it++) off[it + 1] = off[it] + count[it];
+    for (int it = 0; it < nt; it++)
+        for (int k = 0; k < count[it]; k++) {
+            const int j = first[it] + k;
+            jlo[j] = std::min(jlo[j], it);
+            jhi[j] = std::max(jhi[j], it + 1);
+        }
+    for (int j = 0; j < ntd; j++)
+        if (jlo[j] >= jhi[j]) jlo[j] = jhi[j] = 0;
+    auto up = [](DevBuf &b, const void *h, size_t bytes) {
+        b.alloc(std::max<size_t>(bytes, 8));
+        if (bytes) CK(cudaMemcpy(b.p, h, bytes, cudaMemcpyHostToDevice));
+    };
+    up(first_, first.data(), sizeof(int) * first.size());
+    up(count_, count.data(), sizeof(int) * count.size());
+    up(off_, off.data(), sizeof(int) * off.size());
+    up(s_, sv.data(), sizeof(float) * sv.size());
+    up(win_, wv.data(), sizeof(double) * wv.size());
+    up(jlo_, jlo.data(), sizeof(int) * jlo.size());
+    up(jhi_, jhi.data(), sizeof(int) * jhi.size());
+    hl_ = hl;
+    ntd_ = ntd;
+    dtd_ = dtd;
+    nt_ = nt;
+    dt_ = dt;
+}
+
+double DeviceResidual::run(Engine &eng, size_t obs_offset, int ntraces, int seismotype, float alpha, float *residual)
+{
+    if (ntraces <= 0) return 0.0;
+    cudaStream_t st = (cudaStream_t)eng.stream();
+    const size_t nt = (size_t)nt_, ntd = (size_t)ntd_;
+    if (asrc_.bytes < sizeof(float) * ntraces * nt) asrc_.alloc(sizeof(float) * ntraces * nt);
+    if (part_.bytes < sizeof(double) * ntraces) part_.alloc(sizeof(double) * ntraces);
+    if (residual && resid_.bytes < sizeof(float) * ntraces * ntd) resid_.alloc(sizeof(float) * ntraces * ntd);
+    if (!bad_.p) bad_.alloc(sizeof(int));
+    CK(cudaMemsetAsync(bad_.p, 0, sizeof(int), st));
+    ResidualArgs a{};
+    a.rcv = eng.traces_dev();
+    a.obs = obs_.as<float>() + obs_offset;
+    a.asrc = asrc_.as<float>();
+    a.resid = residual ? resid_.as<float>() : nullptr;
+    a.part = part_.as<double>();
+    a.bad = bad_.as<int>();
+    a.first = first_.as<int>();
+    a.count = count_.as<int>();
+    a.off = off_.as<int>();
+    a.s = s_.as<float>();
+    a.win = win_.as<double>();
+    a.jlo = jlo_.as<int>();
+    a.jhi = jhi_.as<int>();
+    a.nt = nt_;
+    a.ntd = ntd_;
+    a.seismotype = seismotype;
+    a.alpha = alpha;
+    a.dt = dt_;
+    a.dtd = dtd_;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        CK(cudaFuncSetAttribute(k_residual, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(sizeof(float) * 4 * kResidualMaxSamples)));
+    });
+    const size_t sm = sizeof(float) * (2 * nt + 2 * std::max(nt, ntd));
+    k_residual<<<ntraces, 128, sm, st>>>(a);
+    CK(cudaGetLastError());
+    std::vector<double> part(ntraces);
+    int bad = 0;
+    CK(cudaMemcpyAsync(part.data(), part_.p, sizeof(double) * ntraces, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&bad, bad_.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (residual) CK(cudaMemcpyAsync(residual, resid_.p, sizeof(float) * ntraces * ntd, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (bad) throw FwiError(FWI_ERR_NAN, "non-finite values in the traces");
+    double sum = 0.0;
+    for (int k = 0; k < ntraces; k++) sum += part[k];
+    return sum;
 }
 
 void Engine::image(int itl, const float *curr, const float *prevl)
@@ -1448,6 +1656,16 @@ void Engine::image(int itl, const float *curr, const float *prevl)
 
 void Engine::adjoint(const InjTable &inj, int ntrace, const float *adj_src, float *grad)
 {
+    adjoint_impl(inj, ntrace, adj_src, nullptr, grad);
+}
+
+void Engine::adjoint_dev(const InjTable &inj, int ntrace, const float *adj_src_dev, float *grad)
+{
+    adjoint_impl(inj, ntrace, nullptr, adj_src_dev, grad);
+}
+
+void Engine::adjoint_impl(const InjTable &inj, int ntrace, const float *adj_src, const float *adj_src_dev, float *grad)
+{
     CK(cudaSetDevice(device_));
     if (!snaps_valid_) throw FwiError(FWI_ERR_STATE, "adjoint needs the snapshots of a preceding forward with sub > 0");
     cudaStream_t s = (cudaStream_t)stream_;
@@ -1455,18 +1673,23 @@ void Engine::adjoint(const InjTable &inj, int ntrace, const float *adj_src, floa
     const int nm = std::min(3, pb_.nmodels);
     DevInj dinj;
     upload_inj(inj, ntrace, dinj);
-    DevBuf asrc(sizeof(float) * (size_t)ntrace * pb_.nt);
-    CK(cudaMemcpyAsync(asrc.p, adj_src, asrc.bytes, cudaMemcpyHostToDevice, s));
+    DevBuf asrc_own;
+    const float *asrc_p = adj_src_dev;
+    if (!asrc_p) {
+        asrc_own.alloc(sizeof(float) * (size_t)ntrace * pb_.nt);
+        CK(cudaMemcpyAsync(asrc_own.p, adj_src, asrc_own.bytes, cudaMemcpyHostToDevice, s));
+        asrc_p = asrc_own.as<float>();
+    }
     grad_.alloc(sizeof(double) * nm * n);
     grad_.zero(s);
     rot_ = 0;
     fields_.zero(s);
-    init_prev(dinj, asrc.as<float>(), level(0));
+    init_prev(dinj, asrc_p, level(0));
     const int sub = pb_.sub;
     for (int it = 0; it < pb_.nt - 1; it++) {
         if ((pb_.nt - 1 - it) % sub == 0 && it != 0) image((pb_.nt - 1 - it) / sub, level(1), level(0));
         step(level(0), level(1), level(2), it > 0);
-        inject(dinj, asrc.as<float>(), it, level(2));
+        inject(dinj, asrc_p, it, level(2));
         rot_ = (rot_ + 1) % 3;
     }
     image(0, level(1), level(0));

@@ -20,6 +20,30 @@ struct FwiError : std::runtime_error {
 };
 
 // Device buffer (RAII).
+// Device residual of the FWI objective, one trace per CUDA block: from the
+// synthetic traces at the propagation sampling to the misfit partial of each
+// trace and the adjoint sources, with the host path's arithmetic (capi.cpp,
+// fwi_objective_evaluate): [Dt], *alpha, sinc resampling to the data axis,
+// - observed, sum of squares minus the half end samples (FP64), Ht, sinc
+// resampling back, Ht^-1, time reversal, *(-alpha), [Dt^T].
+struct ResidualArgs {
+    const float *rcv;      // [ntraces][nt] synthetic traces
+    const float *obs;      // [ntraces][ntd] observed
+    float *asrc;           // [ntraces][nt] adjoint sources (out)
+    float *resid;          // [ntraces][ntd] residual (out, may be null)
+    double *part;          // [ntraces] misfit partials (out)
+    int *bad;              // set when a synthetic sample is not finite
+    const int *first, *count;  // sinc taps per propagation sample (data -> propagation axis)
+    const int *off;            // start of each propagation sample's taps in s / win
+    const float *s;
+    const double *win;
+    const int *jlo, *jhi;      // propagation samples whose taps reach data sample j
+    int nt, ntd, seismotype;
+    float alpha, dt, dtd;
+};
+// Largest trace length (either axis) the device residual keeps in shared memory.
+constexpr int kResidualMaxSamples = 12000;
+
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
@@ -105,6 +129,17 @@ public:
     // adjoint + imaging of every shot of the batch; grad out: [min(3,nm)][nxyz]
     // float, summed over the shots in FP64 (before H quadrature and chain rule)
     void adjoint(const InjTable &inj, int ntrace, const float *adj_src, float *grad);
+    // the same with the adjoint sources [ntrace][nt] already on the device
+    // (stream-ordered after the engine's earlier work)
+    void adjoint_dev(const InjTable &inj, int ntrace, const float *adj_src_dev, float *grad);
+    // traces of the last forward [nshots][ncomp][nr][nt] on the device (a
+    // forward called with rcv == nullptr leaves them there)
+    const float *traces_dev() const { return rcv_dev_.as<float>(); }
+
+private:
+    void adjoint_impl(const InjTable &inj, int ntrace, const float *adj_src, const float *adj_src_dev, float *grad);
+
+public:
     int64_t snapshot_bytes() const { return snaps_.bytes + snapq_.bytes + enc_.bytes + snapz_.bytes + ckpt_.bytes + rec_fields_.bytes; }
 
     // Diagnostic timing of the step's main kernel (the fused interior kernel,
@@ -190,5 +225,27 @@ private:
 // or 1 only, no taper, at most 2^18 grid points (fwi_elastic_step_static).
 void static_elastic_step(const fwi_grid &grid, int nmodels, const int bc[6], float dt, const float *model,
                          const float *prev, const float *curr, float *next, void *stream);
+
+// The FWI objective's residual on the device, batch by batch: observed
+// traces kept on the device, the sinc taps of the data and propagation axes,
+// the adjoint sources of the last batch (kernel k_residual, engine.cu).
+class DeviceResidual {
+public:
+    // upload the observed traces [nshots][ntr][ntd] once per device
+    void set_observed(int device, const std::vector<float> &obs);
+    // sinc taps between the data axis (ntd, dtd) and the propagation axis (nt, dt)
+    void set_axes(int hl, int ntd, float dtd, int nt, float dt);
+    // residual of the ntraces traces of eng's last forward against the observed
+    // traces from obs_offset on; returns the FP64 misfit sum (before 0.5 dt /
+    // dnorm), leaves the adjoint sources on the device and, when residual is
+    // not null, copies the residual [ntraces][ntd] there.  Synchronises eng's stream.
+    double run(Engine &eng, size_t obs_offset, int ntraces, int seismotype, float alpha, float *residual);
+    const float *adjoint_sources() const { return asrc_.as<float>(); }
+
+private:
+    int device_ = -1, nt_ = -1, ntd_ = -1, hl_ = -1;
+    float dt_ = 0.f, dtd_ = 0.f;
+    DevBuf obs_, first_, count_, off_, s_, win_, jlo_, jhi_, asrc_, resid_, part_, bad_;
+};
 
 }  // namespace fwi

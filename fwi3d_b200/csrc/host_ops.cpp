@@ -204,6 +204,16 @@ SincTaps sinc_taps(int hl, int nt_in, float dt_in, int nt_out, float dt_out)
 }
 }  // namespace
 
+void sinc_resample_taps(int hl, int nt_in, float dt_in, int nt_out, float dt_out, std::vector<int> &first,
+                        std::vector<int> &count, std::vector<float> &s, std::vector<double> &win)
+{
+    SincTaps T = sinc_taps(hl, nt_in, dt_in, nt_out, dt_out);
+    first = std::move(T.first);
+    count = std::move(T.count);
+    s = std::move(T.s);
+    win = std::move(T.win);
+}
+
 void resample_forward(bool sinc, int hl, const float *in, int nt_in, float dt_in, float *out, int nt_out, float dt_out,
                       int ntr)
 {

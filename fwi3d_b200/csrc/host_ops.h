@@ -40,6 +40,13 @@ void resample_forward(bool sinc, int hl, const float *in, int nt_in, float dt_in
 void resample_adjoint(bool sinc, int hl, float *in, int nt_in, float dt_in, const float *out, int nt_out, float dt_out,
                       int ntr);
 
+// Windowed-sinc taps of the resampler from an (nt_in, dt_in) axis to an
+// (nt_out, dt_out) axis: output sample t uses input samples first[t] ..
+// first[t] + count[t] - 1 with factors s (float) and window win (double),
+// concatenated in output order (the weights resample_forward/adjoint apply).
+void sinc_resample_taps(int hl, int nt_in, float dt_in, int nt_out, float dt_out, std::vector<int> &first,
+                        std::vector<int> &count, std::vector<float> &s, std::vector<double> &win);
+
 // Trapezoid quadrature Ht and time derivative Dt (misc.cpp:44-94).
 void apply_ht(bool inv, const float *in, float *out, int ntr, int nt, float dt);
 void apply_dt(bool adj, const float *in, float *out, int ntr, int nt, float dt);

@@ -182,3 +182,25 @@ def test_sharded_objective_matches_single_process():
         fs, gs, dns = fs + fl, gs + gl.astype(np.float64), dns + p.dn_local
     assert fs / dns == pytest.approx(f, rel=1e-6)
     assert rel(gs / dns, g) < 1e-6
+
+
+@pytest.mark.parametrize("seismotype", [0, 1])
+def test_device_residual_matches_host_path(monkeypatch, seismotype):
+    """The objective's residual on the device (default: sinc resampling,
+    misfit partials, Ht, time reversal, Dt for velocity data) gives the host
+    path's residual bit for bit (FWI_HOST_RESIDUAL=1), its misfit to FP64
+    reassociation, and its gradient up to the order of the adjoint
+    injection's atomic additions."""
+    sv, obs = _problem(nside=2)
+    sv.par.seismotype = seismotype
+    out = {}
+    for tag, env in (("host", "1"), ("dev", "0")):
+        monkeypatch.setenv("FWI_HOST_RESIDUAL", env)
+        obj = ops.FwiObjective(sv, obs, batch=2)
+        out[tag] = obj.evaluate(sv.model, want_residual=True)
+        obj.close()
+    fh, gh, rh = out["host"]
+    fd, gd, rd = out["dev"]
+    assert np.array_equal(rh, rd)
+    assert abs(fd - fh) <= 1e-12 * abs(fh)
+    assert rel(gd, gh) < 1e-6
