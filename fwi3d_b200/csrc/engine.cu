@@ -532,6 +532,7 @@ __global__ void k_image_batch(ImageArgs a, int nshots, int64_t sst)
     if (!point_of(a.g, (a.g.ny + BY - 1) / BY, ix, iy, iz, s)) return;
     const int64_t i = a.g.idx(ix, iy, iz);
     double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+    const bool in = ix >= 4 && ix < a.g.nx - 4 && iy >= 4 && iy < a.g.ny - 4 && iz >= 4 && iz < a.g.nz - 4;
     for (int sh = 0; sh < nshots; sh++) {
         if (PH == ACOUSTIC) {
             double k, b;
@@ -540,7 +541,8 @@ __global__ void k_image_batch(ImageArgs a, int nshots, int64_t sst)
             g1 += b;
         } else {
             double i0, i1, i2;
-            elastic_image_inc<PH>(a, sh * sst, ix, iy, iz, i0, i1, i2);
+            if (in) elastic_image_inc<PH, true>(a, sh * sst, ix, iy, iz, i0, i1, i2);
+            else elastic_image_inc<PH, false>(a, sh * sst, ix, iy, iz, i0, i1, i2);
             g0 += i0;
             g1 += i1;
             g2 += i2;

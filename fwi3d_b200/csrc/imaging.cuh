@@ -30,9 +30,19 @@ FWI_HD float dx1(const Dims &g, const float *p, int ix, int iy, int iz, float d)
 FWI_HD float dy1(const Dims &g, const float *p, int ix, int iy, int iz, float d) { return d1_row(g.ly(p, ix, iz), iy, g.ny) / d; }
 FWI_HD float dz1(const Dims &g, const float *p, int ix, int iy, int iz, float d) { return d1_row(g.lz(p, ix, iy), iz, g.nz) / d; }
 
+// Interior D1 at flat index i along a stride (with the 1/h): the interior
+// branch of d1_row, term for term.
+FWI_HD float d1s(const float *p, int64_t i, int64_t st, float d)
+{
+    const SbpTables &t = sbp();
+    return (t.d1c0 * (p[i + st] - p[i - st]) + t.d1c1 * (p[i + 2 * st] - p[i - 2 * st])) / d;
+}
+
 // Increments of the three gradients at one point for the shot whose fields
 // start at offset `so` (batches: shot s at s * shot stride).
-template <int PH>
+// IN: the point is at least 4 samples from every face, so every D1 is an
+// interior row and is read at constant strides (no closure tests).
+template <int PH, bool IN = false>
 FWI_HD void elastic_image_inc(const ImageArgs &a, int64_t so, int ix, int iy, int iz, double &inc0, double &inc1,
                               double &inc2)
 {
@@ -40,18 +50,19 @@ FWI_HD void elastic_image_inc(const ImageArgs &a, int64_t so, int ix, int iy, in
     const int64_t i = g.idx(ix, iy, iz);
     const float *const fn[3] = {a.fwd[1][0] + so, a.fwd[1][1] + so, a.fwd[1][2] + so};
     const float *const lag[3] = {a.lag[0] + so, a.lag[1] + so, a.lag[2] + so};
+    const int64_t SX = g.nz, SY = (int64_t)g.nx * g.nz;
+    auto DX = [&](const float *p) { return IN ? d1s(p, i, SX, a.dx) : dx1(g, p, ix, iy, iz, a.dx); };
+    auto DY = [&](const float *p) { return IN ? d1s(p, i, SY, a.dy) : dy1(g, p, ix, iy, iz, a.dy); };
+    auto DZ = [&](const float *p) { return IN ? d1s(p, i, 1, a.dz) : dz1(g, p, ix, iy, iz, a.dz); };
     // forward strains at the imaging time (we_op.cpp:510-518)
-    const float t0 = dx1(g, fn[0], ix, iy, iz, a.dx), t1 = dy1(g, fn[1], ix, iy, iz, a.dy), t2 = dz1(g, fn[2], ix, iy, iz, a.dz);
-    const float t3 = dx1(g, fn[2], ix, iy, iz, a.dx), t4 = dz1(g, fn[0], ix, iy, iz, a.dz);
-    const float t5 = dx1(g, fn[1], ix, iy, iz, a.dx), t6 = dy1(g, fn[0], ix, iy, iz, a.dy);
-    const float t7 = dy1(g, fn[2], ix, iy, iz, a.dy), t8 = dz1(g, fn[1], ix, iy, iz, a.dz);
+    const float t0 = DX(fn[0]), t1 = DY(fn[1]), t2 = DZ(fn[2]);
+    const float t3 = DX(fn[2]), t4 = DZ(fn[0]);
+    const float t5 = DX(fn[1]), t6 = DY(fn[0]);
+    const float t7 = DY(fn[2]), t8 = DZ(fn[1]);
     // adjoint strains (of the previous adjoint step)
-    const float ax0 = dx1(g, lag[0], ix, iy, iz, a.dx), ax1 = dx1(g, lag[1], ix, iy, iz, a.dx),
-                ax2 = dx1(g, lag[2], ix, iy, iz, a.dx);
-    const float ay0 = dy1(g, lag[0], ix, iy, iz, a.dy), ay1 = dy1(g, lag[1], ix, iy, iz, a.dy),
-                ay2 = dy1(g, lag[2], ix, iy, iz, a.dy);
-    const float az0 = dz1(g, lag[0], ix, iy, iz, a.dz), az1 = dz1(g, lag[1], ix, iy, iz, a.dz),
-                az2 = dz1(g, lag[2], ix, iy, iz, a.dz);
+    const float ax0 = DX(lag[0]), ax1 = DX(lag[1]), ax2 = DX(lag[2]);
+    const float ay0 = DY(lag[0]), ay1 = DY(lag[1]), ay2 = DY(lag[2]);
+    const float az0 = DZ(lag[0]), az1 = DZ(lag[1]), az2 = DZ(lag[2]);
     const float dt = a.dtimg;
     const bool first = a.itl == 0;
     const bool mid = a.itl > 0 && a.itl < a.last;
