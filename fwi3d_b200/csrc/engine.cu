@@ -57,6 +57,10 @@ DevBuf &DevBuf::operator=(DevBuf &&o) noexcept
 }
 void DevBuf::alloc(size_t n)
 {
+    // same size: keep the buffer (contents are undefined after alloc either
+    // way), which spares the batches of an objective evaluation a cudaFree /
+    // cudaMalloc pair of their multi-GB snapshot stores
+    if (p && bytes == n) return;
     if (p) cudaFree(p);
     p = nullptr;
     bytes = 0;
