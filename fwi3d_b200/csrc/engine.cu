@@ -1631,6 +1631,9 @@ void Engine::image(int itl, const float *curr, const float *prevl)
     a.dx = pb_.dx;
     a.dy = pb_.dy;
     a.dz = pb_.dz;
+    a.rdx = 1.0f / pb_.dx;
+    a.rdy = 1.0f / pb_.dy;
+    a.rdz = 1.0f / pb_.dz;
     a.dtimg = pb_.sub * pb_.dt;
     a.itl = itl;
     a.last = pb_.nt / pb_.sub;

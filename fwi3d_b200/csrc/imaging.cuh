@@ -15,6 +15,7 @@ namespace fwi {
 struct ImageArgs {
     Dims g;
     float dx, dy, dz;
+    float rdx, rdy, rdz;  // 1/dx, 1/dy, 1/dz (interior taps multiply, as the step kernels do)
     float dtimg;  // sub * dt
     int itl;      // snapshot index of this imaging step
     int last;     // nt / sub (integer division)
@@ -30,12 +31,15 @@ FWI_HD float dx1(const Dims &g, const float *p, int ix, int iy, int iz, float d)
 FWI_HD float dy1(const Dims &g, const float *p, int ix, int iy, int iz, float d) { return d1_row(g.ly(p, ix, iz), iy, g.ny) / d; }
 FWI_HD float dz1(const Dims &g, const float *p, int ix, int iy, int iz, float d) { return d1_row(g.lz(p, ix, iy), iz, g.nz) / d; }
 
-// Interior D1 at flat index i along a stride (with the 1/h): the interior
-// branch of d1_row, term for term.
-FWI_HD float d1s(const float *p, int64_t i, int64_t st, float d)
+// Interior D1 at flat index i along a stride, times rd = 1/h: the interior
+// branch of d1_row, term for term, with the reference's division by h
+// replaced by the product with its reciprocal (as in the step kernels; at
+// most one rounding apart, and 18 IEEE divisions per point and shot were a
+// quarter of the adjoint's time).
+FWI_HD float d1s(const float *p, int64_t i, int64_t st, float rd)
 {
     const SbpTables &t = sbp();
-    return (t.d1c0 * (p[i + st] - p[i - st]) + t.d1c1 * (p[i + 2 * st] - p[i - 2 * st])) / d;
+    return (t.d1c0 * (p[i + st] - p[i - st]) + t.d1c1 * (p[i + 2 * st] - p[i - 2 * st])) * rd;
 }
 
 // Increments of the three gradients at one point for the shot whose fields
@@ -51,9 +55,9 @@ FWI_HD void elastic_image_inc(const ImageArgs &a, int64_t so, int ix, int iy, in
     const float *const fn[3] = {a.fwd[1][0] + so, a.fwd[1][1] + so, a.fwd[1][2] + so};
     const float *const lag[3] = {a.lag[0] + so, a.lag[1] + so, a.lag[2] + so};
     const int64_t SX = g.nz, SY = (int64_t)g.nx * g.nz;
-    auto DX = [&](const float *p) { return IN ? d1s(p, i, SX, a.dx) : dx1(g, p, ix, iy, iz, a.dx); };
-    auto DY = [&](const float *p) { return IN ? d1s(p, i, SY, a.dy) : dy1(g, p, ix, iy, iz, a.dy); };
-    auto DZ = [&](const float *p) { return IN ? d1s(p, i, 1, a.dz) : dz1(g, p, ix, iy, iz, a.dz); };
+    auto DX = [&](const float *p) { return IN ? d1s(p, i, SX, a.rdx) : dx1(g, p, ix, iy, iz, a.dx); };
+    auto DY = [&](const float *p) { return IN ? d1s(p, i, SY, a.rdy) : dy1(g, p, ix, iy, iz, a.dy); };
+    auto DZ = [&](const float *p) { return IN ? d1s(p, i, 1, a.rdz) : dz1(g, p, ix, iy, iz, a.dz); };
     // forward strains at the imaging time (we_op.cpp:510-518)
     const float t0 = DX(fn[0]), t1 = DY(fn[1]), t2 = DZ(fn[2]);
     const float t3 = DX(fn[2]), t4 = DZ(fn[0]);
