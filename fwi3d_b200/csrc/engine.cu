@@ -455,10 +455,11 @@ __global__ void k_elastic_face_sat(const __grid_constant__ StepArgs a, int64_t n
 // (acoustic).  Equivalent to the reference's injection into the operator sum
 // before the update (we_op.cpp:691-693): update, scaling and taper are linear in it.
 __global__ void k_inject(StepArgs a, int c, const int64_t *gidx, const int *trace, const float *w, int n,
-                         const float *src, int nt, int it)
+                         const float *src, int nt, int it, const int *itp)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
+    if (itp) it += *itp;  // replayed graphs: step offset + time index on the device
     const int64_t nxyz = a.g.nxyz();
     const int64_t gi = gidx[k];
     const int64_t sh = gi / nxyz;
@@ -500,11 +501,12 @@ __global__ void k_scale0(float *prev, int64_t sst, const float *coef, int64_t n,
 
 // Receivers: rcv[s][c][r][it] = sum_k w_k u_c(g_k) (injector.cpp:118-140).
 __global__ void k_extract(const float *u, int64_t sst, int64_t nxyz, int ncomp, const int64_t *gidx, const float *w,
-                          int nrec, int nr, float *rcv, int nt, int it, int ntap)
+                          int nrec, int nr, float *rcv, int nt, int it, int ntap, const int *itp)
 {
     const int row = blockIdx.x * blockDim.x + threadIdx.x;
     const int c = blockIdx.y;
     if (row >= nrec) return;
+    if (itp) it += *itp;
     const int sh = row / nr, r = row - sh * nr;
     const float *uc = u + sh * sst + c * nxyz;
     const int64_t b = (int64_t)ntap * row;
@@ -525,6 +527,12 @@ __global__ void k_extract(const float *u, int64_t sst, int64_t nxyz, int ncomp, 
     }
     rcv[(((int64_t)sh * ncomp + c) * nr + r) * nt + it] = acc;
 }
+
+// Time index of replayed graphs: set once before the replays, advanced by
+// one thread at the end of each replayed block of three steps (whose kernels
+// add their step's offset 0, 1, 2).
+__global__ void k_set_it(int *itp, int it) { *itp = it; }
+__global__ void k_tick(int *itp, int by) { *itp += by; }
 
 // Imaging of every shot of a batch at once: the increments of the shots
 // (fields at offsets s * sst) are summed in FP64 per point, then added to the
@@ -655,6 +663,9 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     // (default, the faster on B200) or 1 CTA per SM with up to 128 registers.
     const char *mb = std::getenv("FWI_FUSED_MINB");
     fused_minb_ = (mb && mb[0] == '1') ? 1 : 2;
+    // modeling runs replay CUDA graphs of three steps (FWI_GRAPHS=0: plain launches)
+    const char *ge = std::getenv("FWI_GRAPHS");
+    graphs_ = !(ge && ge[0] == '0');
     // isotropic media: interior and edge tiles in two launches (FWI_FUSED_SPLIT=0: one)
     const char *sp = std::getenv("FWI_FUSED_SPLIT");
     fused_split_ = !(sp && sp[0] == '0');
@@ -682,6 +693,7 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
 
 Engine::~Engine()
 {
+    drop_graph();
     if (stream_) {
         cudaStreamSynchronize((cudaStream_t)stream_);
         cudaStreamDestroy((cudaStream_t)stream_);
@@ -1022,7 +1034,7 @@ void Engine::inject(const DevInj &inj, const float *src_dev, int it, float *next
     for (int c = 0; c < nc; c++) {
         if (inj.n[c] == 0) continue;
         k_inject<<<(inj.n[c] + 127) / 128, 128, 0, s>>>(a, c, inj.gidx[c].as<int64_t>(), inj.trace[c].as<int>(),
-                                                         inj.w[c].as<float>(), inj.n[c], src_dev, pb_.nt, it);
+                                                         inj.w[c].as<float>(), inj.n[c], src_dev, pb_.nt, it, itp_);
     }
     CK(cudaGetLastError());
 }
@@ -1035,7 +1047,7 @@ void Engine::extract(const DevExt &ext, const float *curr, float *rcv_dev, int i
     const int64_t n = pb_.nxyz();
     const dim3 grd((ext.nrec + 127) / 128, nc);
     k_extract<<<grd, 128, 0, s>>>(curr, (int64_t)nc * n, n, nc, ext.gidx.as<int64_t>(), ext.w.as<float>(), ext.nrec,
-                                  ext.nr, rcv_dev, pb_.nt, it, ext.ntap);
+                                  ext.nr, rcv_dev, pb_.nt, it, ext.ntap, itp_);
     CK(cudaGetLastError());
 }
 
@@ -1133,15 +1145,101 @@ void Engine::reset()
     fields_.zero(s);
     if (rcv_dev_.p) rcv_dev_.zero(s);
     init_prev(inj_, src_dev_.as<float>(), level(0));
+    // capture the replayed steps here (nothing runs), so that the first run
+    // does not pay for the capture and instantiation
+    if (graphs_ && !ktime_ && pb_.nt > 9 && (!graph_exec_ || graph_key_ != graph_key())) capture_graph();
+}
+
+void Engine::run_step(int it, bool taper_prev)
+{
+    if (!no_extract_) extract(ext_, level(1), rcv_dev_.as<float>(), it);
+    step(level(0), level(1), level(2), taper_prev);
+    inject(inj_, src_dev_.as<float>(), it, level(2));
+    rot_ = (rot_ + 1) % 3;
+}
+
+// Everything a captured step sequence bakes in: buffers, tables, options.
+uint64_t Engine::graph_key() const
+{
+    const void *ptrs[] = {fields_.p, model_.p, src_dev_.p, rcv_dev_.p, inj_.gidx[0].p, inj_.gidx[1].p, inj_.gidx[2].p,
+                          inj_.trace[0].p, inj_.w[0].p, ext_.gidx.p, ext_.w.p, sdiv_.p, taper_.p};
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](uint64_t v) { h = (h ^ v) * 1099511628211ull; };
+    for (const void *p : ptrs) mix((uint64_t)(uintptr_t)p);
+    for (int c = 0; c < 3; c++) mix((uint64_t)inj_.n[c]);
+    mix((uint64_t)ext_.nrec);
+    mix((uint64_t)no_extract_);
+    mix((uint64_t)pb_.nt);
+    return h;
+}
+
+void Engine::drop_graph()
+{
+    if (graph_exec_) cudaGraphExecDestroy((cudaGraphExec_t)graph_exec_);
+    graph_exec_ = nullptr;
+}
+
+// Capture three steps (the rotation period of the time levels) starting at
+// rotation 0 with the time index read from the device; false if the capture
+// fails (the steps then run as plain launches).
+bool Engine::capture_graph()
+{
+    drop_graph();
+    cudaStream_t s = (cudaStream_t)stream_;
+    if (!it_dev_.p) it_dev_.alloc(sizeof(int));
+    itp_ = it_dev_.as<int>();
+    cudaGraph_t g = nullptr;
+    bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+        try {
+            // kernels read the time index as k + *itp; it > 0 (taper of prev) as every step after the first
+            for (int k = 0; k < 3; k++) run_step(k, true);
+            k_tick<<<1, 1, 0, s>>>(itp_, 3);
+        } catch (const FwiError &) {
+            ok = false;
+        }
+        ok = cudaStreamEndCapture(s, &g) == cudaSuccess && ok;
+    }
+    cudaGraphExec_t ex = nullptr;
+    ok = ok && g && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
+    if (g) cudaGraphDestroy(g);
+    itp_ = nullptr;
+    cudaGetLastError();
+    if (!ok) {
+        graphs_ = false;
+        return false;
+    }
+    graph_exec_ = ex;
+    graph_key_ = graph_key();
+    return true;
 }
 
 void Engine::run(int it0, int nsteps)
 {
-    for (int it = it0; it < it0 + nsteps && it < pb_.nt - 1; it++) {
-        if (!no_extract_) extract(ext_, level(1), rcv_dev_.as<float>(), it);
-        step(level(0), level(1), level(2), it > 0);
-        inject(inj_, src_dev_.as<float>(), it, level(2));
-        rot_ = (rot_ + 1) % 3;
+    const int end = std::min(it0 + nsteps, pb_.nt - 1);
+    int it = it0;
+    // CUDA graph replay in rotation-aligned blocks of three steps when the
+    // run is long enough; step kernels take their per-step arguments from the
+    // rotation and the device time index (the main-kernel timing keeps plain
+    // launches, its events are per launch)
+    const bool graph = graphs_ && !ktime_;
+    while (it < end && graph && (rot_ != 0 || it == 0)) {
+        run_step(it, it > 0);
+        it++;
+    }
+    const int reps = graph ? (end - it) / 3 : 0;
+    if (reps >= 1) {
+        if (!graph_exec_ || graph_key_ != graph_key()) capture_graph();
+        if (graph_exec_) {
+            cudaStream_t s = (cudaStream_t)stream_;
+            k_set_it<<<1, 1, 0, s>>>(it_dev_.as<int>(), it);
+            for (int r = 0; r < reps; r++) CK(cudaGraphLaunch((cudaGraphExec_t)graph_exec_, s));
+            it += 3 * reps;
+        }
+    }
+    while (it < end) {
+        run_step(it, it > 0);
+        it++;
     }
 }
 

@@ -204,6 +204,15 @@ private:
     bool slab_march_ = false;      // fused path: y-wall slabs by the marching kernel (else per-point kernels)
     bool fused_ = false;           // fused elastic kernel for the interior planes
     int fused_minb_ = 2;           // resident CTAs per SM the fused kernel is compiled for
+    bool graphs_ = true;           // modeling runs replay captured three-step graphs
+    void *graph_exec_ = nullptr;   // cudaGraphExec_t of the captured steps
+    uint64_t graph_key_ = 0;       // graph_key() at capture
+    DevBuf it_dev_;                // device time index of replayed steps
+    int *itp_ = nullptr;           // non-null while capturing: kernels read the time index there
+    void run_step(int it, bool taper_prev);
+    uint64_t graph_key() const;
+    bool capture_graph();
+    void drop_graph();
     bool fused_split_ = true;      // interior and edge tiles of the fused kernel in separate launches
     bool fused_split_active() const;
     bool tma_ = false;             // fused kernel copies planes with bulk-tensor copies
