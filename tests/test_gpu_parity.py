@@ -261,3 +261,41 @@ def test_acoustic_fused_traces(oracle_fp32, bc, monkeypatch):
 def test_acoustic_fused_gradient(oracle_fp32, monkeypatch):
     monkeypatch.setenv("FWI_FUSED", "1")
     _grad_case(oracle_fp32, synth.acoustic_linear(n=40, nsteps=120, taper=5, rec_stride=3), 1)
+
+
+def test_graph_replay_matches_plain_launches(monkeypatch):
+    """Modeling runs replayed as three-step CUDA graphs (default) give the
+    traces of plain launches (FWI_GRAPHS=0) bit for bit, for a batch run in
+    uneven chunks (the serving loop's pattern) and for a whole-axis run."""
+    from fwi3d_b200 import _lib
+    import ctypes as C
+
+    sv = _elastic_fused()
+    out = {}
+    for g in ("1", "0"):
+        monkeypatch.setenv("FWI_GRAPHS", g)
+        out["op" + g] = ops.from_survey(sv).forward(False, sv.model)
+        lib = _lib.load()
+        dom = ops.Domain(sv.nx, sv.ny, sv.nz, sv.dx, sv.dy, sv.dz, sv.nmodels)
+        w = np.ascontiguousarray(sv.wavelet, dtype=np.float32)
+        sx = np.ascontiguousarray(np.asarray(sv.par.sxyz, dtype=np.float32))
+        rx = np.ascontiguousarray(np.asarray(sv.par.rxyz, dtype=np.float32))
+        h = C.c_void_p()
+        _lib.check(lib.fwi_batch_create(C.byref(h), 0, C.byref(dom.grid()), sv.nmodels,
+                                        C.byref(ops.to_cparam(sv.par)),
+                                        _lib.fptr(np.ascontiguousarray(sv.model, dtype=np.float32)), _lib.fptr(w),
+                                        1, w.shape[-1], sv.dt_data, 1, _lib.fptr(sx), rx.shape[1], _lib.fptr(rx)))
+        info = _lib.OpInfo()
+        _lib.check(lib.fwi_batch_get_info(h, C.byref(info), None))
+        _lib.check(lib.fwi_batch_reset(h))
+        left = info.nt - 1
+        for k in (1, 7, 20, 2, 50):
+            _lib.check(lib.fwi_batch_run(h, min(k, left)))
+            left -= min(k, left)
+        _lib.check(lib.fwi_batch_run(h, left))
+        tr = np.zeros((1, info.nrcomp, rx.shape[1], w.shape[-1]), dtype=np.float32)
+        _lib.check(lib.fwi_batch_traces(h, _lib.fptr(tr)))
+        lib.fwi_batch_destroy(h)
+        out["b" + g] = tr
+    assert np.array_equal(out["op1"], out["op0"])
+    assert np.array_equal(out["b1"], out["b0"])
