@@ -528,6 +528,35 @@ __global__ void k_extract(const float *u, int64_t sst, int64_t nxyz, int ncomp, 
     rcv[(((int64_t)sh * ncomp + c) * nr + r) * nt + it] = acc;
 }
 
+// D2var closure weights of mu for the 12 closure rows of every line along one
+// axis (StepArgs::w2c): the fused and marching kernels' d2closure_weights,
+// evaluated once per model instead of at every time step.
+__global__ void k_w2c(const float *mu, Dims g, int axis, float *out, int64_t nlines)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nlines * 12) return;
+    const int64_t line = e / 12;
+    const int slot = (int)(e - line * 12);
+    Line l;
+    int n;
+    if (axis == 0) {
+        const int64_t y = line / g.nz, z = line - y * g.nz;
+        l = Line{mu, y * g.nx * g.nz + z, g.nz};
+        n = g.nx;
+    } else if (axis == 1) {
+        const int64_t x = line / g.nz, z = line - x * g.nz;
+        l = Line{mu, x * g.nz + z, (int64_t)g.nx * g.nz};
+        n = g.ny;
+    } else {
+        const int64_t y = line / g.nx, x = line - y * g.nx;
+        l = Line{mu, (y * g.nx + x) * g.nz, 1};
+        n = g.nz;
+    }
+    const int i = slot < 6 ? slot : n - 1 - (slot - 6);
+    const W8 w = d2closure_weights(l, i, n, ConstRows());
+    for (int j = 0; j < 8; j++) out[e * 8 + j] = w.w[j];
+}
+
 // Time index of replayed graphs: set once before the replays, advanced by
 // one thread at the end of each replayed block of three steps (whose kernels
 // add their step's offset 0, 1, 2).
@@ -716,7 +745,7 @@ void Engine::sync()
 
 int64_t Engine::device_bytes() const
 {
-    return model_.bytes + fields_.bytes + aux_.bytes + snaps_.bytes + grad_.bytes + sdiv_.bytes + taper_.bytes +
+    return model_.bytes + w2c_.bytes + fields_.bytes + aux_.bytes + snaps_.bytes + grad_.bytes + sdiv_.bytes + taper_.bytes +
            src_dev_.bytes + rcv_dev_.bytes + snapq_.bytes + snaps_scale_.bytes + enc_.bytes + amax_.bytes +
            snapz_.bytes + ckpt_.bytes + rec_fields_.bytes;
 }
@@ -733,6 +762,24 @@ void Engine::set_model(const float *conv)
     const int64_t n = pb_.nxyz();
     model_.alloc(sizeof(float) * pb_.nmodels * n);
     CK(cudaMemcpyAsync(model_.p, conv, model_.bytes, cudaMemcpyHostToDevice, (cudaStream_t)stream_));
+    // isotropic media: closure weights of mu along x, y, z (FWI_W2C=0: formed in the step kernels)
+    const char *we = std::getenv("FWI_W2C");
+    if (pb_.nmodels == 3 && (fused_ || march_) && !(we && we[0] == '0')) {
+        const int64_t nl[3] = {(int64_t)pb_.ny * pb_.nz, (int64_t)pb_.nx * pb_.nz, (int64_t)pb_.ny * pb_.nx};
+        w2c_.alloc(sizeof(float) * 12 * 8 * (nl[0] + nl[1] + nl[2]));
+        float *o = w2c_.as<float>();
+        const Dims g{pb_.nx, pb_.ny, pb_.nz};
+        for (int ax = 0; ax < 3; ax++) {
+            w2c_ptr_[ax] = o;
+            k_w2c<<<(unsigned)((nl[ax] * 12 + 255) / 256), 256, 0, (cudaStream_t)stream_>>>(
+                model_.as<float>() + n, g, ax, o, nl[ax]);
+            o += 12 * 8 * nl[ax];
+        }
+        CK(cudaGetLastError());
+    } else {
+        w2c_.alloc(0);
+        for (int ax = 0; ax < 3; ax++) w2c_ptr_[ax] = nullptr;
+    }
 
     ScaleTables st = boundary_divisors(conv, pb_.nmodels, pb_.nx, pb_.ny, pb_.nz, pb_.dx, pb_.dy, pb_.dz, pb_.dt, pb_.bc);
     scale_ = 0;
@@ -856,6 +903,7 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         a.prev[c] = prev + c * n;
         a.next[c] = next + c * n;
     }
+    for (int ax = 0; ax < 3; ax++) a.w2c[ax] = w2c_ptr_[ax];
     a.taper_prev = taper_prev ? 1 : 0;
     const dim3 blk(BZ, BX, BY);
     // per-point launch over planes [y0, y1)
@@ -1162,7 +1210,7 @@ void Engine::run_step(int it, bool taper_prev)
 uint64_t Engine::graph_key() const
 {
     const void *ptrs[] = {fields_.p, model_.p, src_dev_.p, rcv_dev_.p, inj_.gidx[0].p, inj_.gidx[1].p, inj_.gidx[2].p,
-                          inj_.trace[0].p, inj_.w[0].p, ext_.gidx.p, ext_.w.p, sdiv_.p, taper_.p};
+                          inj_.trace[0].p, inj_.w[0].p, ext_.gidx.p, ext_.w.p, sdiv_.p, taper_.p, w2c_.p};
     uint64_t h = 1469598103934665603ull;
     auto mix = [&](uint64_t v) { h = (h ^ v) * 1099511628211ull; };
     for (const void *p : ptrs) mix((uint64_t)(uintptr_t)p);

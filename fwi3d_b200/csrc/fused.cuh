@@ -409,6 +409,25 @@ FWI_HD W8 d2closure_weights(const F &f, int i, int n, const R &b)
     }
     return w;
 }
+// Closure weights of row i (of n) on line `line` of a precomputed table
+// (12 rows x 8 weights per line, the low rows first, then the high rows from
+// the face inwards), or formed from the material line when there is none.
+template <class F, class R>
+FWI_HD W8 d2closure_w(const float *tab, int64_t line, const F &f, int i, int n, const R &b)
+{
+    if (!tab) return d2closure_weights(f, i, n, b);
+    const int slot = i < 6 ? i : 6 + (n - 1 - i);
+    const float *p = tab + (line * 12 + slot) * 8;
+    W8 w;
+#if defined(__CUDA_ARCH__)
+    const float4 lo = *reinterpret_cast<const float4 *>(p), hi = *reinterpret_cast<const float4 *>(p + 4);
+    w.w[0] = lo.x; w.w[1] = lo.y; w.w[2] = lo.z; w.w[3] = lo.w;
+    w.w[4] = hi.x; w.w[5] = hi.y; w.w[6] = hi.z; w.w[7] = hi.w;
+#else
+    for (int j = 0; j < 8; j++) w.w[j] = p[j];
+#endif
+    return w;
+}
 template <class U>
 FWI_HD float d2closure_apply(const W8 &w, const U &u, int i, int n, float ad2)
 {
@@ -458,9 +477,9 @@ FWI_HD void fz_output(FusedCtx &c, const FusedThread &th, int tid, int y)
         W5 wx{}, wz{};
         W8 wxc{}, wzc{};
         if (xin) wx = d2w(mux(ix - 2), mux(ix - 1), mux(ix), mux(ix + 1), mux(ix + 2));
-        else wxc = d2closure_weights(mux, ix, g.nx, c.rows);
+        else wxc = d2closure_w(a.w2c[0], (int64_t)y * g.nz + iz, mux, ix, g.nx, c.rows);
         if (zin) wz = d2w(muz(iz - 2), muz(iz - 1), muz(iz), muz(iz + 1), muz(iz + 2));
-        else wzc = d2closure_weights(muz, iz, g.nz, c.rows);
+        else wzc = d2closure_w(a.w2c[2], (int64_t)y * g.nx + ix, muz, iz, g.nz, c.rows);
         const W5 wy = d2w(th.qmu[0], th.qmu[1], th.qmu[2], th.qmu[3], th.qmu[4]);
         for (int k = 0; k < 3; k++) {
             const float adx = k == 0 ? a.ad2[0] : a.ad1[0];
@@ -575,9 +594,9 @@ FWI_HD void fz_output_t(FusedCtx &c, const FusedThread &th, int tid, int y)
         W5 wx{}, wz{};
         W8 wxc{}, wzc{};
         if (xin) wx = d2w(mu[-2 * DX], mu[-DX], mu[0], mu[DX], mu[2 * DX]);
-        else wxc = d2closure_weights(mux, ix, g.nx, c.rows);
+        else wxc = d2closure_w(a.w2c[0], (int64_t)y * g.nz + iz, mux, ix, g.nx, c.rows);
         if (zin) wz = d2w(mu[-2], mu[-1], mu[0], mu[1], mu[2]);
-        else wzc = d2closure_weights(muz, iz, g.nz, c.rows);
+        else wzc = d2closure_w(a.w2c[2], (int64_t)y * g.nx + ix, muz, iz, g.nz, c.rows);
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             const float adx = k == 0 ? a.ad2[0] : a.ad1[0];

@@ -282,11 +282,11 @@ FWI_HD void m3_output(const MarchCtx &c, int tid, int y)
         W5 wx{}, wz{}, wy{};
         W8 wxc{}, wzc{}, wyc{};
         if (xin) wx = d2w(mux(ix - 2), mux(ix - 1), mux(ix), mux(ix + 1), mux(ix + 2));
-        else wxc = d2closure_weights(mux, ix, g.nx, c.rows);
+        else wxc = d2closure_w(a.w2c[0], (int64_t)y * g.nz + iz, mux, ix, g.nx, c.rows);
         if (zin) wz = d2w(muz(iz - 2), muz(iz - 1), muz(iz), muz(iz + 1), muz(iz + 2));
-        else wzc = d2closure_weights(muz, iz, g.nz, c.rows);
+        else wzc = d2closure_w(a.w2c[2], (int64_t)y * g.nx + ix, muz, iz, g.nz, c.rows);
         if (yin) wy = d2w(ydv(YD_MU, 0), ydv(YD_MU, 1), ydv(YD_MU, 2), ydv(YD_MU, 3), ydv(YD_MU, 4));
-        else wyc = d2closure_weights(Line{a.m[1], col, ystr}, y, g.ny, c.rows);
+        else wyc = d2closure_w(a.w2c[1], (int64_t)ix * g.nz + iz, Line{a.m[1], col, ystr}, y, g.ny, c.rows);
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             const float adx = k == 0 ? a.ad2[0] : a.ad1[0];

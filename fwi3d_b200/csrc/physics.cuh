@@ -55,6 +55,10 @@ struct StepArgs {
     int y0, y1;                // planes [y0, y1) covered by the launch
     int64_t sst;               // wavefield shot stride (floats)
     int64_t ast;               // derivative-scratch shot stride (floats)
+    // isotropic media: D2var closure weights of mu, precomputed per model for
+    // the 12 closure rows of every line along x, y, z (null: formed in place);
+    // line index y*nz + z (x lines), x*nz + z (y lines), y*nx + x (z lines)
+    const float *w2c[3];
 };
 
 // Pointers of shot s.
