@@ -531,27 +531,45 @@ __global__ void k_extract(const float *u, int64_t sst, int64_t nxyz, int ncomp, 
 // D2var closure weights of mu for the 12 closure rows of every line along one
 // axis (StepArgs::w2c): the fused and marching kernels' d2closure_weights,
 // evaluated once per model instead of at every time step.
-__global__ void k_w2c(const float *mu, Dims g, int axis, float *out, int64_t nlines)
+// Coefficient f of the closure weights along a line: 0 mu, 1 c66, 2 c11b.
+struct W2cCoef {
+    Line mu, eps, c66;
+    int f;
+    FWI_HD float operator()(int k) const
+    {
+        if (f == 0) return mu(k);
+        if (f == 1) return c66(k);
+        return 2.f * (1.f + 2.f * eps(k)) * mu(k);  // as C11bS / C11bLine
+    }
+};
+
+__global__ void k_w2c(StepArgs a, int axis, int f, float *out, int64_t nlines)
 {
+    const Dims &g = a.g;
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= nlines * 12) return;
     const int64_t line = e / 12;
     const int slot = (int)(e - line * 12);
-    Line l;
+    int64_t base, stride;
     int n;
     if (axis == 0) {
         const int64_t y = line / g.nz, z = line - y * g.nz;
-        l = Line{mu, y * g.nx * g.nz + z, g.nz};
+        base = y * g.nx * g.nz + z;
+        stride = g.nz;
         n = g.nx;
     } else if (axis == 1) {
         const int64_t x = line / g.nz, z = line - x * g.nz;
-        l = Line{mu, x * g.nz + z, (int64_t)g.nx * g.nz};
+        base = x * g.nz + z;
+        stride = (int64_t)g.nx * g.nz;
         n = g.ny;
     } else {
         const int64_t y = line / g.nx, x = line - y * g.nx;
-        l = Line{mu, (y * g.nx + x) * g.nz, 1};
+        base = (y * g.nx + x) * g.nz;
+        stride = 1;
         n = g.nz;
     }
+    const W2cCoef l{Line{a.m[1], base, stride}, Line{f == 2 ? a.m[4] : a.m[1], base, stride},
+                    Line{f == 1 ? a.m[5] : a.m[1], base, stride}, f};
     const int i = slot < 6 ? slot : n - 1 - (slot - 6);
     const W8 w = d2closure_weights(l, i, n, ConstRows());
     for (int j = 0; j < 8; j++) out[e * 8 + j] = w.w[j];
@@ -762,23 +780,32 @@ void Engine::set_model(const float *conv)
     const int64_t n = pb_.nxyz();
     model_.alloc(sizeof(float) * pb_.nmodels * n);
     CK(cudaMemcpyAsync(model_.p, conv, model_.bytes, cudaMemcpyHostToDevice, (cudaStream_t)stream_));
-    // isotropic media: closure weights of mu along x, y, z (FWI_W2C=0: formed in the step kernels)
+    // closure weights of the D2var coefficients along x, y, z, once per model
+    // (FWI_W2C=0: formed in the step kernels): mu on every axis, and for VTI
+    // also c66 and c11b along x and y
     const char *we = std::getenv("FWI_W2C");
-    if (pb_.nmodels == 3 && (fused_ || march_) && !(we && we[0] == '0')) {
+    for (int ax = 0; ax < 3; ax++)
+        for (int f = 0; f < 3; f++) w2c_ptr_[ax][f] = nullptr;
+    if (pb_.nmodels != 2 && (fused_ || march_) && !(we && we[0] == '0')) {
         const int64_t nl[3] = {(int64_t)pb_.ny * pb_.nz, (int64_t)pb_.nx * pb_.nz, (int64_t)pb_.ny * pb_.nx};
-        w2c_.alloc(sizeof(float) * 12 * 8 * (nl[0] + nl[1] + nl[2]));
+        const int nf[3] = {pb_.nmodels == 6 ? 3 : 1, pb_.nmodels == 6 ? 3 : 1, 1};
+        int64_t tot = 0;
+        for (int ax = 0; ax < 3; ax++) tot += nf[ax] * nl[ax];
+        w2c_.alloc(sizeof(float) * 12 * 8 * tot);
         float *o = w2c_.as<float>();
-        const Dims g{pb_.nx, pb_.ny, pb_.nz};
-        for (int ax = 0; ax < 3; ax++) {
-            w2c_ptr_[ax] = o;
-            k_w2c<<<(unsigned)((nl[ax] * 12 + 255) / 256), 256, 0, (cudaStream_t)stream_>>>(
-                model_.as<float>() + n, g, ax, o, nl[ax]);
-            o += 12 * 8 * nl[ax];
-        }
+        StepArgs ma;
+        std::memset(&ma, 0, sizeof(ma));
+        ma.g = Dims{pb_.nx, pb_.ny, pb_.nz};
+        for (int k = 0; k < pb_.nmodels; k++) ma.m[k] = model_.as<float>() + k * n;
+        for (int ax = 0; ax < 3; ax++)
+            for (int f = 0; f < nf[ax]; f++) {
+                w2c_ptr_[ax][f] = o;
+                k_w2c<<<(unsigned)((nl[ax] * 12 + 255) / 256), 256, 0, (cudaStream_t)stream_>>>(ma, ax, f, o, nl[ax]);
+                o += 12 * 8 * nl[ax];
+            }
         CK(cudaGetLastError());
     } else {
         w2c_.alloc(0);
-        for (int ax = 0; ax < 3; ax++) w2c_ptr_[ax] = nullptr;
     }
 
     ScaleTables st = boundary_divisors(conv, pb_.nmodels, pb_.nx, pb_.ny, pb_.nz, pb_.dx, pb_.dy, pb_.dz, pb_.dt, pb_.bc);
@@ -903,7 +930,8 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         a.prev[c] = prev + c * n;
         a.next[c] = next + c * n;
     }
-    for (int ax = 0; ax < 3; ax++) a.w2c[ax] = w2c_ptr_[ax];
+    for (int ax = 0; ax < 3; ax++)
+        for (int f = 0; f < 3; f++) a.w2c[ax][f] = w2c_ptr_[ax][f];
     a.taper_prev = taper_prev ? 1 : 0;
     const dim3 blk(BZ, BX, BY);
     // per-point launch over planes [y0, y1)

@@ -167,8 +167,8 @@ private:
     Problem pb_;
     void *stream_ = nullptr;
     DevBuf model_;                 // [nm][nxyz]
-    DevBuf w2c_;                   // isotropic: closure weights of mu, x / y / z lines (StepArgs::w2c)
-    const float *w2c_ptr_[3] = {nullptr, nullptr, nullptr};
+    DevBuf w2c_;                   // closure weights of the D2var coefficients per axis (StepArgs::w2c)
+    const float *w2c_ptr_[3][3] = {};
     DevBuf fields_;                // [3 levels][nshots][ncomp][nxyz]
     int rot_ = 0;                  // rotation of the three time levels
     DevBuf aux_;                   // elastic derivative scratch [nshots][naux][nxyz] (per-point path)

@@ -436,6 +436,13 @@ FWI_HD float d2closure_apply(const W8 &w, const U &u, int i, int n, float ad2)
     for (int j = 0; j < 8; j++) acc += ad2 * w.w[j] * u(hi ? n - 1 - j : j);
     return acc;
 }
+// d2var_row with the closure weights of a precomputed table (when present).
+template <class U, class F, class R>
+FWI_HD float d2var_tab(const float *tab, int64_t line, const U &u, const F &f, int i, int n, float ad2, const R &b)
+{
+    if (tab && (i < 6 || i >= n - 6)) return d2closure_apply(d2closure_w(tab, line, f, i, n, b), u, i, n, ad2);
+    return d2var_row(u, f, i, n, ad2, b);
+}
 
 // Smem accessors of the output phase.
 FWI_HD SX ux_line(const FusedCtx &c, int slot, int k, int izw) { return SX{&c.sm->u[slot][k][0][izw], c.x0 - fz::HW, fz::ZW}; }
@@ -477,9 +484,9 @@ FWI_HD void fz_output(FusedCtx &c, const FusedThread &th, int tid, int y)
         W5 wx{}, wz{};
         W8 wxc{}, wzc{};
         if (xin) wx = d2w(mux(ix - 2), mux(ix - 1), mux(ix), mux(ix + 1), mux(ix + 2));
-        else wxc = d2closure_w(a.w2c[0], (int64_t)y * g.nz + iz, mux, ix, g.nx, c.rows);
+        else wxc = d2closure_w(a.w2c[0][0], (int64_t)y * g.nz + iz, mux, ix, g.nx, c.rows);
         if (zin) wz = d2w(muz(iz - 2), muz(iz - 1), muz(iz), muz(iz + 1), muz(iz + 2));
-        else wzc = d2closure_w(a.w2c[2], (int64_t)y * g.nx + ix, muz, iz, g.nz, c.rows);
+        else wzc = d2closure_w(a.w2c[2][0], (int64_t)y * g.nx + ix, muz, iz, g.nz, c.rows);
         const W5 wy = d2w(th.qmu[0], th.qmu[1], th.qmu[2], th.qmu[3], th.qmu[4]);
         for (int k = 0; k < 3; k++) {
             const float adx = k == 0 ? a.ad2[0] : a.ad1[0];
@@ -519,13 +526,13 @@ FWI_HD void fz_output(FusedCtx &c, const FusedThread &th, int tid, int y)
             const SZ uzl = uz_line(c, r0, k, ixw);
             float v;
             if (xin) v = d2apply(wx, idx2, ul(ix - 2), ul(ix - 1), ul(ix), ul(ix + 1), ul(ix + 2));
-            else if (k == 0) v = d2var_row(ul, bx, ix, g.nx, idx2, c.rows);
-            else if (k == 1) v = d2var_row(ul, c6x, ix, g.nx, idx2, c.rows);
-            else v = d2var_row(ul, mux, ix, g.nx, idx2, c.rows);
+            else if (k == 0) v = d2var_tab(a.w2c[0][2], (int64_t)y * g.nz + iz, ul, bx, ix, g.nx, idx2, c.rows);
+            else if (k == 1) v = d2var_tab(a.w2c[0][1], (int64_t)y * g.nz + iz, ul, c6x, ix, g.nx, idx2, c.rows);
+            else v = d2var_tab(a.w2c[0][0], (int64_t)y * g.nz + iz, ul, mux, ix, g.nx, idx2, c.rows);
             v += d2apply(wy, idy2, s.u[rm2][k][ixw][izw], s.u[rm1][k][ixw][izw], s.u[r0][k][ixw][izw],
                          s.u[rp1][k][ixw][izw], s.u[rp2][k][ixw][izw]);
             v += zin ? d2apply(wz, adz, uzl(iz - 2), uzl(iz - 1), uzl(iz), uzl(iz + 1), uzl(iz + 2))
-                     : d2var_row(uzl, muz, iz, g.nz, adz, c.rows);
+                     : d2var_tab(a.w2c[2][0], (int64_t)y * g.nx + ix, uzl, muz, iz, g.nz, adz, c.rows);
             acc[k] = v;
         }
     }
@@ -594,9 +601,9 @@ FWI_HD void fz_output_t(FusedCtx &c, const FusedThread &th, int tid, int y)
         W5 wx{}, wz{};
         W8 wxc{}, wzc{};
         if (xin) wx = d2w(mu[-2 * DX], mu[-DX], mu[0], mu[DX], mu[2 * DX]);
-        else wxc = d2closure_w(a.w2c[0], (int64_t)y * g.nz + iz, mux, ix, g.nx, c.rows);
+        else wxc = d2closure_w(a.w2c[0][0], (int64_t)y * g.nz + iz, mux, ix, g.nx, c.rows);
         if (zin) wz = d2w(mu[-2], mu[-1], mu[0], mu[1], mu[2]);
-        else wzc = d2closure_w(a.w2c[2], (int64_t)y * g.nx + ix, muz, iz, g.nz, c.rows);
+        else wzc = d2closure_w(a.w2c[2][0], (int64_t)y * g.nx + ix, muz, iz, g.nz, c.rows);
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             const float adx = k == 0 ? a.ad2[0] : a.ad1[0];
@@ -640,12 +647,15 @@ FWI_HD void fz_output_t(FusedCtx &c, const FusedThread &th, int tid, int y)
                 v = d2apply(wx, idx2, u[-2 * UX], u[-UX], u[0], u[UX], u[2 * UX]);
             } else {
                 const SX ul = ux_line(c, c.sl[2], k, izw);
-                v = k == 0 ? d2var_row(ul, bx, ix, g.nx, idx2, c.rows)
-                           : (k == 1 ? d2var_row(ul, c6x, ix, g.nx, idx2, c.rows) : d2var_row(ul, mux, ix, g.nx, idx2, c.rows));
+                const int64_t xl = (int64_t)y * g.nz + iz;
+                v = k == 0 ? d2var_tab(a.w2c[0][2], xl, ul, bx, ix, g.nx, idx2, c.rows)
+                           : (k == 1 ? d2var_tab(a.w2c[0][1], xl, ul, c6x, ix, g.nx, idx2, c.rows)
+                                     : d2var_tab(a.w2c[0][0], xl, ul, mux, ix, g.nx, idx2, c.rows));
             }
             v += d2apply(wy, idy2, uc[rm2], uc[rm1], u[0], uc[rp1], uc[rp2]);
             v += zin ? d2apply(wz, adz, u[-2], u[-1], u[0], u[1], u[2])
-                     : d2var_row(uz_line(c, c.sl[2], k, ixw), muz, iz, g.nz, adz, c.rows);
+                     : d2var_tab(a.w2c[2][0], (int64_t)y * g.nx + ix, uz_line(c, c.sl[2], k, ixw), muz, iz, g.nz, adz,
+                                 c.rows);
             acc[k] = v;
         }
     }

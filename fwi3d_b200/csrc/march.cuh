@@ -282,11 +282,11 @@ FWI_HD void m3_output(const MarchCtx &c, int tid, int y)
         W5 wx{}, wz{}, wy{};
         W8 wxc{}, wzc{}, wyc{};
         if (xin) wx = d2w(mux(ix - 2), mux(ix - 1), mux(ix), mux(ix + 1), mux(ix + 2));
-        else wxc = d2closure_w(a.w2c[0], (int64_t)y * g.nz + iz, mux, ix, g.nx, c.rows);
+        else wxc = d2closure_w(a.w2c[0][0], (int64_t)y * g.nz + iz, mux, ix, g.nx, c.rows);
         if (zin) wz = d2w(muz(iz - 2), muz(iz - 1), muz(iz), muz(iz + 1), muz(iz + 2));
-        else wzc = d2closure_w(a.w2c[2], (int64_t)y * g.nx + ix, muz, iz, g.nz, c.rows);
+        else wzc = d2closure_w(a.w2c[2][0], (int64_t)y * g.nx + ix, muz, iz, g.nz, c.rows);
         if (yin) wy = d2w(ydv(YD_MU, 0), ydv(YD_MU, 1), ydv(YD_MU, 2), ydv(YD_MU, 3), ydv(YD_MU, 4));
-        else wyc = d2closure_w(a.w2c[1], (int64_t)ix * g.nz + iz, Line{a.m[1], col, ystr}, y, g.ny, c.rows);
+        else wyc = d2closure_w(a.w2c[1][0], (int64_t)ix * g.nz + iz, Line{a.m[1], col, ystr}, y, g.ny, c.rows);
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             const float adx = k == 0 ? a.ad2[0] : a.ad1[0];
@@ -330,19 +330,19 @@ FWI_HD void m3_output(const MarchCtx &c, int tid, int y)
             const SZ uzl{&s.u[s0][k][xu][0], c.z0 - f3::HU};
             float v;
             if (xin) v = d2apply(wx, idx2, ul(ix - 2), ul(ix - 1), ul(ix), ul(ix + 1), ul(ix + 2));
-            else if (k == 0) v = d2var_row(ul, bx, ix, g.nx, idx2, c.rows);
-            else if (k == 1) v = d2var_row(ul, c6x, ix, g.nx, idx2, c.rows);
-            else v = d2var_row(ul, mux, ix, g.nx, idx2, c.rows);
+            else if (k == 0) v = d2var_tab(a.w2c[0][2], (int64_t)y * g.nz + iz, ul, bx, ix, g.nx, idx2, c.rows);
+            else if (k == 1) v = d2var_tab(a.w2c[0][1], (int64_t)y * g.nz + iz, ul, c6x, ix, g.nx, idx2, c.rows);
+            else v = d2var_tab(a.w2c[0][0], (int64_t)y * g.nz + iz, ul, mux, ix, g.nx, idx2, c.rows);
             if (yin) {
                 v += d2apply(wy, idy2, uy(k, y - 2), uy(k, y - 1), uy(k, y), uy(k, y + 1), uy(k, y + 2));
             } else {
                 const Line ucol{a.curr[k] + c.so, col, ystr};
-                if (k == 0) v += d2var_row(ucol, c6y, y, g.ny, idy2, c.rows);
-                else if (k == 1) v += d2var_row(ucol, C11bLine{epsy, muy}, y, g.ny, idy2, c.rows);
-                else v += d2var_row(ucol, muy, y, g.ny, idy2, c.rows);
+                if (k == 0) v += d2var_tab(a.w2c[1][1], (int64_t)ix * g.nz + iz, ucol, c6y, y, g.ny, idy2, c.rows);
+                else if (k == 1) v += d2var_tab(a.w2c[1][2], (int64_t)ix * g.nz + iz, ucol, C11bLine{epsy, muy}, y, g.ny, idy2, c.rows);
+                else v += d2var_tab(a.w2c[1][0], (int64_t)ix * g.nz + iz, ucol, muy, y, g.ny, idy2, c.rows);
             }
             v += zin ? d2apply(wz, adz, uzl(iz - 2), uzl(iz - 1), uzl(iz), uzl(iz + 1), uzl(iz + 2))
-                     : d2var_row(uzl, muz, iz, g.nz, adz, c.rows);
+                     : d2var_tab(a.w2c[2][0], (int64_t)y * g.nx + ix, uzl, muz, iz, g.nz, adz, c.rows);
             acc[k] = v;
         }
     }

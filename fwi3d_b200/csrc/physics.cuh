@@ -55,10 +55,11 @@ struct StepArgs {
     int y0, y1;                // planes [y0, y1) covered by the launch
     int64_t sst;               // wavefield shot stride (floats)
     int64_t ast;               // derivative-scratch shot stride (floats)
-    // isotropic media: D2var closure weights of mu, precomputed per model for
-    // the 12 closure rows of every line along x, y, z (null: formed in place);
-    // line index y*nz + z (x lines), x*nz + z (y lines), y*nx + x (z lines)
-    const float *w2c[3];
+    // D2var closure weights precomputed per model for the 12 closure rows of
+    // every line along x, y, z (w2c[axis][f], null: formed in place), of the
+    // coefficient f = 0 mu, 1 c66, 2 c11b = 2 (1 + 2 eps) mu (VTI); line index
+    // y*nz + z (x lines), x*nz + z (y lines), y*nx + x (z lines)
+    const float *w2c[3][3];
 };
 
 // Pointers of shot s.
