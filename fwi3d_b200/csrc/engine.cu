@@ -224,7 +224,7 @@ __device__ __forceinline__ void fused_march(FusedCtx &c, int tid, int ya, int yb
         if (y >= ya) fz_load_mat<PH>(c, tid, y);
         __syncthreads();
         if (PH == ELASTIC) {
-            // plane y+5 (< ny - 3 for every chunk of [8, ny-8)) into the slot of
+            // plane y+5 (< ny - 1 for every chunk of [6, ny-6)) into the slot of
             // plane y-3, which no phase of this iteration reads
             if (!c.tma) {
                 fz_load_u<true>(c, tid, y + 5, ring<PH>(y + 5));

@@ -12,8 +12,10 @@
 // per thread in 5-deep register queues.  The x/z tiling (tile_range) gives the
 // rows of the SBP boundary closures to the first and last tiles, whose windows
 // hold every sample those rows read; first derivatives at closure rows of the
-// halo are taken from global memory.  Planes within 8 of the y walls are left
-// to the per-point kernels (the launch covers y in [8, ny-8)).
+// halo are taken from global memory.  The 6 planes next to each y wall (the
+// y closure rows) are left to the marching kernel (or the per-point kernels);
+// the launch covers y in [6, ny-6), where every first derivative along y of
+// the planes it reads, y-2 .. y+2 of each output plane y, is an interior row.
 //
 // Every helper is a host/device function of (context, thread index) so a CPU
 // harness can run the same phases thread by thread.
@@ -29,7 +31,7 @@ constexpr int HW = 4;                          // halo of the displacement ring
 constexpr int ZW = TZ + 2 * HW, XW = TX + 2 * HW;
 constexpr int HD = 2;                          // halo of the derived planes
 constexpr int ZH = TZ + 2 * HD, XH = TX + 2 * HD;
-constexpr int YPAD = 8;                        // y planes per side left to the per-point kernels
+constexpr int YPAD = 6;                        // y planes per side left to the closure-capable kernels
 }  // namespace fz
 
 // Derived-plane slots: T0, Y0, Z0, X2, Y2 in dv; T2 (VTI only; the isotropic
@@ -254,7 +256,7 @@ FWI_HD float fz_dz(const FusedCtx &c, int k, int slot, int ixw, int iz)
     return d1_row(s, iz, c.a->g.nz, c.rows) * c.a->idz;
 }
 // Dy at a plane from the ring slots of its four neighbours: interior rows only
-// (the fused launch keeps every differentiated plane in [6, ny-6)).
+// (the fused launch differentiates planes 4 .. ny-5 only, interior D1 rows).
 FWI_HD float fz_dy(const FusedCtx &c, int k, const int *sn, int ixw, int izw)
 {
     const SbpTables &t = sbp();
@@ -740,7 +742,7 @@ inline void fz_interior_range(int n, int T, int &lo, int &hi)
     if (lo == K) lo = hi = 0;
 }
 
-// The march of one CTA over output planes [ya, yb) (all inside [8, ny-8)).
+// The march of one CTA over output planes [ya, yb) (all inside [6, ny-6)).
 template <int PH>
 FWI_HD void fz_prologue(FusedCtx &c, int tid, int ya)
 {
