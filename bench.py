@@ -32,6 +32,7 @@ import argparse
 import json
 import os
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -110,7 +111,7 @@ class Clocks:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"fwi3d_b200_clocks_{os.getpid()}.csv")
 
     def start(self):
         try:
@@ -148,6 +149,10 @@ class Clocks:
                 for name, v in zip(names, parts[3:7]):
                     if v.lower() == "active":
                         reasons.add(name)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
                 "samples": len(sm)}
 
