@@ -154,3 +154,25 @@ def test_timing_is_max_over_ranks_gloo():
         p.join(120)
     res = sorted(q.get(timeout=10) for _ in range(2))
     assert res == [(0, 20.0), (1, 20.0)]
+
+
+def test_reference_arm_json_line():
+    """bench.py --impl reference runs the reference's CPU build on a bounded
+    window and prints one JSON line with the contract's keys."""
+    import json
+    import subprocess
+    import sys
+
+    lib = os.path.join(ROOT, "oracle", "_ref", "libfwi3d_ref_fp32.so")
+    if not os.path.exists(lib):
+        pytest.skip("reference CPU build not present")
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--n", "64",
+                          "--steps", "1", "--warmup", "1"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    for key in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
