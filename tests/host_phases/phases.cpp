@@ -9,9 +9,11 @@
 //     synchronously;
 //   the 6 planes next to each y wall: the marching kernel in slab mode;
 //   then the face SAT pass (k_elastic_face_sat) on every face point.
+// PH 2 runs the acoustic marching kernel (k_acoustic_fused: every plane, SAT
+// inline) against the acoustic per-point step instead.
 // Usage: phases PH nx ny nz nchunks bcset taper tables
-//   PH 3 isotropic / 6 VTI; bcset 0..2; tables 1: closure weights from the
-//   per-model tables (k_w2c), 0: formed in place.
+//   PH 2 acoustic / 3 isotropic / 6 VTI; bcset 0..2; tables 1: closure
+//   weights from the per-model tables (k_w2c), 0: formed in place.
 // Prints "rel <relative L2> max <max abs> nan <count>".
 #include <cmath>
 #include <cstdio>
@@ -22,6 +24,7 @@
 
 #include "fused.cuh"
 #include "march.cuh"
+#include "acoustic.cuh"
 #include "host_ops.h"
 
 using namespace fwi;
@@ -174,6 +177,34 @@ void face_sat(const StepArgs &a)
             }
 }
 
+// k_acoustic_fused over every tile and y chunk
+void acoustic_march(const StepArgs &a, int nch)
+{
+    const Dims &g = a.g;
+    AcousticSmem *sm = new AcousticSmem;
+    const int kz = (g.nz + fa::TZ - 1) / fa::TZ, kx = (g.nx + fa::TX - 1) / fa::TX;
+    auto par = [&](auto &&phase) {
+        for (int t = 0; t < fa::NT; t++) phase(t);
+    };
+    for (int bz = 0; bz < kz; bz++)
+        for (int bx = 0; bx < kx; bx++)
+            for (int ch = 0; ch < nch; ch++) {
+                AcousticCtx c;
+                c.a = &a;
+                c.sm = sm;
+                c.so = 0;
+                tile_range(bz, g.nz, fa::TZ, c.z0, c.zend);
+                tile_range(bx, g.nx, fa::TX, c.x0, c.xend);
+                const int ya = (int)((int64_t)g.ny * ch / nch), yb = (int)((int64_t)g.ny * (ch + 1) / nch);
+                if (ya >= yb) continue;
+                for (size_t k = 0; k < sizeof(AcousticSmem) / 4; k++) ((float *)sm)[k] = NAN;
+                const bool fast = c.x0 >= 6 && c.x0 + fa::TX <= g.nx - 6 && c.z0 >= 6 && c.z0 + fa::TZ <= g.nz - 6;
+                if (fast) fa_march<true>(c, ya, yb, par);
+                else fa_march<false>(c, ya, yb, par);
+            }
+    delete sm;
+}
+
 // closure-weight tables of k_w2c, on the host
 struct W2cHost {
     Line mu, eps, c66;
@@ -243,7 +274,11 @@ int main(int argc, char **argv)
     std::mt19937 rng(7);
     std::uniform_real_distribution<float> U(-1.f, 1.f);
     std::vector<float> model(G.nm * G.n);
-    for (int64_t i = 0; i < G.n; i++) {
+    for (int64_t i = 0; i < G.n && G.nm == 2; i++) {
+        model[i] = 4.0f + 1.0f * U(rng);             // K
+        model[G.n + i] = 0.45f + 0.1f * U(rng);      // 1/rho
+    }
+    for (int64_t i = 0; i < G.n && G.nm != 2; i++) {
         model[i] = 2.0f + 0.5f * U(rng);          // lambda
         model[G.n + i] = 1.5f + 0.4f * U(rng);    // mu
         model[2 * G.n + i] = 2.2f + 0.3f * U(rng);  // rho
@@ -302,6 +337,29 @@ int main(int argc, char **argv)
     for (int c = 0; c < 3; c++) {
         a.curr[c] = curr.data() + c * G.n;
         a.prev[c] = prev.data() + c * G.n;
+    }
+    if (G.nm == 2) {
+        // acoustic: one component
+        for (int iy = 0; iy < G.ny; iy++)
+            for (int ix = 0; ix < G.nx; ix++)
+                for (int iz = 0; iz < G.nz; iz++) ref[a.g.idx(ix, iy, iz)] = acoustic_point(a, ix, iy, iz);
+        StepArgs b = a;
+        b.next[0] = got.data();
+        acoustic_march(b, nch);
+        double num = 0, den = 0, mx = 0;
+        int64_t nan = 0;
+        for (int64_t k = 0; k < G.n; k++) {
+            if (!std::isfinite(got[k])) {
+                nan++;
+                continue;
+            }
+            const double e = (double)got[k] - ref[k];
+            num += e * e;
+            den += (double)ref[k] * ref[k];
+            mx = std::fmax(mx, std::fabs(e));
+        }
+        std::printf("rel %.3e max %.3e nan %lld\n", std::sqrt(num / den), mx, (long long)nan);
+        return 0;
     }
     per_point(a, G, ref);
 

@@ -1,6 +1,7 @@
-"""The elastic step's GPU phases run on the host, thread by thread, in the
-kernels' order (tests/host_phases/phases.cpp): the fused kernel's tiles on
-planes [6, ny-6), the marching kernel's y-wall slabs and the face SAT pass,
+"""The step kernels' phases run on the host, thread by thread, in the
+kernels' order (tests/host_phases/phases.cpp): for elastic media the fused
+kernel's tiles on planes [6, ny-6), the marching kernel's y-wall slabs and
+the face SAT pass, for acoustic media the marching kernel over every plane,
 against the per-point step, on seeded grids whose tiles, chunks and closure
 rows differ per axis.  Every phase is a host/device function, so this checks
 the kernels' index arithmetic, ring slots, closure handling and the per-model
@@ -31,6 +32,9 @@ def phases(tmp_path_factory):
 
 # (physics, nx, ny, nz, y chunks, bc set, taper width, closure-weight tables)
 CASES = [
+    (2, 60, 40, 76, 1, 0, 5, 0),
+    (2, 63, 33, 101, 3, 1, 3, 0),
+    (2, 45, 50, 47, 2, 2, 4, 0),
     (3, 60, 40, 76, 1, 0, 5, 0),
     (3, 60, 40, 76, 2, 1, 5, 1),
     (3, 63, 33, 101, 3, 2, 3, 1),   # odd sizes: shifted last tiles, partial tiles
