@@ -714,6 +714,10 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     const char *ge = std::getenv("FWI_GRAPHS");
     graphs_ = !(ge && ge[0] == '0');
     // isotropic media: interior and edge tiles in two launches (FWI_FUSED_SPLIT=0: one)
+    // y chunks per tile column: about FWI_FUSED_WAVES waves of resident CTAs
+    // (measured at 256^3 x 8: 1 12.88, 2 11.05, 4 10.11, 8 9.85, 16 9.84 ms per step)
+    const char *fw = std::getenv("FWI_FUSED_WAVES");
+    fused_waves_ = fw ? std::max(1, std::atoi(fw)) : 8;
     const char *sp = std::getenv("FWI_FUSED_SPLIT");
     fused_split_ = !(sp && sp[0] == '0');
     // plane copies of the fused kernel by the tensor memory accelerator
@@ -1050,10 +1054,10 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         tm.on = tma_ && encode_level_map(&tm.u, curr, pb_) ? 1 : 0;
         const dim3 fblk(fz::TZ, fz::TX);
         const size_t sm = sizeof(FusedSmem);
-        // y chunks per tile column: about four waves of resident CTAs, at
-        // least 16 planes per chunk
+        // y chunks per tile column: about fused_waves_ waves of resident CTAs,
+        // at least 16 planes per chunk
         auto chunks = [&](int64_t tiles, int minb) {
-            const int64_t target = 148 * minb * 4;
+            const int64_t target = 148 * minb * fused_waves_;
             const int64_t c = (target + tiles - 1) / tiles;
             return (int)std::max<int64_t>(1, std::min<int64_t>(c, (f.y1 - f.y0) / 16));
         };

@@ -216,6 +216,7 @@ private:
     bool capture_graph();
     void drop_graph();
     bool fused_split_ = true;      // interior and edge tiles of the fused kernel in separate launches
+    int fused_waves_ = 8;          // y chunks per tile column: about this many waves of resident CTAs
     bool fused_split_active() const;
     bool tma_ = false;             // fused kernel copies planes with bulk-tensor copies
     DevBuf tma_err_;               // int: a fused-kernel wait for a plane copy gave up
