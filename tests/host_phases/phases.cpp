@@ -11,9 +11,13 @@
 //   then the face SAT pass (k_elastic_face_sat) on every face point.
 // PH 2 runs the acoustic marching kernel (k_acoustic_fused: every plane, SAT
 // inline) against the acoustic per-point step instead.
+// PH 13 / 16 (isotropic / VTI + 10) checks the imaging increments instead:
+// the closure-free interior taps of k_image_batch against its
+// closure-capable per-point code at every interior point.
 // Usage: phases PH nx ny nz nchunks bcset taper tables
-//   PH 2 acoustic / 3 isotropic / 6 VTI; bcset 0..2; tables 1: closure
-//   weights from the per-model tables (k_w2c), 0: formed in place.
+//   PH 2 acoustic / 3 isotropic / 6 VTI (13 / 16 imaging); bcset 0..2;
+//   tables 1: closure weights from the per-model tables (k_w2c), 0: formed
+//   in place.
 // Prints "rel <relative L2> max <max abs> nan <count>".
 #include <cmath>
 #include <cstdio>
@@ -25,6 +29,7 @@
 #include "fused.cuh"
 #include "march.cuh"
 #include "acoustic.cuh"
+#include "imaging.cuh"
 #include "host_ops.h"
 
 using namespace fwi;
@@ -265,6 +270,8 @@ int main(int argc, char **argv)
     }
     Grid G;
     G.nm = std::atoi(argv[1]);
+    const bool imaging = G.nm > 10;
+    if (imaging) G.nm -= 10;
     G.nx = std::atoi(argv[2]);
     G.ny = std::atoi(argv[3]);
     G.nz = std::atoi(argv[4]);
@@ -337,6 +344,57 @@ int main(int argc, char **argv)
     for (int c = 0; c < 3; c++) {
         a.curr[c] = curr.data() + c * G.n;
         a.prev[c] = prev.data() + c * G.n;
+    }
+    if (imaging) {
+        // three snapshot levels and the lagged / current adjoint fields
+        std::vector<float> f3(9 * G.n), adj(3 * G.n), lag(3 * G.n);
+        for (auto &v : f3) v = U(rng);
+        for (auto &v : adj) v = U(rng);
+        for (auto &v : lag) v = U(rng);
+        ImageArgs im;
+        std::memset(&im, 0, sizeof(im));
+        im.g = a.g;
+        im.dx = dx;
+        im.dy = dy;
+        im.dz = dz;
+        im.rdx = 1.0f / dx;
+        im.rdy = 1.0f / dy;
+        im.rdz = 1.0f / dz;
+        im.dtimg = dt;
+        im.itl = 5;
+        im.last = 10;
+        for (int k = 0; k < G.nm; k++) im.m[k] = a.m[k];
+        for (int l = 0; l < 3; l++)
+            for (int c = 0; c < 3; c++) im.fwd[l][c] = f3.data() + (3 * l + c) * G.n;
+        for (int c = 0; c < 3; c++) {
+            im.adj[c] = adj.data() + c * G.n;
+            im.lag[c] = lag.data() + c * G.n;
+        }
+        double num = 0, den = 0, mx = 0;
+        int64_t nan = 0;
+        for (int iy = 4; iy < G.ny - 4; iy++)
+            for (int ix = 4; ix < G.nx - 4; ix++)
+                for (int iz = 4; iz < G.nz - 4; iz++) {
+                    double f[3], r[3];
+                    if (G.nm == 3) {
+                        elastic_image_inc<ELASTIC, true>(im, 0, ix, iy, iz, f[0], f[1], f[2]);
+                        elastic_image_inc<ELASTIC, false>(im, 0, ix, iy, iz, r[0], r[1], r[2]);
+                    } else {
+                        elastic_image_inc<VTI, true>(im, 0, ix, iy, iz, f[0], f[1], f[2]);
+                        elastic_image_inc<VTI, false>(im, 0, ix, iy, iz, r[0], r[1], r[2]);
+                    }
+                    for (int k = 0; k < 3; k++) {
+                        if (!std::isfinite(f[k])) {
+                            nan++;
+                            continue;
+                        }
+                        num += (f[k] - r[k]) * (f[k] - r[k]);
+                        den += r[k] * r[k];
+                        mx = std::fmax(mx, std::fabs(f[k] - r[k]));
+                    }
+                }
+        std::printf("rel %.3e max %.3e nan %lld\n", std::sqrt(num / den), mx, (long long)nan);
+        return 0;
     }
     if (G.nm == 2) {
         // acoustic: one component

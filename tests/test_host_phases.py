@@ -2,7 +2,8 @@
 kernels' order (tests/host_phases/phases.cpp): for elastic media the fused
 kernel's tiles on planes [6, ny-6), the marching kernel's y-wall slabs and
 the face SAT pass, for acoustic media the marching kernel over every plane,
-against the per-point step, on seeded grids whose tiles, chunks and closure
+against the per-point step (and the imaging kernel's interior taps against
+its per-point code), on seeded grids whose tiles, chunks and closure
 rows differ per axis.  Every phase is a host/device function, so this checks
 the kernels' index arithmetic, ring slots, closure handling and the per-model
 closure-weight tables without a GPU (the GPU tests run the same code as
@@ -41,6 +42,8 @@ CASES = [
     (6, 60, 40, 76, 2, 1, 5, 1),
     (6, 45, 30, 47, 1, 2, 4, 0),
     (6, 70, 30, 90, 2, 2, 3, 1),
+    (13, 40, 30, 36, 1, 0, 0, 0),   # imaging: interior taps vs per-point code
+    (16, 40, 30, 36, 1, 0, 0, 0),
 ]
 
 
