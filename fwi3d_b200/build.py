@@ -13,6 +13,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -20,7 +21,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libfwi3d_b200.so")
 REPO = os.path.dirname(HERE)
 
-CU_SOURCES = ["engine.cu"]
+CU_SOURCES = ["engine.cu", "pair.cu"]
 CXX_SOURCES = ["sbp_tables.cpp", "host_ops.cpp", "capi.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -61,6 +62,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_verbose: bool = Fals
     headers.append(os.path.join(REPO, "include", "fwi3d_gpu.h"))
     objs = []
     inc = ["-I", CSRC, "-I", os.path.join(REPO, "include")]
+    jobs = []
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
@@ -70,7 +72,11 @@ def build(verbose: bool = False, force: bool = False, ptxas_verbose: bool = Fals
                    *inc, "-c", s, "-o", o]
             if ptxas_verbose:
                 cmd += ["-Xptxas", "-v"]
-            _run(cmd, verbose)
+            jobs.append(cmd)
+    # the CUDA translation units compile in parallel (each takes minutes)
+    with ThreadPoolExecutor(max_workers=max(1, len(jobs))) as ex:
+        for f in [ex.submit(_run, cmd, verbose) for cmd in jobs]:
+            f.result()
     for src in CXX_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")

@@ -22,6 +22,7 @@
 #include "engine.h"
 #include "imaging.cuh"
 #include "fused.cuh"
+#include "tma.cuh"
 #include "march.cuh"
 #include "acoustic.cuh"
 #include "physics.cuh"
@@ -130,72 +131,6 @@ __global__ void k_elastic_step(StepArgs a)
     b.next[0][i] = v0;
     b.next[1][i] = v1;
     b.next[2][i] = v2;
-}
-
-// Tensor map of one time level for the fused kernel's plane copies: 5-D
-// (z, x, y, component, shot) over the [shot][component][y][x][z] layout, box
-// ZW x XW x 1 x 3 x 1 = one ring slot; out-of-grid positions read as zeros.
-struct FusedTma {
-    CUtensorMap u;
-    int *err;  // set to 1 when a wait for a copy gave up
-    int on;
-};
-
-__device__ __forceinline__ unsigned fz_saddr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void fz_bar_init(FusedCtx &c)
-{
-    for (int k = 0; k < 8; k++)
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(fz_saddr(&c.sm->bar[k])) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-}
-
-// One thread: copy plane q (three components, tile window with halo) into
-// ring slot `slot`; completion is signalled on the slot's barrier.
-__device__ __forceinline__ void fz_tma_issue(const FusedCtx &c, int q, int slot)
-{
-    const unsigned bar = fz_saddr(&c.sm->bar[slot]);
-    // order the block's earlier shared-memory accesses of the slot before the copy
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(FZ_PLANE_BYTES)
-                 : "memory");
-    asm volatile(
-        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
-        "%5, %6}], [%7];\n" ::"r"(fz_saddr(&c.sm->u[slot][0][0][0])),
-        "l"(c.tmap), "r"(c.z0 - fz::HW), "r"(c.x0 - fz::HW), "r"(q), "r"(0), "r"(c.shot), "r"(bar)
-        : "memory");
-}
-
-// Every thread: wait for the copy into `slot`.  The wait gives up after two
-// seconds (the copy takes microseconds), sets the error flag that the host
-// reads at its next synchronisation, and later waits of this thread return
-// at once, so that the kernel always ends.
-__device__ __forceinline__ void fz_tma_wait(FusedCtx &c, int slot)
-{
-    const unsigned bar = fz_saddr(&c.sm->bar[slot]);
-    const unsigned parity = (c.ph >> slot) & 1u;
-    c.ph ^= 1u << slot;
-    if (c.dead) return;
-    unsigned long long t0 = 0;
-    for (;;) {
-        unsigned ok;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(ok)
-            : "r"(bar), "r"(parity)
-            : "memory");
-        if (ok) return;
-        unsigned long long t;
-        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-        if (t0 == 0) {
-            t0 = t;
-        } else if (t - t0 > 2000000000ull) {
-            atomicOr(c.err, 1);
-            c.dead = true;
-            return;
-        }
-    }
 }
 
 // AX: edge tiles of the isotropic kernel take the per-axis output code (the
@@ -718,6 +653,10 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     // (measured at 256^3 x 8: 1 12.88, 2 11.05, 4 10.11, 8 9.85, 16 9.84 ms per step)
     const char *fw = std::getenv("FWI_FUSED_WAVES");
     fused_waves_ = fw ? std::max(1, std::atoi(fw)) : 8;
+    // isotropic interior tiles: two z-adjacent points per thread in packed
+    // FP32 pairs (FWI_PAIR=0: one point per thread)
+    const char *pe = std::getenv("FWI_PAIR");
+    pair_ = !(pe && pe[0] == '0');
     const char *sp = std::getenv("FWI_FUSED_SPLIT");
     fused_split_ = !(sp && sp[0] == '0');
     // plane copies of the fused kernel by the tensor memory accelerator
@@ -739,6 +678,7 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
                                 (int)sizeof(FusedSmem)));
         CK(cudaFuncSetAttribute(k_elastic_fused_part<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(FusedSmem)));
+        CK(pair_init());
     }
 }
 
@@ -1074,7 +1014,8 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
             const int ne = chunks(te, 2), ni = chunks(ti, 2);
             const dim3 ge(kz, kx, ne * pb_.nshots), gi(zh - zl, xh - xl, ni * pb_.nshots);
             k_elastic_fused_part<2><<<ge, fblk, sm, s>>>(f, ne, tm, 0, 0);
-            k_elastic_fused_part<1><<<gi, fblk, sm, s>>>(f, ni, tm, zl, xl);
+            if (!pair_) k_elastic_fused_part<1><<<gi, fblk, sm, s>>>(f, ni, tm, zl, xl);
+            else pair_launch(pb_.nz % 2 == 0, gi, sm, s, f, ni, tm, zl, xl);
         } else {
             const int nch = chunks((int64_t)kz * kx * pb_.nshots, fused_minb_);
             const dim3 grd(kz, kx, nch * pb_.nshots);

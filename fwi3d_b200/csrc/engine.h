@@ -215,6 +215,7 @@ private:
     uint64_t graph_key() const;
     bool capture_graph();
     void drop_graph();
+    bool pair_ = true;             // isotropic interior tiles by the paired kernel (pair.cuh)
     bool fused_split_ = true;      // interior and edge tiles of the fused kernel in separate launches
     int fused_waves_ = 8;          // y chunks per tile column: about this many waves of resident CTAs
     bool fused_split_active() const;
