@@ -220,7 +220,8 @@ __global__ void __launch_bounds__(fz::NT, MINB)
 
 // Isotropic fused step split by tiles: MODE 1 runs the interior tiles only
 // (grid tile indices offset by (bz0, bx0)), MODE 2 the edge tiles only (the
-// interior tiles of its full grid return at once).  Separate launches give
+// interior tiles of its full grid return at once; with bz0 = 1 also the edge
+// tiles that touch no z face).  Separate launches give
 // each its own register allocation: the interior code runs without spills
 // and the edge tiles can keep the closure-free code on their interior axis.
 template <int MODE>
@@ -252,6 +253,7 @@ __global__ void __launch_bounds__(fz::NT, 2)
     }
     const bool xf = fz_interior_tile(c.x0, fz::TX, a.g.nx), zf = fz_interior_tile(c.z0, fz::TZ, a.g.nz);
     if (xf && zf) return;
+    if (bz0 == 1 && zf) return;  // the tiles that touch an x face only run elsewhere
     if (xf) fused_march<ELASTIC, true, false, true>(c, tid, ya, yb);
     else if (zf) fused_march<ELASTIC, false, true, true>(c, tid, ya, yb);
     else fused_march<ELASTIC, false, false, true>(c, tid, ya, yb);
@@ -657,6 +659,10 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     // FP32 pairs (FWI_PAIR=0: one point per thread)
     const char *pe = std::getenv("FWI_PAIR");
     pair_ = !(pe && pe[0] == '0');
+    // its edge tiles (FWI_PAIR_EDGE): 0 all by the one-point kernel, 1 those
+    // touching an x face only by the paired kernel, 2 all by the paired kernel
+    const char *pee = std::getenv("FWI_PAIR_EDGE");
+    pair_edge_ = pee ? std::max(0, std::min(2, std::atoi(pee))) : 2;
     const char *sp = std::getenv("FWI_FUSED_SPLIT");
     fused_split_ = !(sp && sp[0] == '0');
     // plane copies of the fused kernel by the tensor memory accelerator
@@ -1008,14 +1014,27 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         const bool el = pb_.nmodels == 3;
         const bool split = fused_split_active();
         kmark(true, "k_elastic_fused", (int64_t)(f.y1 - f.y0) * pb_.nx * pb_.nz * pb_.nshots);
-        if (split) {
+        if (el && pair_) {
+            // paired kernel: edge tiles (all of them when no tile is interior), then interior tiles
+            const int64_t ti = (int64_t)(zh - zl) * (xh - xl) * pb_.nshots;
+            const int64_t te = (int64_t)kz * kx * pb_.nshots - ti;
+            const int ne = chunks(te, 2), ni = chunks(std::max<int64_t>(ti, 1), 2);
+            const bool even = pb_.nz % 2 == 0;
+            if (te > 0 && pair_edge_ == 2) {
+                pair_launch(even, 2, dim3(kz, kx, ne * pb_.nshots), sm, s, f, ne, tm, 0, 0);
+            } else if (te > 0) {
+                // tiles with a z face: the one-point-per-thread kernel; with x faces only: the paired one
+                k_elastic_fused_part<2><<<dim3(kz, kx, ne * pb_.nshots), fblk, sm, s>>>(f, ne, tm, pair_edge_, 0);
+                if (pair_edge_ == 1) pair_launch(even, 3, dim3(kz, kx, ne * pb_.nshots), sm, s, f, ne, tm, 0, 0);
+            }
+            if (ti > 0) pair_launch(even, 1, dim3(zh - zl, xh - xl, ni * pb_.nshots), sm, s, f, ni, tm, zl, xl);
+        } else if (split) {
             const int64_t ti = (int64_t)(zh - zl) * (xh - xl) * pb_.nshots;
             const int64_t te = (int64_t)kz * kx * pb_.nshots - ti;
             const int ne = chunks(te, 2), ni = chunks(ti, 2);
             const dim3 ge(kz, kx, ne * pb_.nshots), gi(zh - zl, xh - xl, ni * pb_.nshots);
             k_elastic_fused_part<2><<<ge, fblk, sm, s>>>(f, ne, tm, 0, 0);
-            if (!pair_) k_elastic_fused_part<1><<<gi, fblk, sm, s>>>(f, ni, tm, zl, xl);
-            else pair_launch(pb_.nz % 2 == 0, gi, sm, s, f, ni, tm, zl, xl);
+            k_elastic_fused_part<1><<<gi, fblk, sm, s>>>(f, ni, tm, zl, xl);
         } else {
             const int nch = chunks((int64_t)kz * kx * pb_.nshots, fused_minb_);
             const dim3 grd(kz, kx, nch * pb_.nshots);
@@ -1127,7 +1146,15 @@ int Engine::launches_per_step() const
 {
     int k = (pb_.nmodels == 2 ? 1
                               : (march_ ? 2 : (fused_ ? (slab_march_ ? 3 : (pb_.ny < 2 * (fz::YPAD + 2) ? 5 : 6)) : 2)));
-    if (fused_ && fused_split_active()) k += 1;  // interior and edge tiles launched apart
+    if (fused_ && pb_.nmodels == 3 && pair_) {
+        int zl, zh, xl, xh;
+        fz_interior_range(pb_.nz, fz::TZ, zl, zh);
+        fz_interior_range(pb_.nx, fz::TX, xl, xh);
+        if (zh > zl && xh > xl) k += 1;  // interior and edge tiles launched apart
+        if (pair_edge_ == 1) k += 1;     // edge tiles in two launches
+    } else if (fused_ && fused_split_active()) {
+        k += 1;
+    }
     if (ext_.nrec) k += 1;
     for (int c = 0; c < 3; c++) k += inj_.n[c] ? 1 : 0;
     return k;

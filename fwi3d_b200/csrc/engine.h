@@ -216,6 +216,7 @@ private:
     bool capture_graph();
     void drop_graph();
     bool pair_ = true;             // isotropic interior tiles by the paired kernel (pair.cuh)
+    int pair_edge_ = 2;            // its edge tiles: 0 one-point kernel, 1 x-face-only tiles paired, 2 all paired
     bool fused_split_ = true;      // interior and edge tiles of the fused kernel in separate launches
     int fused_waves_ = 8;          // y chunks per tile column: about this many waves of resident CTAs
     bool fused_split_active() const;

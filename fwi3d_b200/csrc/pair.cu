@@ -18,7 +18,7 @@ namespace {
 // and the material plane are written between them, and no phase after the
 // second reads the material plane or a ring slot that the next step's copies
 // overwrite.
-template <bool EVEN>
+template <bool EVEN, bool XC, bool ZC>
 __device__ __forceinline__ void pair_march(FusedCtx &c, int tid, int ya, int yb)
 {
     PairThread th;
@@ -26,6 +26,7 @@ __device__ __forceinline__ void pair_march(FusedCtx &c, int tid, int ya, int yb)
     for (int k = 0; k < 5; k++) th.qmu[k] = th.qT[k] = th.qX1[k] = th.qZ1[k] = f2s(0.f);
     const PairK K = pair_consts(*c.a);
     if (c.tma && tid == 0) fz_bar_init(c);
+    if (XC || ZC) fill_pair_rows(c.sm->rows, tid, pz::NT);
     for (int q = ya - 4; q < ya; q++) pz_load_u<false>(c, tid, q, ring<ELASTIC>(q));
     __syncthreads();
     for (int y = ya - 4; y < yb; y++) {
@@ -47,11 +48,11 @@ __device__ __forceinline__ void pair_march(FusedCtx &c, int tid, int ya, int yb)
             fz_tma_issue(c, y + 5, ring<ELASTIC>(y + 5));
         }
         if (c.tma) fz_tma_wait(c, c.sl[6]);
-        pz_column(c, K, th, tid, cin);
+        pz_column<XC, ZC>(c, K, th, tid, cin);
         F2 acc[3];
         UpdIn uin;
         if (y >= ya) {
-            pz_phase_b(c, K, th, tid, acc);
+            pz_phase_b<XC, ZC>(c, K, th, tid, y, acc);
             uin = pz_upd_in<EVEN>(c, tid, y);
         }
         __syncthreads();
@@ -60,16 +61,20 @@ __device__ __forceinline__ void pair_march(FusedCtx &c, int tid, int ya, int yb)
             pz_load_mat<EVEN, true>(c, tid, y + 1);
             cpa_commit();
         }
-        if (y >= ya) pz_phase_c<EVEN>(c, K, th, tid, y, acc, uin);
+        if (y >= ya) pz_phase_c<EVEN, XC, ZC>(c, K, th, tid, y, acc, uin);
     }
     cpa_wait();
     if (c.tma) fz_tma_wait(c, ring<ELASTIC>(yb + 4));  // the copy issued in the last step
 }
 
-// Paired isotropic step over the interior tiles (tile indices offset by
-// (bz0, bx0)).  grid: (interior z tiles, interior x tiles, y chunks x shots),
-// block 256.  EVEN: nz even, so every pair is 8-byte aligned in global memory.
-template <bool EVEN>
+// Paired isotropic step.  grid: (z tiles, x tiles, y chunks x shots), block
+// 256.  EVEN: nz even, so every pair is 8-byte aligned in global memory.
+// MODE 1: the interior tiles only (tile indices offset by (bz0, bx0)); MODE 2:
+// the edge tiles (the grid covers every tile, interior ones return at once),
+// with the closure rows of the faces they touch; MODE 3: the edge tiles that
+// touch an x face but no z face.  Separate launches give each
+// its own register allocation.
+template <bool EVEN, int MODE>
 __global__ void __launch_bounds__(pz::NT, 2)
     k_elastic_pair(const __grid_constant__ StepArgs a, int nchunks, const __grid_constant__ FusedTma t, int bz0,
                    int bx0)
@@ -86,13 +91,22 @@ __global__ void __launch_bounds__(pz::NT, 2)
     c.shot = blockIdx.z / nchunks;
     const int ch = blockIdx.z - c.shot * nchunks;
     c.so = c.shot * a.sst;
-    tile_range(blockIdx.x + bz0, a.g.nz, fz::TZ, c.z0, c.zend);
-    tile_range(blockIdx.y + bx0, a.g.nx, fz::TX, c.x0, c.xend);
+    tile_range(blockIdx.x + (MODE == 1 ? bz0 : 0), a.g.nz, fz::TZ, c.z0, c.zend);
+    tile_range(blockIdx.y + (MODE == 1 ? bx0 : 0), a.g.nx, fz::TX, c.x0, c.xend);
     const int len = a.y1 - a.y0;
     const int ya = a.y0 + (int)((int64_t)len * ch / nchunks);
     const int yb = a.y0 + (int)((int64_t)len * (ch + 1) / nchunks);
     if (ya >= yb) return;
-    pair_march<EVEN>(c, tid, ya, yb);
+    if (MODE == 1) {
+        pair_march<EVEN, false, false>(c, tid, ya, yb);
+        return;
+    }
+    const bool xi = fz_interior_tile(c.x0, fz::TX, a.g.nx), zi = fz_interior_tile(c.z0, fz::TZ, a.g.nz);
+    if (xi && zi) return;
+    if (MODE == 3 && !zi) return;  // MODE 3: the tiles that touch an x face only
+    if (xi) pair_march<EVEN, false, true>(c, tid, ya, yb);
+    else if (zi) pair_march<EVEN, true, false>(c, tid, ya, yb);
+    else pair_march<EVEN, true, true>(c, tid, ya, yb);
 }
 
 }  // namespace
@@ -101,18 +115,27 @@ cudaError_t pair_init()
 {
     init_sbp_tables();
     cudaError_t e = cudaMemcpyToSymbol(c_sbp, &g_sbp_host, sizeof(SbpTables));
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_elastic_pair<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FusedSmem));
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_elastic_pair<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sizeof(FusedSmem));
+    const void *k[6] = {(const void *)k_elastic_pair<true, 1>,  (const void *)k_elastic_pair<true, 2>,
+                        (const void *)k_elastic_pair<true, 3>,  (const void *)k_elastic_pair<false, 1>,
+                        (const void *)k_elastic_pair<false, 2>, (const void *)k_elastic_pair<false, 3>};
+    for (int i = 0; i < 6 && e == cudaSuccess; i++)
+        e = cudaFuncSetAttribute(k[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FusedSmem));
+    return e;
 }
 
-void pair_launch(bool even, dim3 grid, size_t smem, cudaStream_t s, const StepArgs &a, int nchunks,
+void pair_launch(bool even, int mode, dim3 grid, size_t smem, cudaStream_t s, const StepArgs &a, int nchunks,
                  const FusedTma &t, int bz0, int bx0)
 {
-    if (even) k_elastic_pair<true><<<grid, pz::NT, smem, s>>>(a, nchunks, t, bz0, bx0);
-    else k_elastic_pair<false><<<grid, pz::NT, smem, s>>>(a, nchunks, t, bz0, bx0);
+    if (mode == 1) {
+        if (even) k_elastic_pair<true, 1><<<grid, pz::NT, smem, s>>>(a, nchunks, t, bz0, bx0);
+        else k_elastic_pair<false, 1><<<grid, pz::NT, smem, s>>>(a, nchunks, t, bz0, bx0);
+    } else if (mode == 2) {
+        if (even) k_elastic_pair<true, 2><<<grid, pz::NT, smem, s>>>(a, nchunks, t, 0, 0);
+        else k_elastic_pair<false, 2><<<grid, pz::NT, smem, s>>>(a, nchunks, t, 0, 0);
+    } else {
+        if (even) k_elastic_pair<true, 3><<<grid, pz::NT, smem, s>>>(a, nchunks, t, 0, 0);
+        else k_elastic_pair<false, 3><<<grid, pz::NT, smem, s>>>(a, nchunks, t, 0, 0);
+    }
 }
 
 }  // namespace fwi

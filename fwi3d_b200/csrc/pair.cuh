@@ -1,10 +1,11 @@
-// Isotropic elastic step on the interior tiles, two z-adjacent points per
+// Isotropic elastic step of planes [6, ny-6), two z-adjacent points per
 // thread in packed FP32 pairs.
 //
 // Same tiling, ring and bulk-tensor plane copies as the fused kernel
-// (fused.cuh): a CTA owns a TZ x TX = 32 x 16 tile of (z, x) columns whose
-// outputs and derived halo hold no SBP closure row along x or z, and marches
-// along y over planes of [6, ny-6).  Here a thread owns the pair (z, z+1) of
+// (fused.cuh): a CTA owns a TZ x TX = 32 x 16 tile of (z, x) columns and
+// marches along y over planes of [6, ny-6).  Interior tiles (outputs and
+// derived halo free of SBP closure rows along x and z) run the pair form
+// only; edge tiles add the closure rows (see pxd1/pzd1 and phase B).  Here a thread owns the pair (z, z+1) of
 // one x row, so a CTA has 256 threads: lanes 0-15 of a warp cover row 2w,
 // lanes 16-31 row 2w+1, and each half-warp reads 16 consecutive pairs (128
 // contiguous bytes) per shared-memory access.
@@ -72,8 +73,8 @@ FWI_HD F2 f2s(float a) { return f2(a, a); }
 FWI_HD float f2lo(F2 p)
 {
 #if defined(__CUDA_ARCH__)
-    float a, b;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(p.v));
+    float a;
+    asm("{\n .reg .b32 t;\n mov.b64 {%0, t}, %1;\n}" : "=f"(a) : "l"(p.v));
     return a;
 #else
     return p.x;
@@ -82,8 +83,8 @@ FWI_HD float f2lo(F2 p)
 FWI_HD float f2hi(F2 p)
 {
 #if defined(__CUDA_ARCH__)
-    float a, b;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(p.v));
+    float b;
+    asm("{\n .reg .b32 t;\n mov.b64 {t, %0}, %1;\n}" : "=f"(b) : "l"(p.v));
     return b;
 #else
     return p.y;
@@ -280,23 +281,26 @@ FWI_HD void pz_load_u(FusedCtx &c, int tid, int q, int slot)
 }
 
 // One 8-byte global->shared copy (both addresses 8-byte aligned):
-// asynchronous on the GPU (cp.async), a plain copy on the host.
+// asynchronous on the GPU (cp.async; zero fill when `valid` is false, `src`
+// then only has to be a mapped address), a plain copy on the host.
 template <bool ASYNC>
-FWI_HD void cpa8(float *dst, const float *src)
+FWI_HD void cpa8(float *dst, const float *src, bool valid)
 {
 #if defined(__CUDA_ARCH__)
     if (ASYNC) {
         const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 8 : 0)
+                     : "memory");
         return;
     }
 #endif
-    dst[0] = src[0];
-    dst[1] = src[1];
+    dst[0] = valid ? src[0] : 0.f;
+    dst[1] = valid ? src[1] : 0.f;
 }
 
-// Material planes mu, lambda at y over the derived region, as pairs; with
-// ASYNC the copies are asynchronous (waited for with cpa_wait).
+// Material planes mu, lambda at y over the derived region, as pairs (zeros
+// outside the grid, where edge tiles' windows reach); with ASYNC the copies
+// are asynchronous (waited for with cpa_wait).
 template <bool EVEN, bool ASYNC>
 FWI_HD void pz_load_mat(FusedCtx &c, int tid, int y)
 {
@@ -305,17 +309,20 @@ FWI_HD void pz_load_mat(FusedCtx &c, int tid, int y)
     for (int p = tid; p < fz::XH * NP; p += pz::NT) {
         const int xh = p / NP, zh = 2 * (p - xh * NP);
         const int ix = c.x0 - fz::HD + xh, iz = c.z0 - fz::HD + zh;
-        // interior tiles: every position of the derived region is inside the grid
-        const int64_t i = g.idx(ix, y, iz);
+        const bool xin = ix >= 0 && ix < g.nx;
+        const bool in0 = xin && iz >= 0 && iz < g.nz, in1 = xin && iz + 1 >= 0 && iz + 1 < g.nz;
+        // positions outside the grid copy nothing (zero fill) from the array's start
+        const int64_t i0 = in0 ? g.idx(ix, y, iz) : 0, i1 = in1 ? g.idx(ix, y, iz + 1) : 0;
         float *dm = &fz_mpp(c.sm, MP_MU)[xh][zh], *dl = &fz_mpp(c.sm, MP_LAM)[xh][zh];
         if (EVEN) {
-            cpa8<ASYNC>(dm, c.a->m[1] + i);
-            cpa8<ASYNC>(dl, c.a->m[0] + i);
+            // nz, z0 and zh even: a pair is inside the grid or outside as a whole
+            cpa8<ASYNC>(dm, c.a->m[1] + i0, in0);
+            cpa8<ASYNC>(dl, c.a->m[0] + i0, in0);
         } else {
-            cpa4<ASYNC>(dm, c.a->m[1] + i, true);
-            cpa4<ASYNC>(dm + 1, c.a->m[1] + i + 1, true);
-            cpa4<ASYNC>(dl, c.a->m[0] + i, true);
-            cpa4<ASYNC>(dl + 1, c.a->m[0] + i + 1, true);
+            cpa4<ASYNC>(dm, c.a->m[1] + i0, in0);
+            cpa4<ASYNC>(dm + 1, c.a->m[1] + i1, in1);
+            cpa4<ASYNC>(dl, c.a->m[0] + i0, in0);
+            cpa4<ASYNC>(dl + 1, c.a->m[0] + i1, in1);
         }
     }
 }
@@ -348,11 +355,135 @@ FWI_HD UpdIn pz_upd_in(const FusedCtx &c, int tid, int y)
     return r;
 }
 
+// ---------------------------------------------------------------------------
+// Derivatives at the own pair with the SBP closures of the edge tiles.
+// XC: the tile touches an x face.  x rows are uniform per half-warp, so a row
+// within 4 (D1) or 6 (D2var) of a face takes the reference's closure row for
+// both points of the pair at once (pair taps along x, the row's coefficient in
+// both halves) while the other half-warps take the interior form.
+// ZC: the tile touches a z face.  Its closure pairs are (0,1), (2,3), (4,5)
+// and their mirrors at the high face: both points of such a pair are closure
+// rows that read the same wall samples, so a closure pair multiplies each
+// wall sample (in both halves) by the pair of its two rows' coefficients.
+// Only these pairs diverge from the rest of their warp.  Pairs of other
+// alignments reach closure rows only in rows a tile does not store (the rows
+// beyond the next tile's origin); they take the per-point rows.
+// D2var closure weights come from the per-model tables (a.w2c, 8 weights per
+// closure row and line), read once per plane for the three components.
+// ---------------------------------------------------------------------------
+// Closure coefficient pairs in shared memory (the rows region of FusedSmem):
+//   [0, 48)    D1 along z, kinds 0..3 x 6 wall samples x (point 0, point 1):
+//              rows (0,1), (2,3) of the low face, rows (1,0), (3,2) of the
+//              high face negated (the reference's mirrored closure)
+//   [48, 144)  D1 along x, kinds 0..7 x 6 wall samples x (c, c): row r of the
+//              low face (kind r), row r of the high face negated (kind 4+r)
+constexpr int PR_X = 48, PR_FLOATS = 144;
+static_assert(PR_FLOATS <= SR_FLOATS, "closure pairs must fit the rows region");
+FWI_HD void fill_pair_rows(float *p, int tid, int nt)
+{
+    const SbpTables &t = sbp();
+    for (int e = tid; e < PR_FLOATS / 2; e += nt) {
+        if (e < 24) {
+            const int kind = e / 6, j = e % 6;
+            const int r0 = kind == 0 ? 0 : kind == 1 ? 2 : kind == 2 ? 1 : 3;
+            const int r1 = kind == 0 ? 1 : kind == 1 ? 3 : kind == 2 ? 0 : 2;
+            const float sg = kind < 2 ? 1.f : -1.f;
+            p[2 * e] = sg * t.d1b[r0][j];
+            p[2 * e + 1] = sg * t.d1b[r1][j];
+        } else {
+            const int e2 = e - 24, kind = e2 / 6, j = e2 % 6;
+            const float v = (kind < 4 ? 1.f : -1.f) * t.d1b[kind & 3][j];
+            p[2 * e] = v;
+            p[2 * e + 1] = v;
+        }
+    }
+}
+
+// D1 along x of a field at p (own pair, global row ix), row stride XS
+template <bool XC>
+FWI_HD F2 pxd1(const FusedCtx &c, const float *p, int XS, int ix, F2 c0h, F2 c1h, float ih)
+{
+    const int n = c.a->g.nx;
+    if (XC && (ix < 4 || ix >= n - 4)) {
+        const bool hi = ix >= n - 4;
+        const float *w = c.sm->rows + PR_X + ((hi ? 4 : 0) + (hi ? n - 1 - ix : ix)) * 12;
+        const float *b = p + ((hi ? n - 1 : 0) - ix) * XS;  // the own column at the wall
+        const int st = hi ? -XS : XS;
+        F2 acc = mul2(ld2(w), ld2(b));
+#pragma unroll
+        for (int j = 1; j < 6; j++) acc = fma2(ld2(w + 2 * j), ld2(b + j * st), acc);
+        return mul2(acc, f2s(ih));
+    }
+    return d1p(ld2(p - 2 * XS), ld2(p - XS), ld2(p + XS), ld2(p + 2 * XS), c0h, c1h);
+}
+// D1 along z of a field at p (own pair at global z iz), window origin zoff (global z of index 0)
+template <bool ZC>
+FWI_HD F2 pzd1(const FusedCtx &c, const float *p, int iz, int zoff, F2 c0h, F2 c1h, float ih)
+{
+    const int n = c.a->g.nz;
+    if (ZC && (iz < 4 || iz + 1 >= n - 4)) {
+        const int kind = iz == 0 ? 0 : iz == 2 ? 1 : iz + 1 == n - 1 ? 2 : iz + 1 == n - 3 ? 3 : -1;
+        if (kind >= 0) {
+            const bool hi = kind >= 2;
+            const float *w = c.sm->rows + kind * 12;
+            const float *b = p + (hi ? n - 1 - iz : -iz);  // the wall sample
+            const int st = hi ? -1 : 1;
+            F2 acc = mul2(ld2(w), f2s(b[0]));
+#pragma unroll
+            for (int j = 1; j < 6; j++) acc = fma2(ld2(w + 2 * j), f2s(b[j * st]), acc);
+            return mul2(acc, f2s(ih));
+        }
+        const SZ l{p - (iz - zoff), zoff};
+        return f2(d1_row(l, iz, n, ConstRows()) * ih, d1_row(l, iz + 1, n, ConstRows()) * ih);
+    }
+    const ZT z = ztaps(p);
+    return d1p(z.m, z.m1(), z.p1(), z.b, c0h, c1h);
+}
+
+// D2var closure weights of a pair (8 per point, scaled by s) from a per-model table.
+struct W8p {
+    F2 w[8];
+};
+FWI_HD W8p w8_pair(const float *p0, const float *p1, F2 s)
+{
+    W8p r;
+#if defined(__CUDA_ARCH__)
+    const float4 a0 = *reinterpret_cast<const float4 *>(p0), a1 = *reinterpret_cast<const float4 *>(p0 + 4);
+    const float4 b0 = *reinterpret_cast<const float4 *>(p1), b1 = *reinterpret_cast<const float4 *>(p1 + 4);
+    r.w[0] = f2(a0.x, b0.x); r.w[1] = f2(a0.y, b0.y); r.w[2] = f2(a0.z, b0.z); r.w[3] = f2(a0.w, b0.w);
+    r.w[4] = f2(a1.x, b1.x); r.w[5] = f2(a1.y, b1.y); r.w[6] = f2(a1.z, b1.z); r.w[7] = f2(a1.w, b1.w);
+#else
+    for (int j = 0; j < 8; j++) r.w[j] = f2(p0[j], p1[j]);
+#endif
+#pragma unroll
+    for (int j = 0; j < 8; j++) r.w[j] = mul2(r.w[j], s);
+    return r;
+}
+
+// The same derivatives added to acc (the pair form folds the sum into its FMAs).
+template <bool XC>
+FWI_HD F2 pxd1acc(const FusedCtx &c, const float *p, int XS, int ix, F2 c0h, F2 c1h, float ih, F2 acc)
+{
+    if (XC) return add2(acc, pxd1<XC>(c, p, XS, ix, c0h, c1h, ih));
+    return d1acc(ld2(p - 2 * XS), ld2(p - XS), ld2(p + XS), ld2(p + 2 * XS), c0h, c1h, acc);
+}
+template <bool ZC>
+FWI_HD F2 pzd1acc(const FusedCtx &c, const float *p, int iz, int zoff, F2 c0h, F2 c1h, float ih, F2 acc)
+{
+    if (ZC) return add2(acc, pzd1<ZC>(c, p, iz, zoff, c0h, c1h, ih));
+    const ZT z = ztaps(p);
+    return d1acc(z.m, z.m1(), z.p1(), z.b, c0h, c1h, acc);
+}
+
 // Column phase: plane q = y+2 of the own pair into the y queues.
+template <bool XC, bool ZC>
 FWI_HD void pz_column(const FusedCtx &c, const PairK &K, PairThread &th, int tid, const ColIn &in)
 {
+    const StepArgs &a = *c.a;
     const int pzi = tid % pz::NPR, lx = tid / pz::NPR;
     const int xw = lx + fz::HW, zw = 2 * pzi + fz::HW;
+    const int ix = c.x0 + lx, iz = c.z0 + 2 * pzi;
+    const int zo = c.z0 - fz::HW;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         th.qmu[k] = th.qmu[k + 1];
@@ -365,24 +496,34 @@ FWI_HD void pz_column(const FusedCtx &c, const PairK &K, PairThread &th, int tid
     const int s0 = c.sl[4];
     constexpr int X = fz::ZW;
     const float *u0 = pz_u(c, s0, 0, xw, zw), *u1 = pz_u(c, s0, 1, xw, zw), *u2 = pz_u(c, s0, 2, xw, zw);
-    const F2 ux0 = d1p(ld2(u0 - 2 * X), ld2(u0 - X), ld2(u0 + X), ld2(u0 + 2 * X), K.cx0, K.cx1);
-    const F2 ux1 = d1p(ld2(u1 - 2 * X), ld2(u1 - X), ld2(u1 + X), ld2(u1 + 2 * X), K.cx0, K.cx1);
+    const F2 ux0 = pxd1<XC>(c, u0, X, ix, K.cx0, K.cx1, a.idx);
+    const F2 ux1 = pxd1<XC>(c, u1, X, ix, K.cx0, K.cx1, a.idx);
     const F2 uy1 = d1p(ld2(pz_u(c, c.sl[2], 1, xw, zw)), ld2(pz_u(c, c.sl[3], 1, xw, zw)),
                        ld2(pz_u(c, c.sl[5], 1, xw, zw)), ld2(pz_u(c, c.sl[6], 1, xw, zw)), K.cy0, K.cy1);
-    const ZT z2 = ztaps(u2), z1 = ztaps(u1);
-    const F2 uz2 = d1p(z2.m, z2.m1(), z2.p1(), z2.b, K.cz0, K.cz1);
-    const F2 uz1 = d1p(z1.m, z1.m1(), z1.p1(), z1.b, K.cz0, K.cz1);
+    const F2 uz2 = pzd1<ZC>(c, u2, iz, zo, K.cz0, K.cz1, a.idz);
+    const F2 uz1 = pzd1<ZC>(c, u1, iz, zo, K.cz0, K.cz1, a.idz);
     th.qT[4] = mul2(in.lam, add2(add2(ux0, uy1), uz2));
     th.qX1[4] = mul2(in.mu, ux1);
     th.qZ1[4] = mul2(in.mu, uz1);
 }
 
 // Derived values at one pair of the derived region (xh, zh): T always, and
-// (Y0, Z0) on x-halo rows or (X2, Y2) on z-halo pairs.
-template <bool XHALO>
+// (Y0, Z0) on x-halo rows or (X2, Y2) on z-halo pairs; zeros outside the grid
+// (no closure row reads them).
+template <bool XHALO, bool XC, bool ZC>
 FWI_HD void pz_derived_halo(const FusedCtx &c, const PairK &K, int xh, int zh)
 {
+    const StepArgs &a = *c.a;
+    const int ix = c.x0 - fz::HD + xh, iz = c.z0 - fz::HD + zh;
+    if ((XC && (ix < 0 || ix >= a.g.nx)) || (ZC && (iz < 0 || iz >= a.g.nz))) {
+        const F2 z = f2s(0.f);
+        st2(&fz_dvp(c.sm, DV_T0)[xh][zh], z);
+        st2(&fz_dvp(c.sm, XHALO ? DV_Y0 : DV_X2)[xh][zh], z);
+        st2(&fz_dvp(c.sm, XHALO ? DV_Z0 : DV_Y2)[xh][zh], z);
+        return;
+    }
     const int xw = xh + (fz::HW - fz::HD), zw = zh + (fz::HW - fz::HD);
+    const int zo = c.z0 - fz::HW;
     constexpr int X = fz::ZW;
     const int s0 = c.sl[2];
     const float *u0 = pz_u(c, s0, 0, xw, zw), *u2 = pz_u(c, s0, 2, xw, zw);
@@ -391,37 +532,108 @@ FWI_HD void pz_derived_halo(const FusedCtx &c, const PairK &K, int xh, int zh)
         return d1p(ld2(pz_u(c, c.sl[0], k, xw, zw)), ld2(pz_u(c, c.sl[1], k, xw, zw)),
                    ld2(pz_u(c, c.sl[3], k, xw, zw)), ld2(pz_u(c, c.sl[4], k, xw, zw)), K.cy0, K.cy1);
     };
-    const F2 ux0 = d1p(ld2(u0 - 2 * X), ld2(u0 - X), ld2(u0 + X), ld2(u0 + 2 * X), K.cx0, K.cx1);
+    const F2 ux0 = pxd1<XC>(c, u0, X, ix, K.cx0, K.cx1, a.idx);
     const F2 uy1 = ydiff(1);
-    const ZT z2 = ztaps(u2);
-    const F2 uz2 = d1p(z2.m, z2.m1(), z2.p1(), z2.b, K.cz0, K.cz1);
+    const F2 uz2 = pzd1<ZC>(c, u2, iz, zo, K.cz0, K.cz1, a.idz);
     st2(&fz_dvp(c.sm, DV_T0)[xh][zh], mul2(lam, add2(add2(ux0, uy1), uz2)));
     if (XHALO) {
-        const ZT z0 = ztaps(u0);
         st2(&fz_dvp(c.sm, DV_Y0)[xh][zh], mul2(mu, ydiff(0)));
-        st2(&fz_dvp(c.sm, DV_Z0)[xh][zh], mul2(mu, d1p(z0.m, z0.m1(), z0.p1(), z0.b, K.cz0, K.cz1)));
+        st2(&fz_dvp(c.sm, DV_Z0)[xh][zh], mul2(mu, pzd1<ZC>(c, u0, iz, zo, K.cz0, K.cz1, a.idz)));
     } else {
-        const F2 ux2 = d1p(ld2(u2 - 2 * X), ld2(u2 - X), ld2(u2 + X), ld2(u2 + 2 * X), K.cx0, K.cx1);
-        st2(&fz_dvp(c.sm, DV_X2)[xh][zh], mul2(mu, ux2));
+        st2(&fz_dvp(c.sm, DV_X2)[xh][zh], mul2(mu, pxd1<XC>(c, u2, X, ix, K.cx0, K.cx1, a.idx)));
         st2(&fz_dvp(c.sm, DV_Y2)[xh][zh], mul2(mu, ydiff(2)));
     }
 }
 
 // Phase B: D2var terms of the own pair into acc, derived values of the own
 // pair (and, for threads 0..95, of the halo) into the derived planes.
-FWI_HD void pz_phase_b(const FusedCtx &c, const PairK &K, const PairThread &th, int tid, F2 acc[3])
+template <bool XC, bool ZC>
+FWI_HD void pz_phase_b(const FusedCtx &c, const PairK &K, const PairThread &th, int tid, int y, F2 acc[3])
 {
+    const StepArgs &a = *c.a;
+    const Dims &g = a.g;
     const int pzi = tid % pz::NPR, lx = tid / pz::NPR;
     const int xw = lx + fz::HW, zw = 2 * pzi + fz::HW;
     const int xh = lx + fz::HD, zh = 2 * pzi + fz::HD;
+    const int ix = c.x0 + lx, iz = c.z0 + 2 * pzi;
+    const int xo = c.x0 - fz::HW, zo = c.z0 - fz::HW;
     constexpr int X = fz::ZW, XD = fz::ZH;
+    // closure rows of D2var (rows within 6 of a face) on this pair
+    const bool xcl = XC && (ix < 6 || ix >= g.nx - 6);
+    const bool zcl = ZC && (iz < 6 || iz + 1 >= g.nz - 6);
     const float *mp = &fz_mpp(c.sm, MP_MU)[xh][zh];
     const F2 mu0 = ld2(mp);
     const F2 lam = ld2(&fz_mpp(c.sm, MP_LAM)[xh][zh]);
-    const W5p wx = d2w_pair(ld2(mp - 2 * XD), ld2(mp - XD), mu0, ld2(mp + XD), ld2(mp + 2 * XD), K.sx1);
-    const ZT zm = ztaps(mp);
-    const W5p wz = d2w_pair(zm.m, zm.m1(), mu0, zm.p1(), zm.b, K.sz1);
+    W5p wx{}, wz{};
+    if (!xcl) wx = d2w_pair(ld2(mp - 2 * XD), ld2(mp - XD), mu0, ld2(mp + XD), ld2(mp + 2 * XD), K.sx1);
+    if (!zcl) {
+        const ZT zm = ztaps(mp);
+        wz = d2w_pair(zm.m, zm.m1(), mu0, zm.p1(), zm.b, K.sz1);
+    }
     const W5p wy = d2w_pair(th.qmu[0], th.qmu[1], th.qmu[2], th.qmu[3], th.qmu[4], K.sy1);
+    // D2var closure terms of the three components (scaled by a/h^2, a = 1):
+    // weights read once per plane, wall samples of each component's ring line
+    F2 d2xc[3], d2zc[3];
+    if (XC && xcl) {
+        const bool hi = ix >= g.nx - 6;
+        const int r = hi ? g.nx - 1 - ix : ix, slot = hi ? 6 + r : r;
+        const float *tab = a.w2c[0][0];
+        const int64_t ln = (int64_t)y * g.nz + iz;
+        const int st = hi ? -X : X;
+        if (tab) {
+            const W8p W = w8_pair(tab + (ln * 12 + slot) * 8, tab + ((ln + 1) * 12 + slot) * 8, K.sx1);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const float *b = pz_u(c, c.sl[2], k, xw, zw) + ((hi ? g.nx - 1 : 0) - ix) * X;
+                F2 v = mul2(W.w[0], ld2(b));
+#pragma unroll
+                for (int j = 1; j < 8; j++) v = fma2(W.w[j], ld2(b + j * st), v);
+                d2xc[k] = v;
+            }
+        } else {
+            for (int k = 0; k < 3; k++) {
+                const float *l = pz_u(c, c.sl[2], k, xw, zw) - (ix - xo) * X;
+                d2xc[k] = f2(d2var_row(SX{l, xo, X}, mx_line(c, MP_MU, zh), ix, g.nx, a.ad1[0], ConstRows()),
+                             d2var_row(SX{l + 1, xo, X}, mx_line(c, MP_MU, zh + 1), ix, g.nx, a.ad1[0], ConstRows()));
+            }
+        }
+    }
+    if (ZC && zcl) {
+        const int n = g.nz;
+        const bool lo = iz == 0 || iz == 2 || iz == 4, hi = n - 1 - iz == 1 || n - 1 - iz == 3 || n - 1 - iz == 5;
+        const float *tab = a.w2c[2][0];
+        const int64_t ln = (int64_t)y * g.nx + ix;
+        if (tab && (lo || hi)) {
+            // rows (iz, iz+1) at the low face, (n-1-iz, n-2-iz) at the high face
+            const int s0 = lo ? iz : 6 + (n - 1 - iz), s1 = lo ? iz + 1 : 5 + (n - 1 - iz);
+            const W8p W = w8_pair(tab + (ln * 12 + s0) * 8, tab + (ln * 12 + s1) * 8, K.sz1);
+            const int st = hi ? -1 : 1;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const float *b = pz_u(c, c.sl[2], k, xw, zw) + (hi ? n - 1 - iz : -iz);
+                F2 v = mul2(W.w[0], f2s(b[0]));
+#pragma unroll
+                for (int j = 1; j < 8; j++) v = fma2(W.w[j], f2s(b[j * st]), v);
+                d2zc[k] = v;
+            }
+        } else {
+            const SZ f = mz_line(c, MP_MU, xh);
+            for (int k = 0; k < 3; k++) {
+                const SZ l{pz_u(c, c.sl[2], k, xw, zw) - (iz - zo), zo};
+                d2zc[k] = f2(d2var_tab(tab, ln, l, f, iz, n, a.ad1[2], ConstRows()),
+                             d2var_tab(tab, ln, l, f, iz + 1, n, a.ad1[2], ConstRows()));
+            }
+        }
+    }
+    // D2var along x / z of component k added to v
+    auto d2x = [&](int k, F2 xm2, F2 xm1, F2 u0, F2 xp1, F2 xp2, F2 v) -> F2 {
+        if (XC && xcl) return add2(v, d2xc[k]);
+        return d2acc(wx, xm2, xm1, u0, xp1, xp2, v);
+    };
+    auto d2z = [&](int k, const ZT &z, F2 zm1, F2 zp1, F2 v) -> F2 {
+        if (ZC && zcl) return add2(v, d2zc[k]);
+        return d2acc(wz, z.m, zm1, z.a, zp1, z.b, v);
+    };
     F2 ux0, uy0, uz0, uy1, ux2, uy2, uz2;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
@@ -434,27 +646,27 @@ FWI_HD void pz_phase_b(const FusedCtx &c, const PairK &K, const PairThread &th, 
         // own axis first, doubled (a = 2 for the component's own direction)
         F2 v;
         if (k == 0) {
-            v = d2acc(wx, xm2, xm1, u0, xp1, xp2, f2s(0.f));
+            v = d2x(k, xm2, xm1, u0, xp1, xp2, f2s(0.f));
             v = add2(v, v);
             v = d2acc(wy, ym2, ym1, u0, yp1, yp2, v);
-            v = d2acc(wz, z.m, zm1, u0, zp1, z.b, v);
-            ux0 = d1p(xm2, xm1, xp1, xp2, K.cx0, K.cx1);
+            v = d2z(k, z, zm1, zp1, v);
+            ux0 = XC ? pxd1<XC>(c, u, X, ix, K.cx0, K.cx1, a.idx) : d1p(xm2, xm1, xp1, xp2, K.cx0, K.cx1);
             uy0 = d1p(ym2, ym1, yp1, yp2, K.cy0, K.cy1);
-            uz0 = d1p(z.m, zm1, zp1, z.b, K.cz0, K.cz1);
+            uz0 = ZC ? pzd1<ZC>(c, u, iz, zo, K.cz0, K.cz1, a.idz) : d1p(z.m, zm1, zp1, z.b, K.cz0, K.cz1);
         } else if (k == 1) {
             v = d2acc(wy, ym2, ym1, u0, yp1, yp2, f2s(0.f));
             v = add2(v, v);
-            v = d2acc(wx, xm2, xm1, u0, xp1, xp2, v);
-            v = d2acc(wz, z.m, zm1, u0, zp1, z.b, v);
+            v = d2x(k, xm2, xm1, u0, xp1, xp2, v);
+            v = d2z(k, z, zm1, zp1, v);
             uy1 = d1p(ym2, ym1, yp1, yp2, K.cy0, K.cy1);
         } else {
-            v = d2acc(wz, z.m, zm1, u0, zp1, z.b, f2s(0.f));
+            v = d2z(k, z, zm1, zp1, f2s(0.f));
             v = add2(v, v);
-            v = d2acc(wx, xm2, xm1, u0, xp1, xp2, v);
+            v = d2x(k, xm2, xm1, u0, xp1, xp2, v);
             v = d2acc(wy, ym2, ym1, u0, yp1, yp2, v);
-            ux2 = d1p(xm2, xm1, xp1, xp2, K.cx0, K.cx1);
+            ux2 = XC ? pxd1<XC>(c, u, X, ix, K.cx0, K.cx1, a.idx) : d1p(xm2, xm1, xp1, xp2, K.cx0, K.cx1);
             uy2 = d1p(ym2, ym1, yp1, yp2, K.cy0, K.cy1);
-            uz2 = d1p(z.m, zm1, zp1, z.b, K.cz0, K.cz1);
+            uz2 = ZC ? pzd1<ZC>(c, u, iz, zo, K.cz0, K.cz1, a.idz) : d1p(z.m, zm1, zp1, z.b, K.cz0, K.cz1);
         }
         acc[k] = v;
     }
@@ -468,15 +680,18 @@ FWI_HD void pz_phase_b(const FusedCtx &c, const PairK &K, const PairThread &th, 
     // threads 64..95 (warp-uniform split)
     if (tid < 4 * pz::NPR) {
         const int r = tid / pz::NPR;
-        pz_derived_halo<true>(c, K, r < 2 ? r : fz::XH - 4 + r, fz::HD + 2 * (tid % pz::NPR));
+        pz_derived_halo<true, XC, ZC>(c, K, r < 2 ? r : fz::XH - 4 + r, fz::HD + 2 * (tid % pz::NPR));
     } else if (tid < 4 * pz::NPR + 2 * pz::TX) {
         const int u = tid - 4 * pz::NPR;
-        pz_derived_halo<false>(c, K, fz::HD + (u >> 1), (u & 1) ? fz::ZH - 2 : 0);
+        pz_derived_halo<false, XC, ZC>(c, K, fz::HD + (u >> 1), (u & 1) ? fz::ZH - 2 : 0);
     }
 }
 
-// Phase C: first derivatives of the derived planes and queues, update, taper.
-template <bool EVEN>
+// Phase C: first derivatives of the derived planes and queues, update,
+// absorbing-boundary scaling of face points (edge tiles), taper; points
+// beyond the tile's output rows (xend, zend: rows the next tile owns) are
+// not stored.
+template <bool EVEN, bool XC, bool ZC>
 FWI_HD void pz_phase_c(const FusedCtx &c, const PairK &K, const PairThread &th, int tid, int y, const F2 acc[3],
                        const UpdIn &in)
 {
@@ -486,31 +701,31 @@ FWI_HD void pz_phase_c(const FusedCtx &c, const PairK &K, const PairThread &th, 
     const int ix = c.x0 + lx, iz = c.z0 + 2 * pzi;
     const int xw = lx + fz::HW, zw = 2 * pzi + fz::HW;
     const int xh = lx + fz::HD, zh = 2 * pzi + fz::HD;
+    const int zo = c.z0 - fz::HD;
     constexpr int XD = fz::ZH;
     const float *t0 = &fz_dvp(c.sm, DV_T0)[xh][zh];
     const float *y0 = &fz_dvp(c.sm, DV_Y0)[xh][zh], *z0 = &fz_dvp(c.sm, DV_Z0)[xh][zh];
     const float *x2 = &fz_dvp(c.sm, DV_X2)[xh][zh], *y2 = &fz_dvp(c.sm, DV_Y2)[xh][zh];
     // comp 0: Dx(T) + Dy(mu u_x1) + Dz(mu u_x2) with 1/dy (we_op.cpp:678)
-    F2 v0 = d1acc(ld2(t0 - 2 * XD), ld2(t0 - XD), ld2(t0 + XD), ld2(t0 + 2 * XD), K.cx0, K.cx1, acc[0]);
+    F2 v0 = pxd1acc<XC>(c, t0, XD, ix, K.cx0, K.cx1, a.idx, acc[0]);
     v0 = d1acc(th.qX1[0], th.qX1[1], th.qX1[3], th.qX1[4], K.cy0, K.cy1, v0);
-    const ZT zx2 = ztaps(x2);
-    v0 = d1acc(zx2.m, zx2.m1(), zx2.p1(), zx2.b, K.cy0, K.cy1, v0);
+    v0 = pzd1acc<ZC>(c, x2, iz, zo, K.cy0, K.cy1, a.idy, v0);
     // comp 1: Dy(T) + Dx(mu u_y0) + Dz(mu u_y2)
     F2 v1 = d1acc(th.qT[0], th.qT[1], th.qT[3], th.qT[4], K.cy0, K.cy1, acc[1]);
-    v1 = d1acc(ld2(y0 - 2 * XD), ld2(y0 - XD), ld2(y0 + XD), ld2(y0 + 2 * XD), K.cx0, K.cx1, v1);
-    const ZT zy2 = ztaps(y2);
-    v1 = d1acc(zy2.m, zy2.m1(), zy2.p1(), zy2.b, K.cz0, K.cz1, v1);
+    v1 = pxd1acc<XC>(c, y0, XD, ix, K.cx0, K.cx1, a.idx, v1);
+    v1 = pzd1acc<ZC>(c, y2, iz, zo, K.cz0, K.cz1, a.idz, v1);
     // comp 2: Dz(T) + Dx(mu u_z0) + Dy(mu u_z1)
-    const ZT zt = ztaps(t0);
-    F2 v2 = d1acc(zt.m, zt.m1(), zt.p1(), zt.b, K.cz0, K.cz1, acc[2]);
-    v2 = d1acc(ld2(z0 - 2 * XD), ld2(z0 - XD), ld2(z0 + XD), ld2(z0 + 2 * XD), K.cx0, K.cx1, v2);
+    F2 v2 = pzd1acc<ZC>(c, t0, iz, zo, K.cz0, K.cz1, a.idz, acc[2]);
+    v2 = pxd1acc<XC>(c, z0, XD, ix, K.cx0, K.cx1, a.idx, v2);
     v2 = d1acc(th.qZ1[0], th.qZ1[1], th.qZ1[3], th.qZ1[4], K.cy0, K.cy1, v2);
 
     // update: next = dt^2 acc / rho + 2 curr - prev, then the taper
+    if (ix >= c.xend) return;
     const int64_t i = g.idx(ix, y, iz);
     const float dt2 = a.dt * a.dt;
     const F2 s = f2(dt2 * rcp_rn(f2lo(in.rho)), dt2 * rcp_rn(f2hi(in.rho)));
     const bool tz = in_taper(a, ix, y, iz) || in_taper(a, ix, y, iz + 1);
+    const bool face = (XC && (ix == 0 || ix == g.nx - 1)) || (ZC && (iz == 0 || iz >= g.nz - 2));
     F2 tf = f2s(1.f);
     if (tz) {
         // one factor per point, the product of the six in the reference's
@@ -529,8 +744,14 @@ FWI_HD void pz_phase_c(const FusedCtx &c, const PairK &K, const PairThread &th, 
         if (tz && a.taper_prev) p = mul2(p, tf);
         const F2 u0 = ld2(pz_u(c, c.sl[2], k, xw, zw));
         F2 r = sub2(fma2(v[k], s, add2(u0, u0)), p);
+        if (face) r = f2(boundary_scale(a, f2lo(r), k, ix, y, iz), boundary_scale(a, f2hi(r), k, ix, y, iz + 1));
         if (tz) r = mul2(r, tf);
-        stg2<EVEN>(a.next[k] + c.so + i, r);
+        float *dst = a.next[k] + c.so + i;
+        if (iz + 1 < c.zend) {
+            stg2<EVEN>(dst, r);
+        } else if (iz < c.zend) {
+            dst[0] = f2lo(r);
+        }
     }
 }
 
