@@ -1021,7 +1021,8 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
             const int ne = chunks(te, 2), ni = chunks(std::max<int64_t>(ti, 1), 2);
             const bool even = pb_.nz % 2 == 0;
             if (te > 0 && pair_edge_ == 2) {
-                pair_launch(even, 2, dim3(kz, kx, ne * pb_.nshots), sm, s, f, ne, tm, 0, 0);
+                for (int mode = 3; mode <= 5; mode++)
+                    pair_launch(even, mode, dim3(kz, kx, ne * pb_.nshots), sm, s, f, ne, tm, 0, 0);
             } else if (te > 0) {
                 // tiles with a z face: the one-point-per-thread kernel; with x faces only: the paired one
                 k_elastic_fused_part<2><<<dim3(kz, kx, ne * pb_.nshots), fblk, sm, s>>>(f, ne, tm, pair_edge_, 0);
@@ -1151,7 +1152,7 @@ int Engine::launches_per_step() const
         fz_interior_range(pb_.nz, fz::TZ, zl, zh);
         fz_interior_range(pb_.nx, fz::TX, xl, xh);
         if (zh > zl && xh > xl) k += 1;  // interior and edge tiles launched apart
-        if (pair_edge_ == 1) k += 1;     // edge tiles in two launches
+        k += pair_edge_ == 2 ? 2 : pair_edge_;  // edge tiles in three (two) launches
     } else if (fused_ && fused_split_active()) {
         k += 1;
     }

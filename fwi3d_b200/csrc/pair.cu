@@ -69,11 +69,11 @@ __device__ __forceinline__ void pair_march(FusedCtx &c, int tid, int ya, int yb)
 
 // Paired isotropic step.  grid: (z tiles, x tiles, y chunks x shots), block
 // 256.  EVEN: nz even, so every pair is 8-byte aligned in global memory.
-// MODE 1: the interior tiles only (tile indices offset by (bz0, bx0)); MODE 2:
-// the edge tiles (the grid covers every tile, interior ones return at once),
-// with the closure rows of the faces they touch; MODE 3: the edge tiles that
-// touch an x face but no z face.  Separate launches give each
-// its own register allocation.
+// MODE 1: the interior tiles only (tile indices offset by (bz0, bx0)).  The
+// edge tiles, with the closure rows of the faces they touch (the grid covers
+// every tile, the others return at once): MODE 3 the tiles that touch an x
+// face only, MODE 4 a z face only, MODE 5 both.  Separate launches give each
+// variant its own register allocation and a smaller instruction footprint.
 template <bool EVEN, int MODE>
 __global__ void __launch_bounds__(pz::NT, 2)
     k_elastic_pair(const __grid_constant__ StepArgs a, int nchunks, const __grid_constant__ FusedTma t, int bz0,
@@ -102,23 +102,30 @@ __global__ void __launch_bounds__(pz::NT, 2)
         return;
     }
     const bool xi = fz_interior_tile(c.x0, fz::TX, a.g.nx), zi = fz_interior_tile(c.z0, fz::TZ, a.g.nz);
-    if (xi && zi) return;
-    if (MODE == 3 && !zi) return;  // MODE 3: the tiles that touch an x face only
-    if (xi) pair_march<EVEN, false, true>(c, tid, ya, yb);
-    else if (zi) pair_march<EVEN, true, false>(c, tid, ya, yb);
-    else pair_march<EVEN, true, true>(c, tid, ya, yb);
+    if (MODE == 3 && !xi && zi) pair_march<EVEN, true, false>(c, tid, ya, yb);
+    if (MODE == 4 && xi && !zi) pair_march<EVEN, false, true>(c, tid, ya, yb);
+    if (MODE == 5 && !xi && !zi) pair_march<EVEN, true, true>(c, tid, ya, yb);
 }
 
 }  // namespace
+
+template <int MODE>
+static void launch_mode(bool even, dim3 grid, size_t smem, cudaStream_t s, const StepArgs &a, int nchunks, const FusedTma &t,
+                 int bz0, int bx0)
+{
+    if (even) k_elastic_pair<true, MODE><<<grid, pz::NT, smem, s>>>(a, nchunks, t, bz0, bx0);
+    else k_elastic_pair<false, MODE><<<grid, pz::NT, smem, s>>>(a, nchunks, t, bz0, bx0);
+}
 
 cudaError_t pair_init()
 {
     init_sbp_tables();
     cudaError_t e = cudaMemcpyToSymbol(c_sbp, &g_sbp_host, sizeof(SbpTables));
-    const void *k[6] = {(const void *)k_elastic_pair<true, 1>,  (const void *)k_elastic_pair<true, 2>,
-                        (const void *)k_elastic_pair<true, 3>,  (const void *)k_elastic_pair<false, 1>,
-                        (const void *)k_elastic_pair<false, 2>, (const void *)k_elastic_pair<false, 3>};
-    for (int i = 0; i < 6 && e == cudaSuccess; i++)
+    const void *k[8] = {(const void *)k_elastic_pair<true, 1>,  (const void *)k_elastic_pair<true, 3>,
+                        (const void *)k_elastic_pair<true, 4>,  (const void *)k_elastic_pair<true, 5>,
+                        (const void *)k_elastic_pair<false, 1>, (const void *)k_elastic_pair<false, 3>,
+                        (const void *)k_elastic_pair<false, 4>, (const void *)k_elastic_pair<false, 5>};
+    for (int i = 0; i < 8 && e == cudaSuccess; i++)
         e = cudaFuncSetAttribute(k[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FusedSmem));
     return e;
 }
@@ -126,15 +133,11 @@ cudaError_t pair_init()
 void pair_launch(bool even, int mode, dim3 grid, size_t smem, cudaStream_t s, const StepArgs &a, int nchunks,
                  const FusedTma &t, int bz0, int bx0)
 {
-    if (mode == 1) {
-        if (even) k_elastic_pair<true, 1><<<grid, pz::NT, smem, s>>>(a, nchunks, t, bz0, bx0);
-        else k_elastic_pair<false, 1><<<grid, pz::NT, smem, s>>>(a, nchunks, t, bz0, bx0);
-    } else if (mode == 2) {
-        if (even) k_elastic_pair<true, 2><<<grid, pz::NT, smem, s>>>(a, nchunks, t, 0, 0);
-        else k_elastic_pair<false, 2><<<grid, pz::NT, smem, s>>>(a, nchunks, t, 0, 0);
-    } else {
-        if (even) k_elastic_pair<true, 3><<<grid, pz::NT, smem, s>>>(a, nchunks, t, 0, 0);
-        else k_elastic_pair<false, 3><<<grid, pz::NT, smem, s>>>(a, nchunks, t, 0, 0);
+    switch (mode) {
+    case 1: launch_mode<1>(even, grid, smem, s, a, nchunks, t, bz0, bx0); break;
+    case 3: launch_mode<3>(even, grid, smem, s, a, nchunks, t, 0, 0); break;
+    case 4: launch_mode<4>(even, grid, smem, s, a, nchunks, t, 0, 0); break;
+    default: launch_mode<5>(even, grid, smem, s, a, nchunks, t, 0, 0); break;
     }
 }
 

@@ -82,8 +82,9 @@ __device__ __forceinline__ void fz_tma_wait(FusedCtx &c, int slot)
 cudaError_t pair_init();
 // Launches the paired isotropic kernel (pair.cuh).  mode 1: the interior
 // tiles (grid: interior z tiles, interior x tiles, chunks x shots; tile
-// indices offset by (bz0, bx0)); mode 2: the edge tiles (grid: every tile,
-// chunks x shots); mode 3: as mode 2, the tiles touching an x face only.  even: nz is even (8-byte global pair accesses).
+// indices offset by (bz0, bx0)); modes 3, 4, 5: the edge tiles touching an x
+// face only, a z face only, both (grid: every tile, chunks x shots).  even:
+// nz is even (8-byte global pair accesses).
 void pair_launch(bool even, int mode, dim3 grid, size_t smem, cudaStream_t s, const StepArgs &a, int nchunks,
                  const FusedTma &t, int bz0, int bx0);
 
