@@ -1021,8 +1021,15 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
             const int ne = chunks(te, 2), ni = chunks(std::max<int64_t>(ti, 1), 2);
             const bool even = pb_.nz % 2 == 0;
             if (te > 0 && pair_edge_ == 2) {
-                for (int mode = 3; mode <= 5; mode++)
-                    pair_launch(even, mode, dim3(kz, kx, ne * pb_.nshots), sm, s, f, ne, tm, 0, 0);
+                // tiles touching an x face only, a z face only, both: y chunks per launch
+                const int64_t nzi = zh - zl, nxi = xh - xl;
+                const int64_t tm3 = (kx - nxi) * nzi, tm4 = nxi * (kz - nzi), tm5 = (kx - nxi) * (kz - nzi);
+                const int64_t tiles[3] = {tm3, tm4, tm5};
+                for (int mode = 3; mode <= 5; mode++) {
+                    if (tiles[mode - 3] == 0) continue;
+                    const int nm = chunks(tiles[mode - 3] * pb_.nshots, 2);
+                    pair_launch(even, mode, dim3(kz, kx, nm * pb_.nshots), sm, s, f, nm, tm, 0, 0);
+                }
             } else if (te > 0) {
                 // tiles with a z face: the one-point-per-thread kernel; with x faces only: the paired one
                 k_elastic_fused_part<2><<<dim3(kz, kx, ne * pb_.nshots), fblk, sm, s>>>(f, ne, tm, pair_edge_, 0);
@@ -1152,7 +1159,14 @@ int Engine::launches_per_step() const
         fz_interior_range(pb_.nz, fz::TZ, zl, zh);
         fz_interior_range(pb_.nx, fz::TX, xl, xh);
         if (zh > zl && xh > xl) k += 1;  // interior and edge tiles launched apart
-        k += pair_edge_ == 2 ? 2 : pair_edge_;  // edge tiles in three (two) launches
+        if (pair_edge_ == 2) {
+            // edge tiles in up to three launches (x faces only, z faces only, both)
+            const int nzi = zh - zl, nxi = xh - xl, kz = (pb_.nz + fz::TZ - 1) / fz::TZ,
+                      kx = (pb_.nx + fz::TX - 1) / fz::TX;
+            k += ((kx - nxi) * nzi > 0) + (nxi * (kz - nzi) > 0) + ((kx - nxi) * (kz - nzi) > 0) - 1;
+        } else {
+            k += pair_edge_;  // edge tiles in two launches (1) or one (0)
+        }
     } else if (fused_ && fused_split_active()) {
         k += 1;
     }
