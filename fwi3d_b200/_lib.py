@@ -61,7 +61,7 @@ class CParam(C.Structure):
         ("deltamin", C.c_float), ("deltamax", C.c_float), ("epsilonmin", C.c_float),
         ("epsilonmax", C.c_float), ("gammamin", C.c_float), ("gammamax", C.c_float),
         ("soft_clip", C.c_int), ("verbose", C.c_int), ("snapshot_storage", C.c_int),
-        ("snapshot_budget_gb", C.c_float),
+        ("snapshot_budget_gb", C.c_float), ("checkpoint_slots", C.c_int), ("checkpoint_precision", C.c_int),
     ]
 
 

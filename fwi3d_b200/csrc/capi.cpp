@@ -107,6 +107,7 @@ struct fwi_op {
         if (!same) eng.reset(new Engine(device, pb));
         eng->set_storage(par.snapshot_storage);
         eng->set_snapshot_budget((int64_t)((double)par.snapshot_budget_gb * 1e9));
+        eng->set_checkpointing(par.checkpoint_slots, par.checkpoint_precision);
         eng->set_model(m.data());
         conv.swap(m);
     }
@@ -198,6 +199,8 @@ void fwi_param_default(fwi_param *p)
     p->verbose = 0;
     p->snapshot_storage = 0;
     p->snapshot_budget_gb = 0.f;
+    p->checkpoint_slots = 0;
+    p->checkpoint_precision = 0;
 }
 
 const char *fwi_last_error(void) { return g_err.c_str(); }
@@ -692,6 +695,7 @@ int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, floa
             if (!same) eng.reset(new Engine(o->device, p));
             eng->set_storage(par.snapshot_storage);
             eng->set_snapshot_budget((int64_t)((double)par.snapshot_budget_gb * 1e9));
+            eng->set_checkpointing(par.checkpoint_slots, par.checkpoint_precision);
             eng->set_model(m.data());
             // tables of the batch (shot b of the batch at wavefield offset b)
             InjTable inj, adj;

@@ -9,6 +9,7 @@
 // and, every `sub` steps of the adjoint, the imaging condition k_image_batch.
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -16,7 +17,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <mutex>
+#include <type_traits>
 #include <string>
 
 #include "engine.h"
@@ -715,7 +718,7 @@ int64_t Engine::device_bytes() const
 {
     return model_.bytes + w2c_.bytes + fields_.bytes + aux_.bytes + snaps_.bytes + grad_.bytes + sdiv_.bytes + taper_.bytes +
            src_dev_.bytes + rcv_dev_.bytes + snapq_.bytes + snaps_scale_.bytes + enc_.bytes + amax_.bytes +
-           snapz_.bytes + ckpt_.bytes + rec_fields_.bytes;
+           snapz_.bytes + rv_store_.bytes + rv_scale_.bytes + rec_fields_.bytes;
 }
 
 float *Engine::level(int l) const
@@ -1402,13 +1405,14 @@ void Engine::snap_store(int k)
     const int nsc = pb_.nshots * pb_.ncomp();
     if (k > nsnap_ - 1) return;
     nwritten_ = std::max(nwritten_, k + 1);
-    if (seg_L_ > 0) {
-        // checkpoint j holds (prev, curr) at snapshot ckpt_index(j)
-        const int j = k == 0 ? 0 : ((k + 1) % seg_L_ == 0 ? (k + 1) / seg_L_ : -1);
-        if (j >= 0 && j < nseg_) {
-            float *c = ckpt_.as<float>() + (int64_t)j * 2 * nsc * n;
-            CK(cudaMemcpyAsync(c, level(0), sizeof(float) * nsc * n, cudaMemcpyDeviceToDevice, s));
-            CK(cudaMemcpyAsync(c + (int64_t)nsc * n, level(1), sizeof(float) * nsc * n, cudaMemcpyDeviceToDevice, s));
+    if (rv_C_ > 0) {
+        // binomial checkpointing: the forward sweep keeps the states its schedule marks
+        if (k < (int)rv_mark_.size() && rv_mark_[k]) {
+            const int slot = rv_free_.back();
+            rv_free_.pop_back();
+            rv_store(slot, level(0), level(1));
+            rv_pos_stack_.push_back(k);
+            rv_slot_stack_.push_back(slot);
         }
         return;
     }
@@ -1429,9 +1433,26 @@ const float *Engine::snap_fp32(int kk)
 {
     const int64_t n = pb_.nxyz();
     const int nsc = pb_.nshots * pb_.ncomp();
-    if (seg_L_ > 0) {
+    const int64_t S = (int64_t)nsc * n;
+    if (rv_C_ > 0) {
         if (kk >= nwritten_) return snapz_.as<float>();
-        return snaps_.as<float>() + (int64_t)(kk - seg_lo_) * nsc * n;
+        for (int r = 0; r < 3; r++)
+            if (ring_[r] == kk) return snaps_.as<float>() + (int64_t)r * S;
+        // visit the states below the ring's lowest in decreasing order (the
+        // schedule's order) down to kk, keeping each one's current level
+        int lo = rv_K_ + 1;
+        for (int r = 0; r < 3; r++)
+            if (ring_[r] >= 0) lo = std::min(lo, ring_[r]);
+        if (kk > lo) throw FwiError(FWI_ERR_STATE, "snapshot requested above the states already visited");
+        cudaStream_t s = (cudaStream_t)stream_;
+        for (int t = lo - 1; t >= kk; t--) {
+            rv_goto(t);
+            const int r = t % 3;
+            CK(cudaMemcpyAsync(snaps_.as<float>() + (int64_t)r * S, rec_fields_.as<float>() + ((rv_rot_ + 1) % 3) * S,
+                               sizeof(float) * S, cudaMemcpyDeviceToDevice, s));
+            ring_[r] = t;
+        }
+        return snaps_.as<float>() + (int64_t)(kk % 3) * S;
     }
     if (storage_ == STORE_FP32) return snaps_.as<float>() + (int64_t)kk * nsc * n;
     if (kk >= nwritten_) return snapz_.as<float>();
@@ -1449,38 +1470,226 @@ const float *Engine::snap_fp32(int kk)
     return snaps_.as<float>() + (int64_t)(kk % 3) * nsc * n;
 }
 
-// Forward snapshots of segment j (indices ckpt_index(j) .. min((j+1)L, last))
-// recomputed from its checkpoint on the recomputation levels; the adjoint's
-// own levels are swapped out meanwhile.
-void Engine::recompute_segment(int j)
+// ---------------------------------------------------------------------------
+// Binomial checkpointing.  The chain is the sequence of snapshot states
+// 0..K (state k: time levels (prev, curr) at step k*sub; one chain step is sub
+// time steps).  reverse(s, e, c) visits states e, e-1, ..., s with state s in a
+// slot and c free slots: advance d steps from s, keep state s+d in a slot,
+// reverse(s+d, e, c-1), then reverse(s, s+d-1, c).  With no free slot every
+// state is reached from s again.  The cost table R(l, c) (forward chain steps
+// for l = e - s) and the minimising d come from the recursion
+//   R(0, c) = 0,  R(l, 0) = l (l + 1) / 2,
+//   R(l, c) = min over 1 <= d <= l of  d + R(l - d, c - 1) + R(d - 1, c),
+// whose minimum is the binomial bound of Griewank and Walther (revolve).
+// ---------------------------------------------------------------------------
+struct RevolveTable {
+    int K = -1, C = -1;
+    std::vector<int32_t> split;  // [(K+1) x (C+1)]
+    std::vector<int64_t> cost;
+};
+
+static const RevolveTable &revolve_table(int K, int C)
+{
+    static std::mutex mu;
+    static std::vector<std::unique_ptr<RevolveTable>> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto &t : cache)
+        if (t->K == K && t->C == C) return *t;
+    auto t = std::make_unique<RevolveTable>();
+    t->K = K;
+    t->C = C;
+    const int W = C + 1;
+    t->split.assign((size_t)(K + 1) * W, 0);
+    t->cost.assign((size_t)(K + 1) * W, 0);
+    auto R = [&](int l, int c) -> int64_t & { return t->cost[(size_t)l * W + c]; };
+    for (int l = 0; l <= K; l++) {
+        R(l, 0) = (int64_t)l * (l + 1) / 2;
+        t->split[(size_t)l * W] = l;
+    }
+    // the minimising d does not decrease with l: the search for l starts at
+    // the split of l - 1 (any d gives a valid schedule; this one is optimal)
+    for (int c = 1; c <= C; c++) {
+        int dlo = 1;
+        for (int l = 1; l <= K; l++) {
+            int64_t best = -1;
+            int bd = dlo;
+            for (int d = dlo; d <= l; d++) {
+                const int64_t v = d + R(l - d, c - 1) + R(d - 1, c);
+                if (best < 0 || v < best) {
+                    best = v;
+                    bd = d;
+                }
+            }
+            R(l, c) = best;
+            t->split[(size_t)l * W + c] = bd;
+            dlo = bd;
+        }
+    }
+    cache.push_back(std::move(t));
+    if (cache.size() > 8) cache.erase(cache.begin());
+    return *cache.back();
+}
+
+namespace {
+// Per (shot, component) max |a - b| of one state (b null: max |a|), as float bits.
+__global__ void k_ck_amax(const float *a, const float *b, int64_t n, unsigned *amax)
+{
+    const int f = blockIdx.y;
+    const float *p = a + (int64_t)f * n, *q = b ? b + (int64_t)f * n : nullptr;
+    float m = 0.f;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        m = fmaxf(m, fabsf(q ? p[i] - q[i] : p[i]));
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(amax + f, __float_as_uint(m));
+}
+// 16-bit slot values (a - b) / scale (BF16 or FP16, round to nearest), scale =
+// max |a - b| of the (shot, component) field (1 for an all-zero field)
+template <class T>
+__global__ void k_ck_quant(const float *a, const float *b, int64_t n, const unsigned *amax, T *q, float *scale)
+{
+    const int f = blockIdx.y;
+    const float mx = __uint_as_float(amax[f]);
+    const float sc = mx > 0.f ? mx : 1.f;
+    const float inv = 1.0f / sc;
+    if (blockIdx.x == 0 && threadIdx.x == 0) scale[f] = sc;
+    const float *p = a + (int64_t)f * n, *r = b ? b + (int64_t)f * n : nullptr;
+    T *o = q + (int64_t)f * n;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float v = (r ? p[i] - r[i] : p[i]) * inv;
+        if constexpr (std::is_same<T, __half>::value) o[i] = __float2half_rn(v);
+        else o[i] = __float2bfloat16_rn(v);
+    }
+}
+// v = q * scale, or (base non-null) v = base - q * scale
+template <class T>
+__global__ void k_ck_dequant(const T *q, int64_t n, const float *scale, const float *base, float *v)
+{
+    const int f = blockIdx.y;
+    const float sc = scale[f];
+    const T *p = q + (int64_t)f * n;
+    const float *b = base ? base + (int64_t)f * n : nullptr;
+    float *o = v + (int64_t)f * n;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float x;
+        if constexpr (std::is_same<T, __half>::value) x = __half2float(p[i]) * sc;
+        else x = __bfloat162float(p[i]) * sc;
+        o[i] = b ? b[i] - x : x;
+    }
+}
+}  // namespace
+
+// One restart state (prev, curr of the batch) into checkpoint slot `slot`.
+// FP32: both levels as they are.  16-bit: curr and the step difference
+// curr - prev, each scaled by its own max per (shot, component), so that the
+// rounding of the restart keeps the relative precision of the wave's time
+// difference as well as of its value.
+void Engine::rv_store(int slot, const float *prev, const float *curr)
 {
     cudaStream_t s = (cudaStream_t)stream_;
     const int64_t n = pb_.nxyz();
     const int nsc = pb_.nshots * pb_.ncomp();
     const int64_t S = (int64_t)nsc * n;
-    const int lo = ckpt_index(j);
-    const int hi = std::min((j + 1) * seg_L_, nwritten_ - 1);
+    if (rv_prec_ == 0) {
+        float *d = rv_store_.as<float>() + (int64_t)slot * 2 * S;
+        CK(cudaMemcpyAsync(d, prev, sizeof(float) * S, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(d + S, curr, sizeof(float) * S, cudaMemcpyDeviceToDevice, s));
+        return;
+    }
+    const dim3 grd((unsigned)std::min<int64_t>((n + 255) / 256, 1024), nsc);
+    for (int l = 0; l < 2; l++) {
+        const float *b = l == 0 ? nullptr : prev;  // level 0: curr; level 1: curr - prev
+        CK(cudaMemsetAsync(amax_.p, 0, sizeof(unsigned) * nsc, s));
+        k_ck_amax<<<grd, 256, 0, s>>>(curr, b, n, amax_.as<unsigned>());
+        float *sc = rv_scale_.as<float>() + ((int64_t)slot * 2 + l) * nsc;
+        const int64_t off = ((int64_t)slot * 2 + l) * S;
+        if (rv_prec_ == 1)
+            k_ck_quant<__nv_bfloat16><<<grd, 256, 0, s>>>(curr, b, n, amax_.as<unsigned>(),
+                                                           rv_store_.as<__nv_bfloat16>() + off, sc);
+        else
+            k_ck_quant<__half><<<grd, 256, 0, s>>>(curr, b, n, amax_.as<unsigned>(), rv_store_.as<__half>() + off, sc);
+    }
+    CK(cudaGetLastError());
+}
+
+// Checkpoint `slot` into the recomputation levels (prev at level 0, curr at level 1).
+void Engine::rv_restore(int slot)
+{
+    cudaStream_t s = (cudaStream_t)stream_;
+    const int64_t n = pb_.nxyz();
+    const int nsc = pb_.nshots * pb_.ncomp();
+    const int64_t S = (int64_t)nsc * n;
+    float *lev = rec_fields_.as<float>();
+    rv_rot_ = 0;
+    if (rv_prec_ == 0) {
+        const float *c = rv_store_.as<float>() + (int64_t)slot * 2 * S;
+        CK(cudaMemcpyAsync(lev, c, sizeof(float) * 2 * S, cudaMemcpyDeviceToDevice, s));
+        return;
+    }
+    const dim3 grd((unsigned)std::min<int64_t>((n + 255) / 256, 1024), nsc);
+    const float *sc0 = rv_scale_.as<float>() + (int64_t)slot * 2 * nsc, *sc1 = sc0 + nsc;
+    const int64_t off0 = (int64_t)slot * 2 * S, off1 = off0 + S;
+    // curr into level 1, then prev = curr - (curr - prev) into level 0
+    if (rv_prec_ == 1) {
+        k_ck_dequant<__nv_bfloat16><<<grd, 256, 0, s>>>(rv_store_.as<__nv_bfloat16>() + off0, n, sc0, nullptr, lev + S);
+        k_ck_dequant<__nv_bfloat16><<<grd, 256, 0, s>>>(rv_store_.as<__nv_bfloat16>() + off1, n, sc1, lev + S, lev);
+    } else {
+        k_ck_dequant<__half><<<grd, 256, 0, s>>>(rv_store_.as<__half>() + off0, n, sc0, nullptr, lev + S);
+        k_ck_dequant<__half><<<grd, 256, 0, s>>>(rv_store_.as<__half>() + off1, n, sc1, lev + S, lev);
+    }
+    CK(cudaGetLastError());
+}
+
+// d chain steps (d*sub time steps) on the recomputation levels from state rv_pos_.
+void Engine::rv_advance(int d)
+{
     std::swap(fields_, rec_fields_);
     const int rot_save = rot_;
-    rot_ = 0;
-    const float *c = ckpt_.as<float>() + (int64_t)j * 2 * S;
-    CK(cudaMemcpyAsync(level(0), c, sizeof(float) * S, cudaMemcpyDeviceToDevice, s));
-    CK(cudaMemcpyAsync(level(1), c + S, sizeof(float) * S, cudaMemcpyDeviceToDevice, s));
+    const bool graphs_save = graphs_;
+    rot_ = rv_rot_;
     no_extract_ = true;
-    auto keep = [&](int k) {
-        CK(cudaMemcpyAsync(snaps_.as<float>() + (int64_t)(k - lo) * S, level(1), sizeof(float) * S,
-                           cudaMemcpyDeviceToDevice, s));
-    };
-    for (int it = lo * pb_.sub; it < hi * pb_.sub; it++) {
-        if (it % pb_.sub == 0) keep(it / pb_.sub);
-        run(it, 1);
-    }
-    keep(hi);
+    graphs_ = false;  // the levels swap in and out: plain launches
+    run(rv_pos_ * pb_.sub, d * pb_.sub);
+    graphs_ = graphs_save;
     no_extract_ = false;
+    rv_rot_ = rot_;
     rot_ = rot_save;
     std::swap(fields_, rec_fields_);
-    seg_cur_ = j;
-    seg_lo_ = lo;
+    rv_pos_ += d;
+    rv_steps_ += d;
+}
+
+// Brings the recomputation levels to state t, below every state visited so
+// far: drops the checkpoints above t, restores the highest remaining one and
+// advances, keeping the states where the schedule splits the remaining
+// interval while free slots last.
+void Engine::rv_goto(int t)
+{
+    if (rv_pos_ == t) return;
+    while (rv_pos_stack_.size() > 1 && rv_pos_stack_.back() > t) {
+        rv_free_.push_back(rv_slot_stack_.back());
+        rv_pos_stack_.pop_back();
+        rv_slot_stack_.pop_back();
+    }
+    if (rv_pos_ < rv_pos_stack_.back() || rv_pos_ > t) {
+        rv_restore(rv_slot_stack_.back());
+        rv_pos_ = rv_pos_stack_.back();
+    }
+    const RevolveTable &T = revolve_table(rv_K_, rv_C_);
+    const int W = rv_C_ + 1;
+    const int64_t lv = (int64_t)pb_.nshots * pb_.ncomp() * pb_.nxyz();
+    while (rv_pos_ < t) {
+        const int c = (int)rv_free_.size(), l = t - rv_pos_;
+        const int d = c == 0 ? l : T.split[(size_t)l * W + std::min(c, rv_C_)];
+        rv_advance(d);
+        if (rv_pos_ < t && !rv_free_.empty()) {
+            const int slot = rv_free_.back();
+            rv_free_.pop_back();
+            rv_store(slot, rec_fields_.as<float>() + (rv_rot_ % 3) * lv,
+                     rec_fields_.as<float>() + ((rv_rot_ + 1) % 3) * lv);
+            rv_pos_stack_.push_back(rv_pos_);
+            rv_slot_stack_.push_back(slot);
+        }
+    }
 }
 
 void Engine::forward(const InjTable &inj, int ntrace, const float *src, const ExtTable &ext, float *rcv, bool store)
@@ -1494,8 +1703,13 @@ void Engine::forward(const InjTable &inj, int ntrace, const float *src, const Ex
     snaps_valid_ = false;
     nwritten_ = 0;
     const bool keep = store && pb_.sub > 0;
-    seg_L_ = 0;
-    seg_cur_ = -1;
+    rv_C_ = 0;
+    rv_pos_ = -1;
+    rv_pos_stack_.clear();
+    rv_slot_stack_.clear();
+    rv_free_.clear();
+    rv_mark_.clear();
+    ring_[0] = ring_[1] = ring_[2] = -1;
     if (keep) {
         nsnap_ = 1 + pb_.nt / pb_.sub;
         // FP16P needs at least three stored snapshots to decode backwards
@@ -1503,34 +1717,50 @@ void Engine::forward(const InjTable &inj, int ntrace, const float *src, const Ex
         if (storage_ == STORE_FP16P && written < 3) storage_ = STORE_FP32;
         const int64_t S = (int64_t)sizeof(float) * nsc * n;  // one snapshot of the batch
         const int64_t full = storage_ == STORE_FP32 ? nsnap_ * S : nsnap_ * S / 2 + 8 * S;
-        if (budget_ > 0 && full > budget_) {
-            // segments of L snapshots: nseg FP32 checkpoints (2 levels), an
-            // (L+2)-snapshot buffer, recomputation levels and a zero snapshot
-            int bestL = 0;
-            int64_t best = 0;
-            for (int L = 2; L <= written; L++) {
-                const int ns = (written + L - 1) / L;
-                const int64_t mem = (2 * (int64_t)ns + L + 2 + 3 + 1) * S;
-                if (bestL == 0 || mem < best) {
-                    best = mem;
-                    bestL = L;
-                }
-            }
-            if (best > budget_)
+        // checkpoint slot bytes (two levels) and the fixed part: recomputation
+        // levels, FP32 ring of three snapshots, zero snapshot
+        const int64_t slot_bytes = rv_prec_ == 0 ? 2 * S : S;
+        const int64_t fixed = 7 * S;
+        int C = 0;
+        if (rv_C_req_ > 0) {
+            C = rv_C_req_;
+        } else if (budget_ > 0 && full > budget_) {
+            if (budget_ < fixed + 2 * slot_bytes)
                 throw FwiError(FWI_ERR_OOM, "snapshot budget of " + std::to_string(budget_) +
-                                                " bytes is below the checkpointing minimum of " + std::to_string(best));
-            seg_L_ = bestL;
-            nseg_ = (written + bestL - 1) / bestL;
+                                                " bytes is below the checkpointing minimum of " +
+                                                std::to_string(fixed + 2 * slot_bytes));
+            C = (int)std::min<int64_t>((budget_ - fixed) / slot_bytes, written);
+        }
+        if (C > 0) {
+            // binomial checkpointing over the chain 0..K; slot 0 keeps state 0
+            rv_K_ = written - 1;
+            // more slots than states, or than 256 (the schedule's table grows with them), gain nothing here
+            rv_C_ = std::max(1, std::min({C, std::max(1, rv_K_), 256}));
             snapq_.alloc(0);
             snaps_scale_.alloc(0);
             enc_.alloc(0);
-            ckpt_.alloc((size_t)nseg_ * 2 * S);
+            rv_store_.alloc((size_t)rv_C_ * slot_bytes);
+            rv_scale_.alloc(rv_prec_ == 0 ? 0 : sizeof(float) * 2 * (size_t)rv_C_ * nsc);
+            amax_.alloc(sizeof(unsigned) * (size_t)nsc);
             rec_fields_.alloc(3 * (size_t)S);
-            snaps_.alloc((size_t)(seg_L_ + 2) * S);
+            snaps_.alloc(3 * (size_t)S);
             snapz_.alloc((size_t)S);
             snapz_.zero(s);
+            for (int k = rv_C_ - 1; k >= 0; k--) rv_free_.push_back(k);
+            // the forward sweep keeps state 0 and the splits of the schedule's first descent
+            rv_mark_.assign(rv_K_ + 1, 0);
+            rv_mark_[0] = 1;
+            const RevolveTable &T = revolve_table(rv_K_, rv_C_);
+            int p = 0, c = rv_C_ - 1;
+            while (c > 0 && p < rv_K_) {
+                p += T.split[(size_t)(rv_K_ - p) * (rv_C_ + 1) + c];
+                if (p >= rv_K_) break;
+                rv_mark_[p] = 1;
+                c--;
+            }
         } else if (storage_ == STORE_FP32) {
-            ckpt_.alloc(0);
+            rv_store_.alloc(0);
+            rv_scale_.alloc(0);
             rec_fields_.alloc(0);
             snapq_.alloc(0);
             snaps_scale_.alloc(0);
@@ -1539,7 +1769,8 @@ void Engine::forward(const InjTable &inj, int ntrace, const float *src, const Ex
             snaps_.alloc(sizeof(float) * (size_t)nsnap_ * nsc * n);
             snaps_.zero(s);
         } else {
-            ckpt_.alloc(0);
+            rv_store_.alloc(0);
+            rv_scale_.alloc(0);
             rec_fields_.alloc(0);
             snaps_.alloc(sizeof(float) * 3 * (size_t)nsc * n);
             snapq_.alloc(sizeof(__half) * (size_t)nsnap_ * nsc * n);
@@ -1557,7 +1788,16 @@ void Engine::forward(const InjTable &inj, int ntrace, const float *src, const Ex
         run(it, 1);
     }
     if (keep && (pb_.nt - 1) % pb_.sub == 0) snap_store((pb_.nt - 1) / pb_.sub);
-    if (keep && seg_L_ == 0 && storage_ == STORE_FP16P) {
+    if (keep && rv_C_ > 0 && (pb_.nt - 1) % pb_.sub == 0) {
+        // the last state stays available: the recomputation levels start from it
+        const int64_t S = (int64_t)nsc * n;
+        CK(cudaMemcpyAsync(rec_fields_.as<float>(), level(0), sizeof(float) * S, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(rec_fields_.as<float>() + S, level(1), sizeof(float) * S, cudaMemcpyDeviceToDevice, s));
+        rv_rot_ = 0;
+        rv_pos_ = rv_K_;
+    }
+    rv_steps_ = 0;
+    if (keep && rv_C_ == 0 && storage_ == STORE_FP16P) {
         // decoder starts from the encoder's final state (e_K, e_{K-1})
         const int K = nwritten_ - 1;
         const double *e = enc_.as<double>();
@@ -1799,10 +2039,6 @@ void Engine::image(int itl, const float *curr, const float *prevl)
     a.itl = itl;
     a.last = pb_.nt / pb_.sub;
     for (int k = 0; k < pb_.nmodels; k++) a.m[k] = model_.as<float>() + k * n;
-    if (seg_L_ > 0) {
-        const int j = std::min(itl / seg_L_, nseg_ - 1);
-        if (j != seg_cur_) recompute_segment(j);
-    }
     const float *lev[3];
     for (int l = 0; l < 3; l++) {
         const int k = itl - 1 + l;
@@ -1868,8 +2104,8 @@ void Engine::adjoint_impl(const InjTable &inj, int ntrace, const float *adj_src,
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(grad, gf.p, gf.bytes, cudaMemcpyDeviceToHost, s));
     sync();
-    snaps_valid_ = seg_L_ > 0 || storage_ == STORE_FP32;  // the FP16P decoder state is consumed
-    seg_cur_ = -1;
+    // the FP16P decoder state and the checkpoint stack are consumed by the adjoint
+    snaps_valid_ = rv_C_ == 0 && storage_ == STORE_FP32;
 }
 
 // ---------------------------------------------------------------------------

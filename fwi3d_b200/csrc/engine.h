@@ -118,11 +118,19 @@ public:
     enum Storage { STORE_FP32 = 0, STORE_FP16P = 1 };
     void set_storage(int mode) { storage_ = mode; }
     // HBM budget of the forward-wavefield storage of the gradient path (bytes,
-    // 0: unlimited).  When full storage exceeds it, the forward keeps FP32
-    // checkpoints every L snapshots and the adjoint recomputes one segment of
-    // snapshots at a time from them (one extra forward propagation).
+    // 0: unlimited).  When full storage exceeds it, binomial checkpointing
+    // (below) replaces it with as many checkpoint slots as fit the budget.
     void set_snapshot_budget(int64_t bytes) { budget_ = bytes; }
-    int checkpoint_segment() const { return seg_L_; }  // 0: full storage
+    // Binomial checkpointing (the schedule of Griewank and Walther's revolve):
+    // `slots` restart states (prev, curr) of the batch held on the device,
+    // stored in FP32 (precision 0) or per-(state, level, shot, component)
+    // scaled BF16 (1) or FP16 (2); the adjoint recomputes the forward states
+    // it needs from them, placing new checkpoints on the way so that the
+    // number of recomputed steps is the minimum for that many slots.
+    // slots 0: full storage unless the budget forces checkpointing.
+    void set_checkpointing(int slots, int precision) { rv_C_req_ = slots; rv_prec_ = precision; }
+    int checkpoint_slots() const { return rv_C_; }        // 0: full storage
+    int64_t recomputed_steps() const { return rv_steps_; }  // chain steps recomputed by the last adjoint
     // forward: full time loop; keeps snapshots when store && sub > 0.  Tables of
     // all shots (as set_sources/set_receivers); rcv [nshots][ncomp][nr][nt].
     void forward(const InjTable &inj, int ntrace, const float *src, const ExtTable &ext, float *rcv, bool store);
@@ -140,7 +148,11 @@ private:
     void adjoint_impl(const InjTable &inj, int ntrace, const float *adj_src, const float *adj_src_dev, float *grad);
 
 public:
-    int64_t snapshot_bytes() const { return snaps_.bytes + snapq_.bytes + enc_.bytes + snapz_.bytes + ckpt_.bytes + rec_fields_.bytes; }
+    int64_t snapshot_bytes() const
+    {
+        return snaps_.bytes + snapq_.bytes + enc_.bytes + snapz_.bytes + rv_store_.bytes + rv_scale_.bytes +
+               rec_fields_.bytes;
+    }
 
     // Diagnostic timing of the step's main kernel (the fused interior kernel,
     // else the per-point step kernel): a pair of CUDA events on the engine
@@ -184,15 +196,26 @@ private:
     int dec_lo_ = 0;               // FP16P decoder: state holds snapshots dec_lo_, dec_lo_+1
     void snap_store(int k);
     int64_t budget_ = 0;
-    int seg_L_ = 0;                // checkpointing: snapshots per segment (0: full storage)
-    int nseg_ = 0;
-    int seg_cur_ = -1;             // segment held in snaps_ (snapshots seg_lo_ .. seg_lo_ + L + 1)
-    int seg_lo_ = 0;
-    DevBuf ckpt_;                  // [nseg][2][nshots][ncomp][nxyz] (prev, curr) at each segment start
+    // binomial checkpointing over the chain of snapshot states 0..rv_K_
+    // (state k: the time levels (prev, curr) at step k*sub)
+    int rv_C_req_ = 0, rv_prec_ = 0;
+    int rv_C_ = 0;                 // slots in use for this forward (0: full storage)
+    int rv_K_ = 0;
+    int rv_pos_ = -1;              // state held by the recomputation levels (-1: none)
+    int rv_rot_ = 0;               // their rotation
+    std::vector<int> rv_pos_stack_, rv_slot_stack_, rv_free_;  // checkpoints (positions increase up the stack)
+    std::vector<int> rv_mark_;     // forward sweep: 1 where a checkpoint is taken
+    const int32_t *rv_split_ = nullptr;  // optimal first advance for (length, free slots)
+    int64_t rv_steps_ = 0;
+    int ring_[3] = {-1, -1, -1};   // snapshot index held by each slot of the FP32 ring (snaps_)
+    DevBuf rv_store_;              // [C][2 levels][nshots][ncomp][nxyz], FP32 or 16-bit
+    DevBuf rv_scale_;              // [C][2][nshots*ncomp] scales of the 16-bit slots
     DevBuf rec_fields_;            // time levels of the recomputation
     bool no_extract_ = false;
-    int ckpt_index(int j) const { return j == 0 ? 0 : j * seg_L_ - 1; }
-    void recompute_segment(int j);
+    void rv_store(int slot, const float *prev, const float *curr);
+    void rv_restore(int slot);
+    void rv_advance(int d);        // recomputation levels: d chain steps forward
+    void rv_goto(int t);           // recomputation levels to state t (t below the last visited)
     const float *snap_fp32(int kk);  // FP32 view of snapshot kk (decoding as needed)
     bool snaps_valid_ = false;
     DevBuf grad_;                  // [3][nxyz] double

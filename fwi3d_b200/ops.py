@@ -80,6 +80,8 @@ def to_cparam(p: Param) -> _lib.CParam:
     c.soft_clip, c.verbose = int(bool(p.soft_clip)), p.verbose
     c.snapshot_storage = int(getattr(p, "snapshot_storage", 0))
     c.snapshot_budget_gb = float(getattr(p, "snapshot_budget_gb", 0.0))
+    c.checkpoint_slots = int(getattr(p, "checkpoint_slots", 0))
+    c.checkpoint_precision = int(getattr(p, "checkpoint_precision", 0))
     return c
 
 

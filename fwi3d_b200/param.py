@@ -92,9 +92,15 @@ class Param:
     # gradient snapshot storage (no reference counterpart): 0 FP32, 1 FP16
     # second-difference residuals with per-snapshot scales
     snapshot_storage: int = 0
-    # HBM budget of that storage in GB (0: unlimited); above it, checkpoints
-    # and segment recomputation
+    # HBM budget of that storage in GB (0: unlimited); above it, binomial
+    # checkpointing with as many slots as fit
     snapshot_budget_gb: float = 0.0
+    # binomial checkpointing (no reference counterpart): > 0 restart states
+    # (prev, curr) kept on the device, whatever the budget; their storage
+    # 0 FP32, 1 BF16, 2 FP16 (16-bit forms scaled per state, level, shot and
+    # component by the field's max |value|)
+    checkpoint_slots: int = 0
+    checkpoint_precision: int = 0
 
     def copy(self) -> "Param":
         return copy.deepcopy(self)

@@ -74,7 +74,12 @@ typedef struct fwi_param {
     int snapshot_storage;     /* gradient snapshots: 0 FP32 (as the reference), 1 FP16 second-difference
                                  residuals with per-snapshot scales (half the memory); no reference counterpart */
     float snapshot_budget_gb; /* HBM budget of the gradient's forward-wavefield storage (0: unlimited); above it
-                                 FP32 checkpoints + segment recomputation replace full storage */
+                                 binomial checkpointing with as many slots as fit replaces full storage */
+    int checkpoint_slots;     /* > 0: binomial checkpointing (Griewank-Walther revolve schedule) with this many
+                                 restart states (prev, curr) on the device, whatever the budget; no reference
+                                 counterpart (the reference keeps every snapshot, zfpWrapper.hpp:24-116) */
+    int checkpoint_precision; /* checkpoint storage: 0 FP32, 1 BF16, 2 FP16, the 16-bit forms scaled per
+                                 (state, level, shot, component) by the field's max |value| */
 } fwi_param;
 
 void fwi_param_default(fwi_param *p);
