@@ -89,9 +89,10 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def traffic_per_update():
-    """DRAM bytes per grid-point update of the step kernels, from the committed
-    ncu summary (profiles/ncu_traffic.txt: key=value lines)."""
+def traffic_per_update(physics):
+    """DRAM bytes per grid-point update of the step's main kernels for one
+    physics, from the committed ncu summary (profiles/ncu_traffic.txt:
+    `<physics>.<key>=value` lines): (bytes per update, kernel name)."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
     try:
         vals = {}
@@ -100,7 +101,7 @@ def traffic_per_update():
                 if "=" in line and not line.startswith("#"):
                     k, v = line.strip().split("=", 1)
                     vals[k.strip()] = v.strip()
-        return float(vals["dram_bytes_per_update"]), vals.get("kernel", "")
+        return float(vals[f"{physics}.dram_bytes_per_update"]), vals.get(f"{physics}.kernel", "")
     except Exception:
         return None, ""
 
@@ -169,16 +170,26 @@ def max_over_ranks(value, world, device=None):
     return float(t.item())
 
 
-def cpu_reference(n_steps, threads, n=256, physics="elastic"):
+def cpu_reference(n_steps, threads, n=256, physics="elastic", short=10):
     """Reference CPU code (oracle/_ref, built from the reference sources): one
-    shot of the workload over an n_steps window; returns pt-updates/s."""
+    shot of the workload, timed over a `short`-step and an `n_steps`-step
+    window of the unmodified apply_forward; the difference is the time of
+    n_steps - short steps of its propagate() loop, so model analysis and
+    set-up (timed separately) are not in the rate.  Returns (pt-updates/s,
+    seconds per step, set-up seconds)."""
     from oracle import refpy
 
-    sv = workload(n=n, nshots=1, nsteps=n_steps, physics=physics)
-    t0 = time.perf_counter()
-    refpy.modeling(sv, shot=0, precision="fp32", nthreads=threads)
-    dt = time.perf_counter() - t0
-    return sv.nxyz * n_steps / dt, dt
+    def timed(k):
+        sv = workload(n=n, nshots=1, nsteps=k, physics=physics)
+        t0 = time.perf_counter()
+        refpy.modeling(sv, shot=0, precision="fp32", nthreads=threads)
+        return sv.nxyz, time.perf_counter() - t0
+
+    n_steps = max(n_steps, short + 4)
+    _, t1 = timed(short)
+    nxyz, t2 = timed(n_steps)
+    per_step = max(t2 - t1, 1e-9) / (n_steps - short)
+    return nxyz / per_step, per_step, max(0.0, t1 - short * per_step)
 
 
 def grid_label(sv):
@@ -202,21 +213,23 @@ def run_reference(args, rank, world):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    k = max(10, min(args.steps, args.ref_cap))  # the reference needs nt >= 10 (we_op.cpp:621, 838)
+    k = max(20, min(args.steps, args.ref_cap))  # the reference needs nt >= 10 (we_op.cpp:621, 838)
     if args.warmup > 0:
-        cpu_reference(10, threads, n=args.n, physics=args.physics)
-    value, secs = cpu_reference(k, threads, n=args.n, physics=args.physics)
+        cpu_reference(14, threads, n=args.n, physics=args.physics, short=10)
+    value, per_step, setup = cpu_reference(k, threads, n=args.n, physics=args.physics)
     sv = workload(n=args.n, nshots=1, nsteps=k, physics=args.physics)
-    sample = (f"1 shot of the {grid_label(sv)} {args.physics} workload, {k}-step window, whole apply_forward call "
-              f"(model analysis and setup included), OMP threads={threads}")
+    sample = (f"1 shot of the {grid_label(sv)} {args.physics} workload: the unmodified apply_forward timed over a "
+              f"10-step and a {k}-step window, rate from the difference ({k - 10} steps of propagate(); set-up "
+              f"{setup:.2f} s excluded), OMP threads={threads}")
     line = {
         "impl": "reference", "metric": "grid-pt updates/s", "value": value, "unit": "pt/s", "n_gpus": args.gpus,
-        "steps": k, "warmup": args.warmup, "ms_per_step": secs * 1e3 / k, "higher_is_better": True,
+        "steps": k - 10, "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": workload_label(args.physics, sv, PHYSICS[args.physics]["shots"], len(sv.par.rxyz[0]))
                    + " (CPU: 1-shot bounded window)",
                    "grid": [sv.nx, sv.ny, sv.nz], "shots": PHYSICS[args.physics]["shots"], "parallelism": "cpu"},
-        "cpu_baseline": {"value": value, "unit": "pt/s", "cores": threads, "kind": "reference", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": "pt/s", "cores": threads, "kind": "reference", "sample": sample,
+                         "setup_s": setup},
         "e2e": {"value": value, "unit": "pt/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -290,7 +303,7 @@ def run_ours(args, rank, world, local):
     kernel = (k_name.value or b"").decode()
     achieved = bpu * k_pts.value / (launch_ms * 1e-3) / 1e9 if k_n.value else None
     step_gbs = bpu * units_per_step / (ms_step / 1e3) / 1e9
-    tpu, tkernel = traffic_per_update()
+    tpu, tkernel = traffic_per_update(args.physics)
 
     # e2e through the public C-ABI call, host buffers, 300-step time axis
     e2e = None
@@ -320,10 +333,12 @@ def run_ours(args, rank, world, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        v, secs = cpu_reference(args.cpu_steps, threads, n=args.n, physics=args.physics)
-        cpu = {"value": v, "unit": "pt/s", "cores": threads, "kind": "reference",
+        v, per_step, setup = cpu_reference(args.cpu_steps, threads, n=args.n, physics=args.physics)
+        cpu = {"value": v, "unit": "pt/s", "cores": threads, "kind": "reference", "setup_s": setup,
                "sample": f"reference CPU build, 1 shot of the {grid_label(sv)} {args.physics} workload, "
-                         f"{args.cpu_steps}-step window ({secs:.1f} s, setup included), OMP threads={threads}"}
+                         f"apply_forward over 10- and {max(args.cpu_steps, 14)}-step windows, rate from the "
+                         f"difference ({per_step:.3f} s per step; set-up {setup:.2f} s excluded), "
+                         f"OMP threads={threads}"}
 
     if rank == 0:
         line = {
@@ -347,6 +362,13 @@ def run_ours(args, rank, world, local):
                                  "kernel of the step"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(lps.value) * args.steps, "clocks": clk,
         }
+        # the configuration's other two measures, run after the timed modeling
+        # region: FWI gradients/hour and the serving mix's p50/p99
+        if world == 1 and not args.no_gradient:
+            line["gradient"] = gradient_block(args.n_grad, args.steps_grad, args.shots_side, args.grad_batch,
+                                              device=local)
+        if world == 1 and not args.no_serving:
+            line["serving"] = serving_block(args.requests, args.rate, device=local)
         print(json.dumps(line), flush=True)
     return 0
 
@@ -362,20 +384,33 @@ def gradient_survey(n, nsteps, nside):
     return sv
 
 
-def run_gradient(args):
-    """FWI gradients/hour: the per-shot operator path with FP32 snapshots (the
-    drop-in form of the reference's loop) against the device objective with
-    shots batched in lockstep and FP16 second-difference snapshots."""
+def gradient_block(n, nsteps, nside, batch, slots_plain=40, free_frac=0.8, device=0):
+    """FWI gradients/hour on the elastic FWI configuration (n^3, 10 m, dt 1 ms,
+    nsteps steps, nside^2 shots, 100x100-class receivers).  Full storage of the
+    forward wavefield does not fit (FP32: 96 MB per state per shot at 200^3),
+    so both forms checkpoint with FP32 restart states (exact recomputation):
+      plain: the per-shot operator (forward + jacobianT, one shot per call, as
+             a caller of the reference's operator API runs it) with
+             `slots_plain` checkpoint slots;
+      batched: the device objective with `batch` shots advancing in lockstep
+             and as many checkpoint slots as fit `free_frac` of free HBM,
+             residual, adjoint sources and FP64 sums on the device.
+    Both are timed on the first `batch` shots; shots are independent and of
+    equal cost, so gradients/hour scale by nside^2 / batch.  The gradient of
+    the batched form is compared with the sum of the plain per-shot ones
+    (normalised the same way)."""
     import torch
 
     from fwi3d_b200 import ops, synth
 
-    n, nsteps, nside = args.n_grad, args.steps_grad, args.shots_side
     sv = gradient_survey(n, nsteps, nside)
-    ns = len(sv.par.sxyz)
+    ns_all = len(sv.par.sxyz)
+    sv.par.sxyz = sv.par.sxyz[:batch]
+    sv.par.rxyz = sv.par.rxyz[:batch]
+    sv.par.ns = batch
     true = synth.Survey(sv.name, 3, sv.nx, sv.ny, sv.nz, sv.dx, sv.dy, sv.dz, sv.extra["true_model"], sv.wavelet,
                         sv.dt_data, sv.par.copy())
-    obs = ops.forward_batch(true)
+    obs = ops.forward_batch(true, device=device)
     model = np.ascontiguousarray(sv.model, dtype=np.float32)
     dt = sv.dt_data
     dnorm = float(np.sum(obs.astype(np.float64) ** 2)) * dt
@@ -386,87 +421,88 @@ def run_gradient(args):
         a[..., -1] = (r[..., -1].astype(np.float64) * 0.5 * dt).astype(np.float32)
         return a
 
-    def plain():
-        g = np.zeros((3,) + model.shape[1:], dtype=np.float64)
-        f = 0.0
-        for s in range(ns):
-            op = ops.from_survey(sv, s)
-            r = op.forward(False, model) - obs[s]
-            rr = r.astype(np.float64)
-            f += np.sum(rr ** 2) - 0.5 * np.sum(rr[..., 0] ** 2 + rr[..., -1] ** 2)
-            g += op.jacobianT(False, None, model, ht(r))
-            op.close()
-        return 0.5 * dt * f / dnorm, g / dnorm
-
-    torch.cuda.synchronize()
+    # plain: per-shot operators, FP32 checkpoints
+    sp = sv.par.copy()
+    sp.checkpoint_slots = slots_plain
+    svp = synth.Survey(sv.name, 3, sv.nx, sv.ny, sv.nz, sv.dx, sv.dy, sv.dz, model, sv.wavelet, dt, sp)
+    torch.cuda.synchronize(device)
     t0 = time.perf_counter()
-    f_plain, g_plain = plain()
+    g_plain = np.zeros((3,) + model.shape[1:], dtype=np.float64)
+    for s in range(batch):
+        op = ops.from_survey(svp, s, device=device)
+        r = op.forward(False, model) - obs[s]
+        g_plain += op.jacobianT(False, None, model, ht(r))
+        op.close()
     t_plain = time.perf_counter() - t0
+    g_plain /= dnorm
 
-    sv.par.snapshot_storage = 1
-    obj = ops.FwiObjective(sv, obs, batch=args.grad_batch)
-    obj.evaluate(model)  # warm-up (engine creation, allocation)
+    # batched: device objective, checkpoint slots sized to the free memory
+    free, _ = torch.cuda.mem_get_info(device)
+    sv.par.snapshot_budget_gb = free_frac * free / 1e9
+    obj = ops.FwiObjective(sv, obs, batch=batch, device=device)
+    torch.cuda.synchronize(device)
     t0 = time.perf_counter()
     f_b, g_b = obj.evaluate(model)
     t_b = time.perf_counter() - t0
-    diff = float(np.linalg.norm(g_b - g_plain) / np.linalg.norm(g_plain))
-
-    cpu = None
-    if not args.no_cpu:
-        from oracle import refpy
-
-        k = 12  # the reference divides by nt/10 in its time loop (we_op.cpp:621, 838): nt must be >= 10
-        svc = gradient_survey(n, k, nside)
-        rng = np.random.default_rng(0)
-        d, _ = refpy.modeling(svc, shot=0, precision="fp32", nthreads=os.cpu_count() or 1)
-        adj = (rng.standard_normal(d.shape) * np.abs(d).max()).astype(np.float32)
-        t0 = time.perf_counter()
-        refpy.forward_jacobianT(svc, adj, shot=0, precision="fp32", nthreads=os.cpu_count() or 1)
-        tc = time.perf_counter() - t0
-        sec_per_grad = tc * (nsteps / k) * ns
-        cpu = {"value": 3600.0 / sec_per_grad, "unit": "gradients/h", "cores": os.cpu_count() or 1,
-               "kind": "reference",
-               "sample": f"reference CPU build, 1 shot forward+jacobianT on the {n}^3 grid over a {k}-step time "
-                         f"axis ({tc:.1f} s), scaled by {nsteps}/{k} steps x {ns} shots"}
-    line = {
-        "metric": "FWI gradients/hour", "value": 3600.0 / t_b, "unit": "gradients/h", "n_gpus": 1, "steps": 1,
-        "warmup": 1, "ms_per_step": t_b * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 stencils, FP16 snapshots, FP64 sums", "data": "synthetic (seeded layered model + 3 anomalies)",
-        "config": {"workload": f"elastic FWI gradient {n}^3, 10 m, dt 1 ms, {nsteps} steps, {ns} shots "
-                               f"({nside}x{nside}), 2-point receiver stride, sub 1",
-                   "batch": args.grad_batch, "storage": "FP16 second-difference residuals"},
-        "plain": {"value": 3600.0 / t_plain, "unit": "gradients/h", "seconds": t_plain,
-                  "form": "per-shot operator (forward + jacobianT), FP32 snapshots"},
+    dev_bytes = obj.device_bytes()
+    obj.close()
+    diff = float(np.linalg.norm(g_b - g_plain) / max(np.linalg.norm(g_plain), 1e-30))
+    scale = ns_all / batch
+    return {
+        "metric": "FWI gradients/hour", "value": 3600.0 / (t_b * scale), "unit": "gradients/h",
+        "workload": f"elastic FWI gradient {n}^3, 10 m, dt 1 ms, {nsteps} steps, {ns_all} shots "
+                    f"({nside}x{nside}), 2-point receiver stride, sub 1; timed on {batch} shots, scaled by "
+                    f"{ns_all}/{batch}",
+        "form": f"device objective, {batch} shots per launch, FP32 restart checkpoints (binomial schedule) in "
+                f"{free_frac:.0%} of free HBM, FP64 misfit and gradient sums",
+        "seconds_per_batch": t_b, "device_bytes": dev_bytes,
+        "plain": {"value": 3600.0 / (t_plain * scale), "unit": "gradients/h", "seconds_per_batch": t_plain,
+                  "form": f"per-shot operator (forward + jacobianT), FP32 restart checkpoints, {slots_plain} slots"},
         "speedup_vs_plain": t_plain / t_b,
-        "misfit": f_b, "misfit_plain": f_plain,
         "gradient_rel_l2_vs_plain": diff,
-        "cpu_baseline": cpu,
-        "device_bytes": obj.device_bytes(),
+        "misfit": f_b,
     }
+
+
+def serving_block(nreq, rate, device=0):
+    """Serving mix shaped like the serving configuration, scaled to a bounded
+    run: Poisson arrivals, six models of the three physics at uneven grids,
+    modeling and gradient shots; throughput and p50/p99 latency (service and
+    queueing reported apart)."""
+    from fwi3d_b200 import servemix, serving
+
+    models, reqs = servemix.make_mix(nreq=nreq, rate=rate, seed=5, grids=servemix.BENCH_GRIDS,
+                                     steps=servemix.BENCH_STEPS, rec=servemix.BENCH_REC, p_gradient=0.25)
+    srv = serving.Server(models, chunk=100, max_batch=8, gradient_workers=2)
+    rep = srv.run(reqs)
+    s = rep.summary()
+    return {
+        "metric": "serving grid-pt updates/s", "value": s["gpt_per_s"] * 1e9, "unit": "pt/s",
+        "workload": f"{nreq} requests (of the configuration's 512), Poisson {rate}/s, acoustic/elastic/VTI x 2 models, "
+                    f"grids {servemix.BENCH_GRIDS}, steps {servemix.BENCH_STEPS}, 8-15 Hz, receiver lines "
+                    f"{servemix.BENCH_REC}, 25 % gradients (FP32 checkpoints)",
+        "requests_per_s": s["requests_per_s"], "p50_s": s["p50_s"], "p99_s": s["p99_s"],
+        "service_p50_s": s["service_p50_s"], "service_p99_s": s["service_p99_s"],
+        "queue_p50_s": s["queue_p50_s"], "queue_p99_s": s["queue_p99_s"], "makespan_s": s["seconds"],
+        "latency_unit": "s",
+    }
+
+
+def run_gradient(args):
+    line = gradient_block(args.n_grad, args.steps_grad, args.shots_side, args.grad_batch)
+    line.update({"n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": line["seconds_per_batch"] * 1e3,
+                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                 "dtype": "f32 stencils, FP32 checkpoints, FP64 sums",
+                 "data": "synthetic (seeded layered model + 3 anomalies)", "config": {"workload": line["workload"]}})
     print(json.dumps(line), flush=True)
     return 0
 
 
 def run_serving(args):
-    """Serving mix: Poisson arrivals of modeling and gradient shots on six
-    models (acoustic, elastic, VTI at uneven grids); throughput and p50/p99
-    latency of the continuous-batching loop."""
-    from fwi3d_b200 import servemix, serving
-
-    models, reqs = servemix.make_mix(nreq=args.requests, rate=args.rate, seed=5)
-    srv = serving.Server(models, chunk=50, max_batch=8, gradient_workers=2)
-    rep = srv.run(reqs)
-    s = rep.summary()
-    line = {
-        "metric": "serving grid-pt updates/s", "value": s["gpt_per_s"] * 1e9, "unit": "pt/s", "n_gpus": 1,
-        "steps": 1, "warmup": 0, "ms_per_step": s["seconds"] * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded request mix)",
-        "config": {"workload": f"{args.requests} requests, Poisson {args.rate}/s, acoustic/elastic/VTI x 2 models, "
-                               "grids 64^3..128x112x96, 200-400 steps, 8-15 Hz, 16^2-24^2 receivers, 25 % gradients",
-                   "admission": "device bytes vs 90 % of free HBM", "chunk_steps": 50, "max_batch": 8},
-        "requests_per_s": s["requests_per_s"], "p50_s": s["p50_s"], "p99_s": s["p99_s"],
-        "latency_unit": "s", "makespan_s": s["seconds"],
-    }
+    line = serving_block(args.requests, args.rate)
+    line.update({"n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": line["makespan_s"] * 1e3,
+                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                 "data": "synthetic (seeded request mix)", "config": {"workload": line["workload"]}})
     print(json.dumps(line), flush=True)
     return 0
 
@@ -479,7 +515,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-steps", type=int, default=16)
+    ap.add_argument("--cpu-steps", type=int, default=30)
     ap.add_argument("--ref-cap", type=int, default=40, help="max time steps of the CPU reference window")
     ap.add_argument("--physics", default="elastic", choices=sorted(PHYSICS),
                     help="modeling workload: elastic 256^3 x 8 shots (default), acoustic 101^3 x 1, "
@@ -487,10 +523,12 @@ def main():
     ap.add_argument("--n", type=int, default=None, help="grid points per axis (profiling runs use smaller grids)")
     ap.add_argument("--shots", type=int, default=None)
     ap.add_argument("--workload", default="modeling", choices=["modeling", "gradient", "serving"])
-    ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--requests", type=int, default=24)
     ap.add_argument("--rate", type=float, default=20.0)
     ap.add_argument("--n-grad", type=int, default=200)
-    ap.add_argument("--steps-grad", type=int, default=500)
+    ap.add_argument("--steps-grad", type=int, default=2500)
+    ap.add_argument("--no-gradient", action="store_true", help="skip the gradients/hour block of the default line")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving block of the default line")
     ap.add_argument("--shots-side", type=int, default=4)
     ap.add_argument("--grad-batch", type=int, default=4)
     args = ap.parse_args()

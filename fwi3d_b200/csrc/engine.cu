@@ -1016,7 +1016,8 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         fz_interior_range(pb_.nx, fz::TX, xl, xh);
         const bool el = pb_.nmodels == 3;
         const bool split = fused_split_active();
-        kmark(true, "k_elastic_fused", (int64_t)(f.y1 - f.y0) * pb_.nx * pb_.nz * pb_.nshots);
+        kmark(true, el && pair_ ? "k_elastic_pair" : "k_elastic_fused",
+              (int64_t)(f.y1 - f.y0) * pb_.nx * pb_.nz * pb_.nshots);
         if (el && pair_) {
             // paired kernel: edge tiles (all of them when no tile is interior), then interior tiles
             const int64_t ti = (int64_t)(zh - zl) * (xh - xl) * pb_.nshots;

@@ -26,12 +26,25 @@ def _model(kind: str, n: Tuple[int, int, int], seed: int):
     return np.stack([vp, vs, rho, dlt, eps, np.zeros_like(vp)]).astype(np.float32), 6
 
 
+# The bench's serving mix: grids from the lower part of the configuration's
+# range (96^3 .. 384x384x256), time axes of 1000-2000 steps (of 1000-4000),
+# receiver lines of 48-96 (of 64-192) per side, so that a mix of a few dozen
+# requests runs in about a minute.
+BENCH_GRIDS = ((96, 96, 96), (160, 144, 128), (224, 192, 160))
+BENCH_STEPS = (1000, 1500, 2000)
+BENCH_REC = (48, 64, 96)
+# checkpoint slots of a gradient request (FP32 restart states, binomial schedule)
+GRADIENT_SLOTS = 40
+
+
 def make_mix(nreq: int = 48, rate: float = 20.0, seed: int = 5, grids=((64, 64, 64), (96, 96, 80), (128, 112, 96)),
              steps=(200, 300, 400), rec=(16, 24), p_gradient: float = 0.25):
     """Returns (models, requests).  Six models (acoustic, elastic, VTI, two
     grids each), each request one shot on a random model with a 8-15 Hz
     Ricker, steps and receiver lines drawn from small sets (so that shots of
-    the same model can share a batch), mode gradient with `p_gradient`."""
+    the same model can share a batch), mode gradient with `p_gradient`
+    (FP32 checkpoints with GRADIENT_SLOTS slots when the time axis is longer
+    than 500 steps)."""
     rng = np.random.default_rng(seed)
     kinds = ["acoustic", "elastic", "vti"]
     models: Dict[str, np.ndarray] = {}
@@ -64,6 +77,8 @@ def make_mix(nreq: int = 48, rate: float = 20.0, seed: int = 5, grids=((64, 64, 
         par.ns = 1
         w = synth.ricker(round(f0), dt, nsteps + 1)  # f0 rounded so that same-model shots may batch
         sv = synth.Survey(f"{mid}_{i}", nm, nx, ny, nz, d, d, d, models[mid], w, dt, par)
+        if mode == "gradient" and nsteps > 500:
+            sv.par.checkpoint_slots = GRADIENT_SLOTS
         r = serving.Request(i, mid, mode, sv, arrival=t)
         reqs.append(r)
     # observed data of the gradient requests: the model with a 3 % slower top half

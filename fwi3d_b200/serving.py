@@ -71,8 +71,13 @@ def session_bytes(sv, nshots: int, gradient: bool = False) -> int:
     if sv.nmodels != 2:
         b += nshots * 9 * n * 4
     if gradient:
-        nsnap = nt + 1
-        b += nsnap * nshots * nc * n * 2 + 2 * nshots * nc * n * 8 + 4 * nshots * nc * n * 4 + 3 * n * 8
+        slots = int(getattr(sv.par, "checkpoint_slots", 0))
+        if slots > 0:
+            # FP32 restart states (two levels), recomputation levels, ring, zero snapshot
+            b += (2 * slots + 7) * nshots * nc * n * 4 + 3 * n * 8
+        else:
+            nsnap = nt + 1
+            b += nsnap * nshots * nc * n * 2 + 2 * nshots * nc * n * 8 + 4 * nshots * nc * n * 4 + 3 * n * 8
     return int(b * 1.1)
 
 
@@ -138,15 +143,21 @@ class Report:
     requests: int
     makespan: float
     updates: int
-    latencies: List[float] = field(default_factory=list)
+    latencies: List[float] = field(default_factory=list)   # completion - arrival
+    service: List[float] = field(default_factory=list)     # completion - admission
+    queueing: List[float] = field(default_factory=list)    # admission - arrival
 
     def summary(self) -> Dict[str, float]:
-        lat = np.asarray(self.latencies, dtype=np.float64)
+        def pct(v, q):
+            a = np.asarray(v, dtype=np.float64)
+            return float(np.percentile(a, q)) if a.size else 0.0
+
         return {"requests": self.requests, "seconds": self.makespan,
                 "gpt_per_s": self.updates / self.makespan / 1e9 if self.makespan > 0 else 0.0,
                 "requests_per_s": self.requests / self.makespan if self.makespan > 0 else 0.0,
-                "p50_s": float(np.percentile(lat, 50)) if lat.size else 0.0,
-                "p99_s": float(np.percentile(lat, 99)) if lat.size else 0.0}
+                "p50_s": pct(self.latencies, 50), "p99_s": pct(self.latencies, 99),
+                "service_p50_s": pct(self.service, 50), "service_p99_s": pct(self.service, 99),
+                "queue_p50_s": pct(self.queueing, 50), "queue_p99_s": pct(self.queueing, 99)}
 
 
 class Server:
@@ -255,4 +266,5 @@ class Server:
         finally:
             pool.shutdown(wait=True)
         makespan = clock() - t0
-        return Report(len(requests), makespan, updates, [r.done - r.arrival for r in requests])
+        return Report(len(requests), makespan, updates, [r.done - r.arrival for r in requests],
+                      [r.done - r.admitted for r in requests], [r.admitted - r.arrival for r in requests])
