@@ -159,3 +159,53 @@ def forward_jacobianT(sv, adj_data: np.ndarray, shot: int = 0, precision: str = 
     if rc != 0:
         raise RuntimeError(f"oracle_forward_jacobianT failed ({rc})")
     return syn, grad, info
+
+
+class OracleSolver(C.Structure):
+    _fields_ = [("solver", C.c_int), ("lsearch", C.c_int), ("niter", C.c_int), ("max_trial", C.c_int),
+                ("threshold", C.c_float), ("ls_c1", C.c_float), ("ls_c2", C.c_float), ("ls_a0", C.c_float),
+                ("ls_a1", C.c_float), ("ls_max_step", C.c_float), ("ls_version", C.c_int), ("lbfgs_m", C.c_int),
+                ("nlcg_method", C.c_int), ("normalize_obj_func", C.c_int)]
+
+
+SOLVERS = {"none": 0, "lbfgs": 1, "nlcg": 2, "nlsd": 3}
+LSEARCH = {"weak_wolfe": 0, "regular_wolfe": 1}
+
+
+def fwi(sv, observed: np.ndarray, solver: str = "none", lsearch: str = "regular_wolfe", niter: int = 1,
+        max_trial: int = 10, normalize: bool = True, precision: str = "fp32", nthreads: int = 0, lbfgs_m: int = 5,
+        nlcg_method: int = 0, c1: float = 1e-4, c2: float = 0.9, a0: float = 1.0, a1: float = 0.0):
+    """The reference's FWI objective (nlls_fwi, optimization.cpp) on all shots
+    of the survey, or a run of its solver (nlsolver.cpp) from sv.model.
+    Returns dict(f=[objective history], model=final model, grad=gradient at
+    the last evaluated model, feval, geval)."""
+    lib = _lib(precision)
+    if not hasattr(lib, "_fwi_bound"):
+        fp = C.POINTER(C.c_float)
+        dp = C.POINTER(C.c_double)
+        ip = C.POINTER(C.c_int)
+        lib.oracle_fwi.argtypes = [C.POINTER(OracleParam), fp, fp, C.c_int, C.c_int, fp, C.c_int, fp, fp,
+                                   C.POINTER(OracleSolver), dp, ip, dp, dp, ip]
+        lib.oracle_fwi.restype = C.c_int
+        lib._fwi_bound = True
+    op = make_param(sv, nthreads)
+    model = np.ascontiguousarray(sv.model, dtype=np.float32)
+    w = np.ascontiguousarray(sv.wavelet, dtype=np.float32)
+    ncomp = 1 if w.ndim == 1 else w.shape[0]
+    ns = len(sv.par.sxyz)
+    s = np.ascontiguousarray(np.asarray(sv.par.sxyz, dtype=np.float32)[:, :3])
+    nr = len(sv.par.rxyz[0])
+    r = np.ascontiguousarray(np.asarray(sv.par.rxyz, dtype=np.float32).reshape(ns, nr, 5))
+    obs = np.ascontiguousarray(observed, dtype=np.float32)
+    so = OracleSolver(SOLVERS[solver], LSEARCH[lsearch], niter, max_trial, 0.0, c1, c2, a0, a1, 1e6, 0, lbfgs_m,
+                      nlcg_method, 1 if normalize else 0)
+    fh = np.zeros(niter + 2, dtype=np.float64)
+    nf = C.c_int()
+    mo = np.zeros(model.shape, dtype=np.float64)
+    go = np.zeros(model.shape, dtype=np.float64)
+    counts = (C.c_int * 2)()
+    rc = lib.oracle_fwi(C.byref(op), _fptr(model), _fptr(w), ncomp, ns, _fptr(s), nr, _fptr(r), _fptr(obs),
+                        C.byref(so), _dptr(fh), C.byref(nf), _dptr(mo), _dptr(go), counts)
+    if rc != 0:
+        raise RuntimeError(f"oracle_fwi failed ({rc})")
+    return {"f": fh[: nf.value].tolist(), "model": mo, "grad": go, "feval": counts[0], "geval": counts[1]}

@@ -119,18 +119,17 @@ def test_finite_difference_directional_derivative():
 
 
 def test_lbfgs_decreases_misfit():
-    from fwi3d_b200 import lbfgs
+    """Two l-BFGS iterations with the regular Wolfe search on the device
+    objective: the misfit decreases at each accepted step."""
+    from fwi3d_b200 import nlsolver
 
     sv, obs = _problem()
     obj = ops.FwiObjective(sv, obs, batch=4)
-    m = sv.model.astype(np.float32)
-    f0, g0 = obj.evaluate(m)
-    solver = lbfgs.LBFGS(m.size, m=5)
-    m1, f1, g1, a1 = lbfgs.step(obj.evaluate, m, f0, g0, solver, nm=3)
-    assert f1 < f0
-    m2, f2, g2, a2 = lbfgs.step(obj.evaluate, m1, f1, g1, solver, nm=3)
-    assert f2 < f1
-    assert len(solver.s) == 2
+    prob = nlsolver.Problem(sv.model.astype(np.float32), obj.evaluate, nlsolver.Backend("cuda:0"))
+    s = nlsolver.Lbfgs(2, max_trial=10, ls=nlsolver.RegularWolfe())
+    s.run(prob)
+    assert len(s.func) == 3
+    assert s.func[2] < s.func[1] < s.func[0]
 
 
 def test_autograd_function_gradient():

@@ -1,0 +1,88 @@
+"""The FWI objective and the non-linear solvers against the reference's own
+(nlls_fwi, optimization.cpp; lbfgs / nlcg with its Wolfe line searches,
+nlsolver.cpp), compiled into the CPU oracle.
+
+Tolerances: misfit within 1e-6 (relative), gradient within 1e-4 relative L2
+(the propagation parity bound), the solver's objective history within 1e-5,
+its final model within 1e-4, and the same numbers of function and gradient
+evaluations (the line search takes the same branches).
+"""
+import numpy as np
+import pytest
+
+from fwi3d_b200 import nlsolver, ops, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def _problem(oracle, nside=1, n=24, steps=120):
+    sv = synth.elastic_anomaly(n=n, nsteps=steps, nshots_side=nside, taper=6, rec_stride=3)
+    sv.par.sub = 1
+    true = synth.Survey(sv.name, 3, sv.nx, sv.ny, sv.nz, sv.dx, sv.dy, sv.dz, sv.extra["true_model"], sv.wavelet,
+                        sv.dt_data, sv.par.copy())
+    obs = np.stack([oracle.modeling(true, shot=s, precision="fp32")[0] for s in range(len(sv.par.sxyz))])
+    return sv, obs.astype(np.float32)
+
+
+def test_objective_matches_reference(oracle_fp32):
+    """One shot: nlls_fwi's getFunc and gradient (res + grad)."""
+    sv, obs = _problem(oracle_fp32)
+    ref = oracle_fp32.fwi(sv, obs, solver="none")
+    f, g = ops.FwiObjective(sv, obs, normalize=True, batch=1).evaluate(sv.model)
+    print(f"misfit {f:.9e} vs {ref['f'][0]:.9e}; gradient {rel(g, ref['grad'][:3]):.3e}")
+    assert abs(f - ref["f"][0]) / ref["f"][0] < 1e-6
+    for k in range(3):
+        assert rel(g[k], ref["grad"][k]) < 1e-4, k
+
+
+def test_multi_shot_gradient_chaining(oracle_fp32):
+    """Several shots: the reference accumulates shots with
+    apply_jacobianT(add=true), whose quadrature and chain rule also act on the
+    gradient accumulated so far (we_op.cpp:968-972, 1027-1075).  The per-shot
+    operators reproduce that chaining; the device objective returns the sum of
+    the per-shot gradients instead, and the difference is stated."""
+    sv, obs = _problem(oracle_fp32, nside=2)
+    ref = oracle_fp32.fwi(sv, obs, solver="none")
+    f, g = ops.FwiObjective(sv, obs, normalize=True, batch=4).evaluate(sv.model)
+    assert abs(f - ref["f"][0]) / ref["f"][0] < 1e-6
+    dt = sv.dt_data
+    dnorm = float(np.sum(obs.astype(np.float64) ** 2)) * dt
+    gc = np.zeros((3,) + sv.model.shape[1:], dtype=np.float32)
+    for s in range(len(sv.par.sxyz)):
+        op = ops.from_survey(sv, s)
+        r = (op.forward(False, sv.model) - obs[s]).astype(np.float32)
+        a = (r * np.float32(dt)).astype(np.float32)
+        a[..., 0] = (r[..., 0].astype(np.float64) * 0.5 * dt).astype(np.float32)
+        a[..., -1] = (r[..., -1].astype(np.float64) * 0.5 * dt).astype(np.float32)
+        gc = op.jacobianT(True, gc, sv.model, a)
+        op.close()
+    gc = gc.astype(np.float64) / dnorm
+    for k in range(3):
+        assert rel(gc[k], ref["grad"][k]) < 1e-4, k
+    print("device objective (sum of per-shot gradients) vs the reference's chained gradient:",
+          [f"{rel(g[k], ref['grad'][k]):.3e}" for k in range(3)])
+
+
+@pytest.mark.parametrize("solver,lsearch,niter", [("lbfgs", "regular_wolfe", 2), ("nlcg", "weak_wolfe", 2),
+                                                  ("nlsd", "regular_wolfe", 1)])
+def test_solver_iterations_match_reference(oracle_fp32, solver, lsearch, niter):
+    sv, obs = _problem(oracle_fp32)
+    ref = oracle_fp32.fwi(sv, obs, solver=solver, lsearch=lsearch, niter=niter)
+    obj = ops.FwiObjective(sv, obs, normalize=True, batch=1)
+    prob = nlsolver.Problem(sv.model, obj.evaluate, nlsolver.Backend("cuda:0"))
+    s = nlsolver.make_solver(solver, niter, max_trial=10, ls=nlsolver.make_line_search(lsearch))
+    s.run(prob)
+    m = prob.model_f32()
+    print(f"{solver}/{lsearch}: f {s.func} vs {ref['f']}; evals {s.counts} vs {ref['feval']}, {ref['geval']}; "
+          f"model {rel(m, ref['model']):.3e}")
+    assert len(s.func) == len(ref["f"])
+    for a, b in zip(s.func, ref["f"]):
+        assert abs(a - b) / b < 1e-5
+    assert s.counts["feval"] == ref["feval"] and s.counts["geval"] == ref["geval"]
+    assert rel(m - sv.model, ref["model"] - sv.model) < 1e-4
