@@ -82,8 +82,8 @@ def build(verbose: bool = False, force: bool = False, ptxas_verbose: bool = Fals
         o = os.path.join(BUILD, src + ".o")
         objs.append(o)
         if force or _stale(o, [s] + headers):
-            _run([cxx(), "-O2", "-std=c++17", "-fPIC", "-fopenmp", "-Wall", "-Wno-unused-variable", *inc, "-c", s,
-                  "-o", o], verbose)
+            _run([cxx(), "-O2", "-std=c++17", "-fPIC", "-fopenmp", "-Wall", "-Wno-unused-variable", *inc,
+                  "-I", os.path.join(os.path.dirname(os.path.dirname(nvcc())), "include"), "-c", s, "-o", o], verbose)
     if force or _stale(LIB, objs):
         _run([nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-lgomp"], verbose)
     return LIB

@@ -16,6 +16,8 @@
 #include <vector>
 
 #include "../../include/fwi3d_gpu.h"
+#include <nvtx3/nvToolsExt.h>
+
 #include "engine.h"
 #include "host_ops.h"
 
@@ -735,8 +737,10 @@ int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, floa
                 eng->forward(inj, B * o->nscomp, src.data(), ext, nullptr, true);
                 const auto t2 = now();
                 const size_t ntrb = (size_t)B * ntr;
+                nvtxRangePushA("fwi3d residual");
                 fsum += o->dres.run(*eng, (size_t)s0 * ntr * ntd, (int)ntrb, par.seismotype, alpha,
                                     residual ? residual + (size_t)s0 * ntr * ntd : nullptr);
+                nvtxRangePop();
                 std::vector<float> gb((size_t)nm * n);
                 const auto t3 = now();
                 eng->adjoint_dev(adj, (int)ntrb, o->dres.adjoint_sources(), gb.data());

@@ -22,6 +22,8 @@
 #include <type_traits>
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "engine.h"
 #include "imaging.cuh"
 #include "fused.cuh"
@@ -31,6 +33,16 @@
 #include "physics.cuh"
 
 namespace fwi {
+
+// Named range of host-side phases (forward, recomputation, adjoint, imaging)
+// for timeline tools; without a tool attached a push/pop is a few
+// nanoseconds.
+struct PhaseRange {
+    explicit PhaseRange(const char *name) { nvtxRangePushA(name); }
+    ~PhaseRange() { nvtxRangePop(); }
+    PhaseRange(const PhaseRange &) = delete;
+    PhaseRange &operator=(const PhaseRange &) = delete;
+};
 
 #define CK(x)                                                                                               \
     do {                                                                                                    \
@@ -608,6 +620,8 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     if (pb.nshots < 1) throw FwiError(FWI_ERR_ARG, "at least one shot");
     init_sbp_tables();
     CK(cudaMemcpyToSymbol(c_sbp, &g_sbp_host, sizeof(SbpTables)));
+    // the y chunking of the marching kernels aims at whole waves of resident CTAs
+    CK(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device));
     cudaStream_t s;
     CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     stream_ = s;
@@ -898,7 +912,7 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         if (afused_) {
             const int kz = (pb_.nz + fa::TZ - 1) / fa::TZ, kx = (pb_.nx + fa::TX - 1) / fa::TX;
             const int tiles = kz * kx * pb_.nshots;
-            int nch = (148 * 2 * 4 + tiles - 1) / tiles;  // about four waves of resident CTAs
+            int nch = (sm_count_ * 2 * 4 + tiles - 1) / tiles;  // about four waves of resident CTAs
             nch = std::max(1, std::min(nch, pb_.ny / 8));
             kmark(true, "k_acoustic_fused", n * pb_.nshots);
             k_acoustic_fused<<<dim3(kz, kx, nch * pb_.nshots), dim3(fa::TZ, fa::TX), 0, s>>>(a, nch);
@@ -915,7 +929,7 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
     if (march_) {
         const int kz = (pb_.nz + f3::TZ - 1) / f3::TZ, kx = (pb_.nx + f3::TX - 1) / f3::TX;
         const int tiles = kz * kx * pb_.nshots;
-        const int target = 148 * 3;  // about three waves of resident CTAs
+        const int target = sm_count_ * 3;  // about three waves of resident CTAs
         int nch = (target + tiles - 1) / tiles;
         nch = std::max(1, std::min(nch, (pb_.ny - 12) / 24));
         const dim3 grd(kz, kx, nch * pb_.nshots), mblk(f3::TZ, f3::TX);
@@ -1006,7 +1020,7 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         // y chunks per tile column: about fused_waves_ waves of resident CTAs,
         // at least 16 planes per chunk
         auto chunks = [&](int64_t tiles, int minb) {
-            const int64_t target = 148 * minb * fused_waves_;
+            const int64_t target = (int64_t)sm_count_ * minb * fused_waves_;
             const int64_t c = (target + tiles - 1) / tiles;
             return (int)std::max<int64_t>(1, std::min<int64_t>(c, (f.y1 - f.y0) / 16));
         };
@@ -1665,6 +1679,7 @@ void Engine::rv_advance(int d)
 // interval while free slots last.
 void Engine::rv_goto(int t)
 {
+    PhaseRange phase_range("fwi3d recompute");
     if (rv_pos_ == t) return;
     while (rv_pos_stack_.size() > 1 && rv_pos_stack_.back() > t) {
         rv_free_.push_back(rv_slot_stack_.back());
@@ -1695,6 +1710,7 @@ void Engine::rv_goto(int t)
 
 void Engine::forward(const InjTable &inj, int ntrace, const float *src, const ExtTable &ext, float *rcv, bool store)
 {
+    PhaseRange phase_range("fwi3d forward");
     CK(cudaSetDevice(device_));
     cudaStream_t s = (cudaStream_t)stream_;
     const int64_t n = pb_.nxyz();
@@ -2045,6 +2061,7 @@ void Engine::image(int itl, const float *curr, const float *prevl)
         const int k = itl - 1 + l;
         lev[l] = snap_fp32(std::min(std::max(k, 0), nsnap_ - 1));
     }
+    PhaseRange phase_range("fwi3d imaging");  // after the snapshots' retrieval (decoding, recomputation)
     const dim3 blk(BZ, BX, BY), grd = grid_of(a.g, 1);
     for (int l = 0; l < 3; l++)
         for (int c = 0; c < 3; c++) a.fwd[l][c] = lev[l] + (int64_t)(c < nc ? c : 0) * n;
@@ -2073,6 +2090,7 @@ void Engine::adjoint_dev(const InjTable &inj, int ntrace, const float *adj_src_d
 
 void Engine::adjoint_impl(const InjTable &inj, int ntrace, const float *adj_src, const float *adj_src_dev, float *grad)
 {
+    PhaseRange phase_range("fwi3d adjoint");
     CK(cudaSetDevice(device_));
     if (!snaps_valid_) throw FwiError(FWI_ERR_STATE, "adjoint needs the snapshots of a preceding forward with sub > 0");
     cudaStream_t s = (cudaStream_t)stream_;
@@ -2194,6 +2212,20 @@ void static_elastic_step(const fwi_grid &grid, int nmodels, const int bc[6], flo
             throw FwiError(FWI_ERR_UNSUPPORTED,
                            "only bc 0 (none) and 1 (traction-free) faces: absorbing and rigid faces need the "
                            "model-dependent boundary tables that the operator and batch paths build");
+    // next is written at every point while curr is read at neighbouring
+    // points and prev at the point itself: next may be prev (the leapfrog
+    // in place) but may overlap neither curr nor the model, nor prev in part
+    {
+        const uintptr_t nb = (uintptr_t)next, ne = nb + sizeof(float) * 3 * (size_t)n;
+        auto overlaps = [&](const float *p, size_t count) {
+            const uintptr_t b = (uintptr_t)p, e = b + sizeof(float) * count;
+            return b < ne && nb < e;
+        };
+        if (overlaps(curr, 3 * (size_t)n)) throw FwiError(FWI_ERR_ARG, "next overlaps curr");
+        if (overlaps(model, (size_t)nmodels * n)) throw FwiError(FWI_ERR_ARG, "next overlaps the model");
+        if (next != prev && overlaps(prev, 3 * (size_t)n))
+            throw FwiError(FWI_ERR_ARG, "next overlaps prev in part (it may only be prev itself)");
+    }
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) throw FwiError(FWI_ERR_NOGPU, "no CUDA device");
     if (dev >= kStaticMaxDevices) throw FwiError(FWI_ERR_ARG, "device ordinal above the static set-up table");

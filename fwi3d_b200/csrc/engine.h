@@ -176,6 +176,7 @@ private:
     float *level(int l) const;
 
     int device_;
+    int sm_count_ = 148;           // streaming multiprocessors of the device
     Problem pb_;
     void *stream_ = nullptr;
     DevBuf model_;                 // [nm][nxyz]

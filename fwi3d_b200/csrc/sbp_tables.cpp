@@ -7,6 +7,7 @@
 // as the reference's `data_t` initialisers are, so both codes use identical
 // single-precision coefficients.
 #include <cstring>
+#include <mutex>
 #include "sbp.cuh"
 
 namespace fwi {
@@ -17,10 +18,9 @@ namespace {
 inline float q(double p, double r) { return (float)(p / r); }
 }  // namespace
 
-void init_sbp_tables()
+namespace {
+void build_sbp_tables()
 {
-    static bool done = false;
-    if (done) return;
     SbpTables t;
     std::memset(&t, 0, sizeof(t));
 
@@ -56,7 +56,16 @@ void init_sbp_tables()
     t.hq[3] = q(49, 48);
 
     g_sbp_host = t;
-    done = true;
+}
+}  // namespace
+
+// Built once per process: engines are created on several host threads (the
+// serving loop's workers), so the table is written under std::call_once,
+// whose completion every later caller observes before reading it.
+void init_sbp_tables()
+{
+    static std::once_flag once;
+    std::call_once(once, build_sbp_tables);
 }
 
 }  // namespace fwi

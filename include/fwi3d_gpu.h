@@ -157,6 +157,9 @@ void fwi_batch_destroy(fwi_batch *b);
  *   model: converted [nmodels][ny][nx][nz] (lambda, mu, rho[, c13, eps, c66]);
  *   prev, curr (read), next (written at every point): [3][ny][nx][nz];
  *   all on the current device; stream: a cudaStream_t (0: legacy default).
+ *   next may be prev itself (the leapfrog in place: prev is read only at the
+ *   point written) but must not overlap curr, the model, or prev in part
+ *   (FWI_ERR_ARG).
  * Limits: at most 262,144 grid points (the static scratch is 9 x 2^18 floats,
  * 9 MiB, reserved with the library's device code when that loads), each axis >= 12, bc[6] each 0 (none) or 1 (traction-free), no taper
  * (FWI_ERR_ARG / FWI_ERR_UNSUPPORTED otherwise).  Nothing needs to start at

@@ -50,6 +50,23 @@ def test_static_step_rejects_absorbing_faces_and_acoustic():
     assert rc == _lib.FWI_ERR_ARG
 
 
+def test_static_step_rejects_overlapping_outputs():
+    """next may be prev itself but must overlap neither curr, nor the model,
+    nor prev in part (the addresses are checked before any device access)."""
+    lib = _lib.load()
+    g = _grid(24, 24, 24)
+    n = 24 ** 3
+    base = 1 << 32
+    model, prev, curr = base, base + 16 * n * 4, base + 32 * n * 4
+    bc = _bc(1, 1, 1, 1, 1, 1)
+    cases = {"curr": curr + 4 * n, "the model": model + 4, "prev in part": prev + 4}
+    for what, nxt in cases.items():
+        rc = lib.fwi_elastic_step_static(C.byref(g), 3, bc, 1e-4, C.c_void_p(model), C.c_void_p(prev),
+                                         C.c_void_p(curr), C.c_void_p(nxt), None)
+        assert rc == _lib.FWI_ERR_ARG, what
+        assert "overlaps " + what in lib.fwi_last_error().decode(), what
+
+
 def _survey(nmodels, nsteps, cut):
     """Traction-free box (every face bc 1, no taper), one source whose wavelet
     is zero from sample `cut` on, a displacement receiver on every node."""
@@ -150,3 +167,12 @@ def test_static_step_matches_batch_two_calls(nmodels):
     o1, o2 = out1.cpu().numpy(), out2.cpu().numpy()
     # the same per-point kernels on the same inputs: bit-identical
     assert np.array_equal(o1, u[k]) and np.array_equal(o2, u[k + 1]), (_rel(o1, u[k]), _rel(o2, u[k + 1]))
+    # a warm call takes no device memory: the free memory of the device and
+    # the caching allocator's figures are the same before and after it
+    free0, _ = torch.cuda.mem_get_info(dev)
+    alloc0 = torch.cuda.memory_allocated(dev)
+    _lib.check(lib.fwi_elastic_step_static(C.byref(g), nmodels, bc, dt, model.data_ptr(), out1.data_ptr(),
+                                           out2.data_ptr(), prev.data_ptr(), stream))
+    torch.cuda.synchronize(dev)
+    free1, _ = torch.cuda.mem_get_info(dev)
+    assert free1 == free0 and torch.cuda.memory_allocated(dev) == alloc0
