@@ -43,8 +43,20 @@ def test_size_mismatch_is_an_error(tmp_path):
         sepio.read(str(tmp_path / "x.H"))
 
 
-# the reference tree, where the oracle recipe (oracle/Makefile) finds it
-REF_PY = "/root/reference/src/python"
+def _reference_tree() -> str:
+    """The reference tree: FWI3D_REFERENCE, else the one the oracle recipe
+    compiled from (oracle/_ref/REF_PATH); empty where neither exists."""
+    if os.environ.get("FWI3D_REFERENCE"):
+        return os.environ["FWI3D_REFERENCE"]
+    rec = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "REF_PATH")
+    try:
+        with open(rec) as f:
+            return f.read().strip()
+    except OSError:
+        return ""
+
+
+REF_PY = os.path.join(_reference_tree(), "src", "python")
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(REF_PY, "seppy.py")), reason="reference tree not mounted")
