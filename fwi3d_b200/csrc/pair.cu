@@ -25,6 +25,7 @@ __device__ __forceinline__ void pair_march(FusedCtx &c, int tid, int ya, int yb)
 #pragma unroll
     for (int k = 0; k < 5; k++) th.qmu[k] = th.qT[k] = th.qX1[k] = th.qZ1[k] = f2s(0.f);
     const PairK K = pair_consts(*c.a);
+    const PairTaper tp = pair_taper(c, tid);
     if (c.tma && tid == 0) fz_bar_init(c);
     if (XC || ZC) fill_pair_rows(c.sm->rows, tid, pz::NT);
     for (int q = ya - 4; q < ya; q++) pz_load_u<false>(c, tid, q, ring<ELASTIC>(q));
@@ -61,7 +62,7 @@ __device__ __forceinline__ void pair_march(FusedCtx &c, int tid, int ya, int yb)
             pz_load_mat<EVEN, true>(c, tid, y + 1);
             cpa_commit();
         }
-        if (y >= ya) pz_phase_c<EVEN, XC, ZC>(c, K, th, tid, y, acc, uin);
+        if (y >= ya) pz_phase_c<EVEN, XC, ZC>(c, K, th, tid, y, acc, uin, tp);
     }
     cpa_wait();
     if (c.tma) fz_tma_wait(c, ring<ELASTIC>(yb + 4));  // the copy issued in the last step

@@ -230,6 +230,33 @@ struct ZT {
 };
 FWI_HD ZT ztaps(const float *p) { return ZT{ld2(p - 2), ld2(p), ld2(p + 2)}; }
 
+// Taper of the own pair: the z and x factors do not change along the march,
+// so they are read once; a plane adds its two y factors.
+struct PairTaper {
+    F2 zx;      // tz_lo * tz_hi * tx_lo * tx_hi per point (the reference's factor order)
+    bool inzx;  // a point of the pair lies in a z or x taper zone
+};
+FWI_HD PairTaper pair_taper(const FusedCtx &c, int tid)
+{
+    const StepArgs &a = *c.a;
+    const Dims &g = a.g;
+    const int pzi = tid % pz::NPR, lx = tid / pz::NPR;
+    // points past the grid's end (their stores are masked) take the last
+    // row's factors, so that the tables are read in bounds
+    const int ix = min(c.x0 + lx, g.nx - 1), iz = min(c.z0 + 2 * pzi, g.nz - 1), iz1 = min(iz + 1, g.nz - 1);
+    auto zin = [&](int z) { return z < a.tw[0] || z >= g.nz - a.tw[1]; };
+    PairTaper t;
+    t.inzx = zin(iz) || zin(iz1) || ix < a.tw[2] || ix >= g.nx - a.tw[3];
+    t.zx = f2s(1.f);
+    if (t.inzx) {
+        t.zx = f2(a.tap[0][iz], a.tap[0][iz1]);
+        t.zx = mul2(t.zx, f2(a.tap[1][iz], a.tap[1][iz1]));
+        t.zx = mul2(t.zx, f2s(a.tap[2][ix]));
+        t.zx = mul2(t.zx, f2s(a.tap[3][ix]));
+    }
+    return t;
+}
+
 // Per-thread queues along y (planes y-2 .. y+2 of the own pair).
 struct PairThread {
     F2 qmu[5];  // mu
@@ -563,7 +590,6 @@ FWI_HD void pz_phase_b(const FusedCtx &c, const PairK &K, const PairThread &th, 
     const bool zcl = ZC && (iz < 6 || iz + 1 >= g.nz - 6);
     const float *mp = &fz_mpp(c.sm, MP_MU)[xh][zh];
     const F2 mu0 = ld2(mp);
-    const F2 lam = ld2(&fz_mpp(c.sm, MP_LAM)[xh][zh]);
     W5p wx{}, wz{};
     if (!xcl) wx = d2w_pair(ld2(mp - 2 * XD), ld2(mp - XD), mu0, ld2(mp + XD), ld2(mp + 2 * XD), K.sx1);
     if (!zcl) {
@@ -634,7 +660,7 @@ FWI_HD void pz_phase_b(const FusedCtx &c, const PairK &K, const PairThread &th, 
         if (ZC && zcl) return add2(v, d2zc[k]);
         return d2acc(wz, z.m, zm1, z.a, zp1, z.b, v);
     };
-    F2 ux0, uy0, uz0, uy1, ux2, uy2, uz2;
+    F2 uy0, uz0, ux2, uy2;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         const float *u = pz_u(c, c.sl[2], k, xw, zw);
@@ -650,7 +676,6 @@ FWI_HD void pz_phase_b(const FusedCtx &c, const PairK &K, const PairThread &th, 
             v = add2(v, v);
             v = d2acc(wy, ym2, ym1, u0, yp1, yp2, v);
             v = d2z(k, z, zm1, zp1, v);
-            ux0 = XC ? pxd1<XC>(c, u, X, ix, K.cx0, K.cx1, a.idx) : d1p(xm2, xm1, xp1, xp2, K.cx0, K.cx1);
             uy0 = d1p(ym2, ym1, yp1, yp2, K.cy0, K.cy1);
             uz0 = ZC ? pzd1<ZC>(c, u, iz, zo, K.cz0, K.cz1, a.idz) : d1p(z.m, zm1, zp1, z.b, K.cz0, K.cz1);
         } else if (k == 1) {
@@ -658,7 +683,6 @@ FWI_HD void pz_phase_b(const FusedCtx &c, const PairK &K, const PairThread &th, 
             v = add2(v, v);
             v = d2x(k, xm2, xm1, u0, xp1, xp2, v);
             v = d2z(k, z, zm1, zp1, v);
-            uy1 = d1p(ym2, ym1, yp1, yp2, K.cy0, K.cy1);
         } else {
             v = d2z(k, z, zm1, zp1, f2s(0.f));
             v = add2(v, v);
@@ -666,11 +690,11 @@ FWI_HD void pz_phase_b(const FusedCtx &c, const PairK &K, const PairThread &th, 
             v = d2acc(wy, ym2, ym1, u0, yp1, yp2, v);
             ux2 = XC ? pxd1<XC>(c, u, X, ix, K.cx0, K.cx1, a.idx) : d1p(xm2, xm1, xp1, xp2, K.cx0, K.cx1);
             uy2 = d1p(ym2, ym1, yp1, yp2, K.cy0, K.cy1);
-            uz2 = ZC ? pzd1<ZC>(c, u, iz, zo, K.cz0, K.cz1, a.idz) : d1p(z.m, zm1, zp1, z.b, K.cz0, K.cz1);
         }
         acc[k] = v;
     }
-    st2(&fz_dvp(c.sm, DV_T0)[xh][zh], mul2(lam, add2(add2(ux0, uy1), uz2)));
+    // lambda div u of the own pair is the column phase's value of this plane
+    st2(&fz_dvp(c.sm, DV_T0)[xh][zh], th.qT[2]);
     st2(&fz_dvp(c.sm, DV_Y0)[xh][zh], mul2(mu0, uy0));
     st2(&fz_dvp(c.sm, DV_Z0)[xh][zh], mul2(mu0, uz0));
     st2(&fz_dvp(c.sm, DV_X2)[xh][zh], mul2(mu0, ux2));
@@ -693,7 +717,7 @@ FWI_HD void pz_phase_b(const FusedCtx &c, const PairK &K, const PairThread &th, 
 // not stored.
 template <bool EVEN, bool XC, bool ZC>
 FWI_HD void pz_phase_c(const FusedCtx &c, const PairK &K, const PairThread &th, int tid, int y, const F2 acc[3],
-                       const UpdIn &in)
+                       const UpdIn &in, const PairTaper &tp)
 {
     const StepArgs &a = *c.a;
     const Dims &g = a.g;
@@ -724,17 +748,13 @@ FWI_HD void pz_phase_c(const FusedCtx &c, const PairK &K, const PairThread &th, 
     const int64_t i = g.idx(ix, y, iz);
     const float dt2 = a.dt * a.dt;
     const F2 s = f2(dt2 * rcp_rn(f2lo(in.rho)), dt2 * rcp_rn(f2hi(in.rho)));
-    const bool tz = in_taper(a, ix, y, iz) || in_taper(a, ix, y, iz + 1);
+    const bool tz = tp.inzx || y < a.tw[4] || y >= g.ny - a.tw[5];
     const bool face = (XC && (ix == 0 || ix == g.nx - 1)) || (ZC && (iz == 0 || iz >= g.nz - 2));
     F2 tf = f2s(1.f);
     if (tz) {
         // one factor per point, the product of the six in the reference's
         // order: z (top, bottom), x (left, right), y (front, back)
-        tf = f2(a.tap[0][iz], a.tap[0][iz + 1]);
-        tf = mul2(tf, f2(a.tap[1][iz], a.tap[1][iz + 1]));
-        tf = mul2(tf, f2s(a.tap[2][ix]));
-        tf = mul2(tf, f2s(a.tap[3][ix]));
-        tf = mul2(tf, f2s(a.tap[4][y]));
+        tf = mul2(tp.zx, f2s(a.tap[4][y]));
         tf = mul2(tf, f2s(a.tap[5][y]));
     }
     const F2 v[3] = {v0, v1, v2};
