@@ -25,14 +25,15 @@ __device__ __forceinline__ void pair_march(FusedCtx &c, int tid, int ya, int yb)
 #pragma unroll
     for (int k = 0; k < 5; k++) th.qmu[k] = th.qT[k] = th.qX1[k] = th.qZ1[k] = f2s(0.f);
     const PairK K = pair_consts(*c.a);
-    const PairTaper tp = pair_taper(c, tid);
+    constexpr bool ZQ = ZC && !XC;  // thread layout of the z-face tiles (pz_pos)
+    const PairTaper tp = pair_taper<ZQ>(c, tid);
     if (c.tma && tid == 0) fz_bar_init(c);
     if (XC || ZC) fill_pair_rows(c.sm->rows, tid, pz::NT);
     for (int q = ya - 4; q < ya; q++) pz_load_u<false>(c, tid, q, ring<ELASTIC>(q));
     __syncthreads();
     for (int y = ya - 4; y < yb; y++) {
         fz_slots<ELASTIC>(c, y);
-        const ColIn cin = pz_col_in<EVEN>(c, tid, y + 2);
+        const ColIn cin = pz_col_in<EVEN, ZQ>(c, tid, y + 2);
         // plane y+4: copied in here on the first step, else during the previous one
         if (y == ya - 4) {
             if (!c.tma) pz_load_u<false>(c, tid, y + 4, c.sl[6]);
@@ -54,7 +55,7 @@ __device__ __forceinline__ void pair_march(FusedCtx &c, int tid, int ya, int yb)
         UpdIn uin;
         if (y >= ya) {
             pz_phase_b<XC, ZC>(c, K, th, tid, y, acc);
-            uin = pz_upd_in<EVEN>(c, tid, y);
+            uin = pz_upd_in<EVEN, ZQ>(c, tid, y);
         }
         __syncthreads();
         // material plane y+1 for the next step (phase B of this one has read plane y)

@@ -46,6 +46,31 @@ constexpr int NPR = TZ / 2;   // pairs per x row
 constexpr int NT = NPR * TX;  // 256 threads
 }  // namespace pz
 
+// Thread -> own pair: pair index pzi along z, x row lx of the tile.  The
+// default layout gives each half-warp one x row (16 consecutive pairs), so the
+// x closure rows are uniform per half-warp.  ZQ, for the tiles that touch a z
+// face only: a warp holds 4 pairs of 8 x rows, so the closure pairs of a face
+// (the first or last three of the tile) fall into two warps instead of all
+// eight, warps 2b and 2b+1 for pair block b, which the SM issues from
+// different sub-partitions (warp index mod 4); the x rows of a half-warp are
+// interleaved so that its 16 eight-byte accesses hit distinct bank pairs at
+// both row strides of the tile (ZW for the ring, ZH for the derived and
+// material planes).
+template <bool ZQ>
+FWI_HD void pz_pos(int tid, int &pzi, int &lx)
+{
+    if (!ZQ) {
+        pzi = tid % pz::NPR;
+        lx = tid / pz::NPR;
+        return;
+    }
+    const int w = tid >> 5, h = (tid >> 4) & 1, j = (tid >> 2) & 3, p = tid & 3;
+    pzi = 4 * (w >> 1) + p;
+    lx = 8 * (w & 1) + j + 4 * (h ^ ((p < 2 && j > 0) ? 1 : 0));
+}
+static_assert(pz::NPR == 16 && pz::TX == 16, "the ZQ layout covers 16 pairs x 16 rows");
+static_assert(fz::ZW % 32 == 8 && fz::ZH % 32 == 4, "the ZQ layout is bank-conflict free at these row strides");
+
 // ---------------------------------------------------------------------------
 // Packed FP32 pairs.  On the GPU a pair lives in one 64-bit register pair and
 // the arithmetic is one .f32x2 instruction; on the host it is two floats.
@@ -236,11 +261,13 @@ struct PairTaper {
     F2 zx;      // tz_lo * tz_hi * tx_lo * tx_hi per point (the reference's factor order)
     bool inzx;  // a point of the pair lies in a z or x taper zone
 };
+template <bool ZQ>
 FWI_HD PairTaper pair_taper(const FusedCtx &c, int tid)
 {
     const StepArgs &a = *c.a;
     const Dims &g = a.g;
-    const int pzi = tid % pz::NPR, lx = tid / pz::NPR;
+    int pzi, lx;
+    pz_pos<ZQ>(tid, pzi, lx);
     // points past the grid's end (their stores are masked) take the last
     // row's factors, so that the tables are read in bounds
     const int ix = min(c.x0 + lx, g.nx - 1), iz = min(c.z0 + 2 * pzi, g.nz - 1), iz1 = min(iz + 1, g.nz - 1);
@@ -360,20 +387,22 @@ FWI_HD void pz_load_mat(FusedCtx &c, int tid, int y)
 struct ColIn {
     F2 mu, lam;
 };
-template <bool EVEN>
+template <bool EVEN, bool ZQ>
 FWI_HD ColIn pz_col_in(const FusedCtx &c, int tid, int q)
 {
-    const int pzi = tid % pz::NPR, lx = tid / pz::NPR;
+    int pzi, lx;
+    pz_pos<ZQ>(tid, pzi, lx);
     const int64_t i = c.a->g.idx(c.x0 + lx, q, c.z0 + 2 * pzi);
     return ColIn{ldg2<EVEN>(c.a->m[1] + i), ldg2<EVEN>(c.a->m[0] + i)};
 }
 struct UpdIn {
     F2 rho, p[3];
 };
-template <bool EVEN>
+template <bool EVEN, bool ZQ>
 FWI_HD UpdIn pz_upd_in(const FusedCtx &c, int tid, int y)
 {
-    const int pzi = tid % pz::NPR, lx = tid / pz::NPR;
+    int pzi, lx;
+    pz_pos<ZQ>(tid, pzi, lx);
     const int64_t i = c.a->g.idx(c.x0 + lx, y, c.z0 + 2 * pzi);
     UpdIn r;
     r.rho = ldg2<EVEN>(c.a->m[2] + i);
@@ -467,6 +496,31 @@ FWI_HD F2 pzd1(const FusedCtx &c, const float *p, int iz, int zoff, F2 c0h, F2 c
     return d1p(z.m, z.m1(), z.p1(), z.b, c0h, c1h);
 }
 
+// L2 prefetch hint (no register result): the closure weights and face
+// divisors of the next plane are requested a step ahead of their use.
+FWI_HD void prefetch_l2(const void *p)
+{
+#if defined(__CUDA_ARCH__)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+#else
+    (void)p;
+#endif
+}
+
+// Absorbing-boundary scale of point (ix, y, iz) of component k (boundary_scale),
+// with a prefetch of the same face's divisor at plane y+1.  Planes of the
+// paired kernel lie in [6, ny-6), so only the x and z faces own its points.
+FWI_HD float pz_face_scale(const StepArgs &a, float v, int k, int ix, int y, int iz)
+{
+    if (!a.scale) return v;
+    int64_t off;
+    const int f = owner_face(a.g, ix, y, iz, off);
+    if (f < 0) return v;
+    const float *d = a.sdiv[f][k] + off;
+    prefetch_l2(d + (f == TOP || f == BOTTOM ? a.g.nx : a.g.nz));
+    return v / d[0];
+}
+
 // D2var closure weights of a pair (8 per point, scaled by s) from a per-model table.
 struct W8p {
     F2 w[8];
@@ -507,7 +561,8 @@ template <bool XC, bool ZC>
 FWI_HD void pz_column(const FusedCtx &c, const PairK &K, PairThread &th, int tid, const ColIn &in)
 {
     const StepArgs &a = *c.a;
-    const int pzi = tid % pz::NPR, lx = tid / pz::NPR;
+    int pzi, lx;
+    pz_pos<ZC && !XC>(tid, pzi, lx);
     const int xw = lx + fz::HW, zw = 2 * pzi + fz::HW;
     const int ix = c.x0 + lx, iz = c.z0 + 2 * pzi;
     const int zo = c.z0 - fz::HW;
@@ -579,7 +634,8 @@ FWI_HD void pz_phase_b(const FusedCtx &c, const PairK &K, const PairThread &th, 
 {
     const StepArgs &a = *c.a;
     const Dims &g = a.g;
-    const int pzi = tid % pz::NPR, lx = tid / pz::NPR;
+    int pzi, lx;
+    pz_pos<ZC && !XC>(tid, pzi, lx);
     const int xw = lx + fz::HW, zw = 2 * pzi + fz::HW;
     const int xh = lx + fz::HD, zh = 2 * pzi + fz::HD;
     const int ix = c.x0 + lx, iz = c.z0 + 2 * pzi;
@@ -608,6 +664,9 @@ FWI_HD void pz_phase_b(const FusedCtx &c, const PairK &K, const PairThread &th, 
         const int st = hi ? -X : X;
         if (tab) {
             const W8p W = w8_pair(tab + (ln * 12 + slot) * 8, tab + ((ln + 1) * 12 + slot) * 8, K.sx1);
+            // the same rows of plane y+1 (line ln + nz; y+1 < ny-5, so in the table)
+            prefetch_l2(tab + ((ln + g.nz) * 12 + slot) * 8);
+            prefetch_l2(tab + ((ln + g.nz + 1) * 12 + slot) * 8);
 #pragma unroll
             for (int k = 0; k < 3; k++) {
                 const float *b = pz_u(c, c.sl[2], k, xw, zw) + ((hi ? g.nx - 1 : 0) - ix) * X;
@@ -633,6 +692,8 @@ FWI_HD void pz_phase_b(const FusedCtx &c, const PairK &K, const PairThread &th, 
             // rows (iz, iz+1) at the low face, (n-1-iz, n-2-iz) at the high face
             const int s0 = lo ? iz : 6 + (n - 1 - iz), s1 = lo ? iz + 1 : 5 + (n - 1 - iz);
             const W8p W = w8_pair(tab + (ln * 12 + s0) * 8, tab + (ln * 12 + s1) * 8, K.sz1);
+            prefetch_l2(tab + ((ln + g.nx) * 12 + s0) * 8);  // plane y+1
+            prefetch_l2(tab + ((ln + g.nx) * 12 + s1) * 8);
             const int st = hi ? -1 : 1;
 #pragma unroll
             for (int k = 0; k < 3; k++) {
@@ -721,7 +782,8 @@ FWI_HD void pz_phase_c(const FusedCtx &c, const PairK &K, const PairThread &th, 
 {
     const StepArgs &a = *c.a;
     const Dims &g = a.g;
-    const int pzi = tid % pz::NPR, lx = tid / pz::NPR;
+    int pzi, lx;
+    pz_pos<ZC && !XC>(tid, pzi, lx);
     const int ix = c.x0 + lx, iz = c.z0 + 2 * pzi;
     const int xw = lx + fz::HW, zw = 2 * pzi + fz::HW;
     const int xh = lx + fz::HD, zh = 2 * pzi + fz::HD;
@@ -764,7 +826,7 @@ FWI_HD void pz_phase_c(const FusedCtx &c, const PairK &K, const PairThread &th, 
         if (tz && a.taper_prev) p = mul2(p, tf);
         const F2 u0 = ld2(pz_u(c, c.sl[2], k, xw, zw));
         F2 r = sub2(fma2(v[k], s, add2(u0, u0)), p);
-        if (face) r = f2(boundary_scale(a, f2lo(r), k, ix, y, iz), boundary_scale(a, f2hi(r), k, ix, y, iz + 1));
+        if (face) r = f2(pz_face_scale(a, f2lo(r), k, ix, y, iz), pz_face_scale(a, f2hi(r), k, ix, y, iz + 1));
         if (tz) r = mul2(r, tf);
         float *dst = a.next[k] + c.so + i;
         if (iz + 1 < c.zend) {
