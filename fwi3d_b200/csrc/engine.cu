@@ -347,27 +347,27 @@ __global__ void __launch_bounds__(f3::NT, 1) k_elastic_march(const __grid_consta
 // update, scaling and taper are linear in it.  Each boundary point of the
 // slab is enumerated once: z faces whole, x faces without z edges, y faces
 // (when inside the slab) without x and z edges.
-__device__ __forceinline__ bool face_point(const Dims &g, int y0, int y1, int64_t k, int &ix, int &iy, int &iz)
+__device__ __forceinline__ bool face_point(const Dims &g, int y0, int y1, int k, int &ix, int &iy, int &iz)
 {
     const int ly = y1 - y0;
-    const int64_t nzf = (int64_t)g.nx * ly;          // each z face
-    const int64_t nxf = (int64_t)(g.nz - 2) * ly;    // each x face
-    const int64_t nyf = (int64_t)(g.nx - 2) * (g.nz - 2);
+    const int nzf = g.nx * ly;          // each z face
+    const int nxf = (g.nz - 2) * ly;    // each x face
+    const int nyf = (g.nx - 2) * (g.nz - 2);
     if (k < 2 * nzf) {
-        const int side = (int)(k / nzf);
-        const int64_t r = k - side * nzf;
+        const int side = k >= nzf;
+        const int r = k - side * nzf;
         iz = side ? g.nz - 1 : 0;
-        ix = (int)(r % g.nx);
-        iy = y0 + (int)(r / g.nx);
+        ix = r % g.nx;
+        iy = y0 + r / g.nx;
         return true;
     }
     k -= 2 * nzf;
     if (k < 2 * nxf) {
-        const int side = (int)(k / nxf);
-        const int64_t r = k - side * nxf;
+        const int side = k >= nxf;
+        const int r = k - side * nxf;
         ix = side ? g.nx - 1 : 0;
-        iz = 1 + (int)(r % (g.nz - 2));
-        iy = y0 + (int)(r / (g.nz - 2));
+        iz = 1 + r % (g.nz - 2);
+        iy = y0 + r / (g.nz - 2);
         return true;
     }
     k -= 2 * nxf;
@@ -376,8 +376,8 @@ __device__ __forceinline__ bool face_point(const Dims &g, int y0, int y1, int64_
         if (yy < y0 || yy >= y1) continue;
         if (k < nyf) {
             iy = yy;
-            iz = 1 + (int)(k % (g.nz - 2));
-            ix = 1 + (int)(k / (g.nz - 2));
+            iz = 1 + k % (g.nz - 2);
+            ix = 1 + k / (g.nz - 2);
             return true;
         }
         k -= nyf;
@@ -385,22 +385,41 @@ __device__ __forceinline__ bool face_point(const Dims &g, int y0, int y1, int64_
     return false;
 }
 
+// One thread per face point and shot (blockIdx.y), the three components in
+// turn: a point's samples are read from memory once for the three terms.
 template <int PH>
-__global__ void k_elastic_face_sat(const __grid_constant__ StepArgs a, int64_t npts)
+__global__ void k_elastic_face_sat(const __grid_constant__ StepArgs a, int npts)
 {
-    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= npts) return;
     int ix, iy, iz;
     if (!face_point(a.g, a.y0, a.y1, k, ix, iy, iz)) return;
     const int64_t so = (int64_t)blockIdx.y * a.sst;
-    const int c = blockIdx.z;  // one component per thread: three independent load chains per point
     const int64_t i = a.g.idx(ix, iy, iz);
-    const float sat = elastic_sat<PH>(a, 0.f, c, ix, iy, iz, so);
-    if (sat == 0.f) return;
-    float v = a.dt * a.dt / a.m[2][i] * sat;
-    v = boundary_scale(a, v, c, ix, iy, iz);
-    v = taper(a, v, ix, iy, iz);
-    a.next[c][so + i] += v;
+    float sat[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) sat[c] = elastic_sat<PH>(a, 0.f, c, ix, iy, iz, so);
+    const float dt2r = a.dt * a.dt / a.m[2][i];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        if (sat[c] == 0.f) continue;
+        float v = dt2r * sat[c];
+        v = boundary_scale(a, v, c, ix, iy, iz);
+        v = taper(a, v, ix, iy, iz);
+        a.next[c][so + i] += v;
+    }
+}
+
+// Face points of planes [y0, y1) (both z faces, both x faces without the z
+// edges, the y faces inside the range without x and z edges) as an int grid.
+static int face_points(const Problem &pb, int y0, int y1)
+{
+    const int64_t ly = y1 - y0;
+    int64_t nf = 2 * (int64_t)pb.nx * ly + 2 * (int64_t)(pb.nz - 2) * ly;
+    if (y0 == 0) nf += (int64_t)(pb.nx - 2) * (pb.nz - 2);
+    if (y1 == pb.ny) nf += (int64_t)(pb.nx - 2) * (pb.nz - 2);
+    if (nf >= (int64_t)INT32_MAX - 128) throw std::runtime_error("grid faces exceed the SAT kernel's index range");
+    return (int)nf;
 }
 
 // Post-injection: next += taper(scale(dt^2 (w s)/rho)) (elastic) or dt^2 (w s) K
@@ -938,12 +957,11 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         else k_elastic_march<VTI><<<grd, mblk, sizeof(MarchSmem), s>>>(a, nch, 0);
         kmark(false, nullptr, 0);
         // SAT of every face point
-        const int64_t nf = 2 * (int64_t)pb_.nx * pb_.ny + 2 * (int64_t)(pb_.nz - 2) * pb_.ny +
-                           2 * (int64_t)(pb_.nx - 2) * (pb_.nz - 2);
         StepArgs f = a;
         f.y0 = 0;
         f.y1 = pb_.ny;
-        const dim3 sgrd((unsigned)((nf + 127) / 128), pb_.nshots, 3);
+        const int nf = face_points(pb_, f.y0, f.y1);
+        const dim3 sgrd((unsigned)((nf + 127) / 128), pb_.nshots);
         if (pb_.nmodels == 3) k_elastic_face_sat<ELASTIC><<<sgrd, 128, 0, s>>>(f, nf);
         else k_elastic_face_sat<VTI><<<sgrd, 128, 0, s>>>(f, nf);
         CK(cudaGetLastError());
@@ -1080,10 +1098,8 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
             sat.y0 = 0;
             sat.y1 = pb_.ny;
         }
-        const int64_t ly = sat.y1 - sat.y0;
-        int64_t nf = 2 * (int64_t)pb_.nx * ly + 2 * (int64_t)(pb_.nz - 2) * ly;
-        if (slab_march_) nf += 2 * (int64_t)(pb_.nx - 2) * (pb_.nz - 2);
-        const dim3 sgrd((unsigned)((nf + 127) / 128), pb_.nshots, 3);
+        const int nf = face_points(pb_, sat.y0, sat.y1);
+        const dim3 sgrd((unsigned)((nf + 127) / 128), pb_.nshots);
         if (pb_.nmodels == 3) k_elastic_face_sat<ELASTIC><<<sgrd, 128, 0, s>>>(sat, nf);
         else k_elastic_face_sat<VTI><<<sgrd, 128, 0, s>>>(sat, nf);
     }
