@@ -644,6 +644,18 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     cudaStream_t s;
     CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     stream_ = s;
+    const char *cc = std::getenv("FWI_CONCURRENT");
+    conc_ = !(cc && cc[0] == '0');
+    if (conc_) {
+        cudaStream_t s2;
+        cudaEvent_t e0, e1;
+        CK(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+        side_ = s2;
+        CK(cudaEventCreateWithFlags(&e0, cudaEventDisableTiming));
+        ev_fork_ = e0;
+        CK(cudaEventCreateWithFlags(&e1, cudaEventDisableTiming));
+        ev_join_ = e1;
+    }
     const int64_t n = pb.nxyz();
     const int nc = pb.ncomp();
     fields_.alloc(sizeof(float) * 3 * (size_t)pb.nshots * nc * n);
@@ -731,6 +743,12 @@ Engine::~Engine()
         cudaStreamSynchronize((cudaStream_t)stream_);
         cudaStreamDestroy((cudaStream_t)stream_);
     }
+    if (side_) {
+        cudaStreamSynchronize((cudaStream_t)side_);
+        cudaStreamDestroy((cudaStream_t)side_);
+    }
+    if (ev_fork_) cudaEventDestroy((cudaEvent_t)ev_fork_);
+    if (ev_join_) cudaEventDestroy((cudaEvent_t)ev_join_);
     for (void *e : kev_) cudaEventDestroy((cudaEvent_t)e);
 }
 
@@ -1006,12 +1024,23 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         step_range(0, pb_.ny);
         kmark(false, nullptr, 0);
     } else {
+        // With a second stream the y-wall slabs and the paired kernel's edge
+        // tiles run on it beside the interior tiles (they write disjoint
+        // points of next); the SAT, which adds to face points of all of them,
+        // follows the join.  The main-kernel timing keeps one stream.
+        const bool conc = side_ && slab_march_ && pb_.nmodels == 3 && pair_ && pair_edge_ == 2 && !ktime_;
+        cudaStream_t se = s;
+        if (conc) {
+            se = (cudaStream_t)side_;
+            CK(cudaEventRecord((cudaEvent_t)ev_fork_, s));
+            CK(cudaStreamWaitEvent(se, (cudaEvent_t)ev_fork_, 0));
+        }
         if (slab_march_) {
             // planes near the y walls: the marching kernel (y closures), two chunks per tile column
             const int kz3 = (pb_.nz + f3::TZ - 1) / f3::TZ, kx3 = (pb_.nx + f3::TX - 1) / f3::TX;
             const dim3 grd3(kz3, kx3, 2 * pb_.nshots), mblk(f3::TZ, f3::TX);
-            if (pb_.nmodels == 3) k_elastic_march<ELASTIC><<<grd3, mblk, sizeof(MarchSmem), s>>>(a, 2, P);
-            else k_elastic_march<VTI><<<grd3, mblk, sizeof(MarchSmem), s>>>(a, 2, P);
+            if (pb_.nmodels == 3) k_elastic_march<ELASTIC><<<grd3, mblk, sizeof(MarchSmem), se>>>(a, 2, P);
+            else k_elastic_march<VTI><<<grd3, mblk, sizeof(MarchSmem), se>>>(a, 2, P);
         } else {
             // planes near the y walls: per-point kernels (derivative scratch two planes deeper)
             if (pb_.ny < 2 * (P + 2)) {
@@ -1064,7 +1093,7 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
                 for (int mode = 3; mode <= 5; mode++) {
                     if (tiles[mode - 3] == 0) continue;
                     const int nm = chunks(tiles[mode - 3] * pb_.nshots, 2);
-                    pair_launch(even, mode, dim3(kz, kx, nm * pb_.nshots), sm, s, f, nm, tm, 0, 0);
+                    pair_launch(even, mode, dim3(kz, kx, nm * pb_.nshots), sm, se, f, nm, tm, 0, 0);
                 }
             } else if (te > 0) {
                 // tiles with a z face: the one-point-per-thread kernel; with x faces only: the paired one
@@ -1072,6 +1101,10 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
                 if (pair_edge_ == 1) pair_launch(even, 3, dim3(kz, kx, ne * pb_.nshots), sm, s, f, ne, tm, 0, 0);
             }
             if (ti > 0) pair_launch(even, 1, dim3(zh - zl, xh - xl, ni * pb_.nshots), sm, s, f, ni, tm, zl, xl);
+            if (conc) {
+                CK(cudaEventRecord((cudaEvent_t)ev_join_, se));
+                CK(cudaStreamWaitEvent(s, (cudaEvent_t)ev_join_, 0));
+            }
         } else if (split) {
             const int64_t ti = (int64_t)(zh - zl) * (xh - xl) * pb_.nshots;
             const int64_t te = (int64_t)kz * kx * pb_.nshots - ti;

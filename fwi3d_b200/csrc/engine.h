@@ -179,6 +179,11 @@ private:
     int sm_count_ = 148;           // streaming multiprocessors of the device
     Problem pb_;
     void *stream_ = nullptr;
+    // second stream of a step: the edge tiles and y-wall slabs run beside the
+    // interior tiles (fork and join events on stream_); FWI_CONCURRENT=0 keeps
+    // one stream
+    void *side_ = nullptr, *ev_fork_ = nullptr, *ev_join_ = nullptr;
+    bool conc_ = true;
     DevBuf model_;                 // [nm][nxyz]
     DevBuf w2c_;                   // closure weights of the D2var coefficients per axis (StepArgs::w2c)
     const float *w2c_ptr_[3][3] = {};

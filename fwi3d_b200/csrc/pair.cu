@@ -34,6 +34,7 @@ __device__ __forceinline__ void pair_march(FusedCtx &c, int tid, int ya, int yb)
     for (int y = ya - 4; y < yb; y++) {
         fz_slots<ELASTIC>(c, y);
         const ColIn cin = pz_col_in<EVEN, ZQ>(c, tid, y + 2);
+        pz_prefetch_next(c, tid, y);
         // plane y+4: copied in here on the first step, else during the previous one
         if (y == ya - 4) {
             if (!c.tma) pz_load_u<false>(c, tid, y + 4, c.sl[6]);

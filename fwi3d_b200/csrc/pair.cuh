@@ -381,6 +381,40 @@ FWI_HD void pz_load_mat(FusedCtx &c, int tid, int y)
     }
 }
 
+// L2 prefetch hint (no register result): the closure weights and face
+// divisors of the next plane are requested a step ahead of their use.
+FWI_HD void prefetch_l2(const void *p)
+{
+#if defined(__CUDA_ARCH__)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+#else
+    (void)p;
+#endif
+}
+
+// L2 prefetch of the next step's global inputs, so that their loads (issued
+// a phase ahead of use) find them in L2 rather than in HBM.  By warp: the
+// material plane y+2 (mu, lambda; tile and halo rows), the column's
+// materials of plane y+3 (mu, lambda), rho and the three prev components of
+// plane y+1.  A lane takes one x row and prefetches the first, middle and
+// last word of its z span (at most three 128-byte lines).
+FWI_HD void pz_prefetch_next(const FusedCtx &c, int tid, int y)
+{
+    const StepArgs &a = *c.a;
+    const Dims &g = a.g;
+    const int w = tid >> 5, l = tid & 31;
+    const bool mat = w < 2;
+    const int q = mat ? y + 2 : w < 4 ? y + 3 : y + 1;
+    const int ix = mat ? c.x0 - fz::HD + l : c.x0 + l;
+    if (l >= (mat ? fz::XH : fz::TX) || ix < 0 || ix >= g.nx || q >= g.ny) return;
+    const float *base = w == 0 || w == 2 ? a.m[1] : w == 1 || w == 3 ? a.m[0] : w == 4 ? a.m[2] : a.prev[w - 5] + c.so;
+    const int za = max(mat ? c.z0 - fz::HD : c.z0, 0), zb = min((mat ? c.z0 + fz::TZ + fz::HD : c.z0 + fz::TZ) - 1, g.nz - 1);
+    const float *row = base + g.idx(ix, q, 0);
+    prefetch_l2(row + za);
+    prefetch_l2(row + (za + zb) / 2);
+    prefetch_l2(row + zb);
+}
+
 // Global inputs of the own pair, loaded one phase before they are used so
 // that their latency overlaps shared-memory work: mu and lambda of the column
 // plane, rho and the three prev components of the output plane.
@@ -496,16 +530,6 @@ FWI_HD F2 pzd1(const FusedCtx &c, const float *p, int iz, int zoff, F2 c0h, F2 c
     return d1p(z.m, z.m1(), z.p1(), z.b, c0h, c1h);
 }
 
-// L2 prefetch hint (no register result): the closure weights and face
-// divisors of the next plane are requested a step ahead of their use.
-FWI_HD void prefetch_l2(const void *p)
-{
-#if defined(__CUDA_ARCH__)
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
-#else
-    (void)p;
-#endif
-}
 
 // Absorbing-boundary scale of point (ix, y, iz) of component k (boundary_scale),
 // with a prefetch of the same face's divisor at plane y+1.  Planes of the
@@ -760,14 +784,19 @@ FWI_HD void pz_phase_b(const FusedCtx &c, const PairK &K, const PairThread &th, 
     st2(&fz_dvp(c.sm, DV_Z0)[xh][zh], mul2(mu0, uz0));
     st2(&fz_dvp(c.sm, DV_X2)[xh][zh], mul2(mu0, ux2));
     st2(&fz_dvp(c.sm, DV_Y2)[xh][zh], mul2(mu0, uy2));
-    // halo of the derived planes: rows 0, 1, XH-2, XH-1 (T, Y0, Z0) by
-    // threads 0..63, the first and last pair of rows 2..XH-3 (T, X2, Y2) by
-    // threads 64..95 (warp-uniform split)
-    if (tid < 4 * pz::NPR) {
-        const int r = tid / pz::NPR;
-        pz_derived_halo<true, XC, ZC>(c, K, r < 2 ? r : fz::XH - 4 + r, fz::HD + 2 * (tid % pz::NPR));
-    } else if (tid < 4 * pz::NPR + 2 * pz::TX) {
-        const int u = tid - 4 * pz::NPR;
+    // halo of the derived planes: rows 0, 1, XH-2, XH-1 (T, Y0, Z0) by the
+    // first two of three warps from warp hw, the first and last pair of rows
+    // 2..XH-3 (T, X2, Y2) by the third (warp-uniform split).  hw keeps this
+    // work off the warps that hold closure rows: warps 0..2 in a tile whose
+    // first x rows are closure rows, warps 0, 1 or 6, 7 (the z faces' pair
+    // blocks) in the z-face layout.
+    const int hw = (ZC && !XC) ? 2 : (XC && (c.x0 < 6 || c.x0 >= g.nx - 6)) ? 5 : 0;
+    const int ht = (tid - 32 * hw) & (pz::NT - 1);
+    if (ht < 4 * pz::NPR) {
+        const int r = ht / pz::NPR;
+        pz_derived_halo<true, XC, ZC>(c, K, r < 2 ? r : fz::XH - 4 + r, fz::HD + 2 * (ht % pz::NPR));
+    } else if (ht < 4 * pz::NPR + 2 * pz::TX) {
+        const int u = ht - 4 * pz::NPR;
         pz_derived_halo<false, XC, ZC>(c, K, fz::HD + (u >> 1), (u & 1) ? fz::ZH - 2 : 0);
     }
 }
