@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <chrono>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -147,7 +148,94 @@ struct fwi_batch {
     int it = 0;  // time steps run since reset
     Problem pb{};
     std::unique_ptr<Engine> eng;
+    std::vector<float> sxyz, rxyz;  // geometry of every slot: [nshots][3], [nshots][nr][5]
+    std::vector<int> t0;            // start step of every slot (shot slots)
 };
+
+namespace {
+// DAS channel s*nr + r of a [nshots][nr][5] receiver array: its fibre, and
+// the projection weights of dipole_to_strain (misc.cpp:11-42) as that
+// routine forms them in float.
+std::vector<Loc5> shot_fibres(const float *rxyz, int s, int nr)
+{
+    std::vector<Loc5> l(nr);
+    const float *r5 = rxyz + (size_t)5 * nr * s;
+    for (int r = 0; r < nr; r++) l[r] = Loc5{r5[5 * r], r5[5 * r + 1], r5[5 * r + 2], r5[5 * r + 3], r5[5 * r + 4]};
+    return l;
+}
+std::vector<float> das_weights(const float *rxyz, int s0, int nsh, int nr)
+{
+    std::vector<float> w((size_t)nsh * nr * 3);
+    for (int b = 0; b < nsh; b++)
+        for (int r = 0; r < nr; r++) {
+            const float *r5 = rxyz + ((size_t)(s0 + b) * nr + r) * 5;
+            const float cd = (float)std::cos((double)r5[3]), sd = (float)std::sin((double)r5[3]);
+            const float ca = (float)std::cos((double)r5[4]), sa = (float)std::sin((double)r5[4]);
+            float *o = w.data() + ((size_t)b * nr + r) * 3;
+            o[0] = cd * ca;
+            o[1] = cd * sa;
+            o[2] = sd;
+        }
+    return w;
+}
+
+// Injection and extraction tables of a batch's current geometry (gidx offset
+// by shot; source traces shot * nscomp + component).
+void batch_tables(const fwi_batch &b, InjTable &all, ExtTable &ext)
+{
+    const Problem &p = b.pb;
+    const int64_t n = p.nxyz();
+    const int nc = p.ncomp();
+    ext.nrec = b.nshots * b.nr;
+    for (int s = 0; s < b.nshots; s++) {
+        const float *sx = b.sxyz.data() + 3 * s;
+        PointOp inj = make_delta(p.nx, p.ny, p.nz, p.dx, p.dy, p.dz, b.grid.ox, b.grid.oy, b.grid.oz,
+                                 {Loc{sx[0], sx[1], sx[2]}}, b.par.mt != 0);
+        InjTable t = injection_table(inj, p.nx, p.ny, p.nz, nc);
+        for (int c = 0; c < nc; c++)
+            for (size_t k = 0; k < t.gidx[c].size(); k++) {
+                all.gidx[c].push_back(t.gidx[c][k] + s * n);
+                all.trace[c].push_back(t.trace[c][k] + s * b.nscomp);
+                all.w[c].push_back(t.w[c][k]);
+            }
+        ExtTable e;
+        if (b.par.gl > 0) {
+            // DAS: the channel's two dipole ends (dipole_m3, injector.cpp:313-493)
+            e = dipole_extraction_table(make_dipole(p.nx, p.ny, p.nz, p.dx, p.dy, p.dz, b.grid.ox, b.grid.oy, b.grid.oz,
+                                                    shot_fibres(b.rxyz.data(), s, b.nr), b.par.gl),
+                                        p.nx, p.ny, p.nz);
+        } else {
+            std::vector<Loc> rl(b.nr);
+            const float *rs = b.rxyz.data() + (size_t)5 * b.nr * s;
+            for (int r = 0; r < b.nr; r++) rl[r] = Loc{rs[5 * r], rs[5 * r + 1], rs[5 * r + 2]};
+            PointOp rop = make_delta(p.nx, p.ny, p.nz, p.dx, p.dy, p.dz, b.grid.ox, b.grid.oy, b.grid.oz, rl, false);
+            e = extraction_table(rop, p.nx, p.ny, p.nz);
+        }
+        ext.ntap = e.ntap;
+        for (auto g : e.gidx) ext.gidx.push_back(g + s * n);
+        ext.w.insert(ext.w.end(), e.w.begin(), e.w.end());
+    }
+}
+
+// Raw traces [nrcomp*nr][nt] of one shot to data [nrcomp*nr][nt_data]: time
+// derivative for velocity data, dt/dt_data, resampling (as fwi_batch_traces).
+void batch_shot_output(const fwi_batch &b, float *r, float *d)
+{
+    const int nt = b.pb.nt;
+    const int ntr = b.nrcomp * b.nr;
+    std::vector<float> v;
+    if (b.par.seismotype == 1) {
+        v.resize((size_t)ntr * nt);
+        apply_dt(false, r, v.data(), ntr, nt, b.pb.dt);
+        r = v.data();
+    }
+    const float alpha = b.pb.dt / b.dt_data;
+    for (size_t i = 0; i < (size_t)ntr * nt; i++) r[i] *= alpha;
+    std::fill(d, d + (size_t)ntr * b.nt_data, 0.f);
+    resample_adjoint(b.par.resampling_linear == 0, b.par.sinc_half_length, d, b.nt_data, b.dt_data, r, nt, b.pb.dt,
+                     ntr);
+}
+}  // namespace
 
 struct fwi_objective {
     int device = 0;
@@ -159,11 +247,29 @@ struct fwi_objective {
     int nshots = 1, nr = 0, nscomp = 1, nrcomp = 1, batch = 1;
     std::vector<float> wavelet, sxyz, rxyz, observed;
     double dnorm = 1.0;
+    int normalize = 1;
     Problem pb{};
     std::map<int, std::unique_ptr<Engine>> eng;  // one engine per batch size
     int64_t device_bytes = 0;
     DeviceResidual dres;  // residual on the device (observed traces, resampling taps)
 };
+
+namespace {
+// Normalisation of the misfit (nlls_fwi::_dnorm, optimization.hpp:386-393):
+// sum of the squared observed data times dt, or 1; over all shots, or (sh
+// >= 0) over shot sh alone (each request of a batched gradient is normalised
+// by its own data).
+double data_norm(const fwi_objective &o, int sh = -1)
+{
+    if (!o.normalize) return 1.0;
+    const size_t nd = (size_t)o.nrcomp * o.nr * o.nt_data;
+    const size_t b = sh < 0 ? 0 : (size_t)sh * nd, e = sh < 0 ? o.observed.size() : b + nd;
+    double ss = 0;
+    for (size_t i = b; i < e; i++) ss += (double)o.observed[i] * o.observed[i];
+    const double dn = ss * o.dt_data;
+    return dn < 1e-16 ? 1.0 : dn;
+}
+}  // namespace
 
 extern "C" {
 
@@ -407,9 +513,6 @@ int fwi_batch_create(fwi_batch **out, int device, const fwi_grid *grid, int nmod
     *out = nullptr;
     if (nmodels != 2 && nmodels != 3 && nmodels != 6)
         return fail(FWI_ERR_ARG, "The model must contain 2, 3, or 6 parameters");
-    if (par->gl > 0 && nmodels != 2)
-        return fail(FWI_ERR_UNSUPPORTED, "DAS receivers (gl > 0) are taken by the operator path (fwi_op_*); "
-                                         "batches and the objective take point receivers");
     return guarded([&] {
         std::unique_ptr<fwi_batch> b(new fwi_batch());
         b->device = device;
@@ -417,12 +520,20 @@ int fwi_batch_create(fwi_batch **out, int device, const fwi_grid *grid, int nmod
         b->nmodels = nmodels;
         b->par = *par;
         if (nmodels == 2) b->par.mt = 0;
+        if (nmodels == 2) b->par.gl = 0.f;  // analyzeGeometry, we_op.cpp:11-14
         b->nt_data = nt_data;
         b->dt_data = dt_data;
         b->nshots = nshots;
         b->nr = nr;
         b->nscomp = nmodels == 2 ? 1 : (b->par.mt ? 6 : 3);
-        b->nrcomp = nmodels == 2 ? 1 : 3;
+        b->nrcomp = nmodels == 2 ? 1 : (b->par.gl > 0 ? 1 : 3);  // DAS: strain along each fibre
+        if (b->par.gl > 0)
+            for (int s = 0; s < nshots; s++)
+                for (const Loc5 &l : shot_fibres(rxyz, s, nr))
+                    if (!dipole_inside(l, b->par.gl, grid->nx, grid->ny, grid->nz, grid->dx, grid->dy, grid->dz,
+                                       grid->ox, grid->oy, grid->oz))
+                        throw FwiError(FWI_ERR_ARG, "a DAS channel has its gauge length falling outside subsurface "
+                                                    "model boundaries");
         const int64_t n = (int64_t)grid->nx * grid->ny * grid->nz;
         if (!finite_all(model, nmodels * n)) throw FwiError(FWI_ERR_NAN, "model contains non-finite values");
         std::vector<float> m(model, model + nmodels * n);
@@ -455,30 +566,15 @@ int fwi_batch_create(fwi_batch **out, int device, const fwi_grid *grid, int nmod
         resample_forward(sinc, b->par.sinc_half_length, w.data(), nt_data, dt_data, w1.data(), p.nt, p.dt, b->nscomp);
         std::vector<float> src((size_t)nshots * b->nscomp * p.nt);
         for (int s = 0; s < nshots; s++) std::memcpy(src.data() + (size_t)s * w1.size(), w1.data(), sizeof(float) * w1.size());
-        const int nc = p.ncomp();
+        b->sxyz.assign(sxyz, sxyz + 3 * (size_t)nshots);
+        b->rxyz.assign(rxyz, rxyz + 5 * (size_t)nr * nshots);
+        b->t0.assign(nshots, 0);
         InjTable all;
         ExtTable ext;
-        ext.nrec = nshots * nr;
-        for (int s = 0; s < nshots; s++) {
-            PointOp inj = make_delta(p.nx, p.ny, p.nz, p.dx, p.dy, p.dz, grid->ox, grid->oy, grid->oz,
-                                     {Loc{sxyz[3 * s], sxyz[3 * s + 1], sxyz[3 * s + 2]}}, b->par.mt != 0);
-            InjTable t = injection_table(inj, p.nx, p.ny, p.nz, nc);
-            for (int c = 0; c < nc; c++)
-                for (size_t k = 0; k < t.gidx[c].size(); k++) {
-                    all.gidx[c].push_back(t.gidx[c][k] + s * n);
-                    all.trace[c].push_back(t.trace[c][k] + s * b->nscomp);
-                    all.w[c].push_back(t.w[c][k]);
-                }
-            std::vector<Loc> rl(nr);
-            const float *rs = rxyz + (size_t)5 * nr * s;
-            for (int r = 0; r < nr; r++) rl[r] = Loc{rs[5 * r], rs[5 * r + 1], rs[5 * r + 2]};
-            PointOp rop = make_delta(p.nx, p.ny, p.nz, p.dx, p.dy, p.dz, grid->ox, grid->oy, grid->oz, rl, false);
-            ExtTable e = extraction_table(rop, p.nx, p.ny, p.nz);
-            for (auto g : e.gidx) ext.gidx.push_back(g + s * n);
-            ext.w.insert(ext.w.end(), e.w.begin(), e.w.end());
-        }
+        batch_tables(*b, all, ext);
         b->eng->set_sources(all, nshots * b->nscomp, src.data());
         b->eng->set_receivers(ext, nr);
+        if (b->par.gl > 0) b->eng->set_das(das_weights(rxyz, 0, nshots, nr), nr, b->par.gl);
         b->eng->sync();
         *out = b.release();
     });
@@ -490,6 +586,7 @@ int fwi_batch_reset(fwi_batch *b)
     return guarded([&] {
         b->eng->reset();
         b->it = 0;
+        std::fill(b->t0.begin(), b->t0.end(), 0);
     });
 }
 
@@ -497,9 +594,80 @@ int fwi_batch_run(fwi_batch *b, int nsteps)
 {
     if (!b || nsteps < 0) return fail(FWI_ERR_ARG, "bad argument");
     return guarded([&] {
-        const int k = std::min(nsteps, b->pb.nt - 1 - b->it);
+        // shot slots: no common end, each slot's sources and receivers stop at its own
+        const int k = b->eng->continuous() ? nsteps : std::min(nsteps, b->pb.nt - 1 - b->it);
+        if ((int64_t)b->it + k > INT32_MAX - 2 * (int64_t)b->pb.nt)
+            throw FwiError(FWI_ERR_ARG, "time index range of the batch exhausted");
         b->eng->run(b->it, k);
         b->it += k;
+    });
+}
+
+int fwi_batch_enable_slots(fwi_batch *b)
+{
+    if (!b) return fail(FWI_ERR_ARG, "null batch");
+    return guarded([&] {
+        if (b->it != 0) throw FwiError(FWI_ERR_STATE, "shot slots are enabled at time index 0 (after a reset)");
+        b->eng->set_continuous();
+        std::fill(b->t0.begin(), b->t0.end(), 0);
+    });
+}
+
+int fwi_batch_join(fwi_batch *b, int slot, const float *sxyz, const float *rxyz)
+{
+    if (!b || !sxyz || !rxyz) return fail(FWI_ERR_ARG, "null argument");
+    if (slot < 0 || slot >= b->nshots) return fail(FWI_ERR_ARG, "slot out of range");
+    return guarded([&] {
+        const std::vector<float> s0(b->sxyz), r0(b->rxyz);
+        std::memcpy(b->sxyz.data() + 3 * (size_t)slot, sxyz, sizeof(float) * 3);
+        std::memcpy(b->rxyz.data() + 5 * (size_t)b->nr * slot, rxyz, sizeof(float) * 5 * b->nr);
+        InjTable all;
+        ExtTable ext;
+        try {
+            if (b->par.gl > 0) {
+                for (const Loc5 &l : shot_fibres(b->rxyz.data(), slot, b->nr))
+                    if (!dipole_inside(l, b->par.gl, b->grid.nx, b->grid.ny, b->grid.nz, b->grid.dx, b->grid.dy,
+                                       b->grid.dz, b->grid.ox, b->grid.oy, b->grid.oz))
+                        throw FwiError(FWI_ERR_ARG, "a DAS channel has its gauge length falling outside subsurface "
+                                                    "model boundaries");
+            }
+            batch_tables(*b, all, ext);
+            b->eng->join_shot(slot, all, ext, b->it);
+            if (b->par.gl > 0) b->eng->set_das(das_weights(b->rxyz.data(), 0, b->nshots, b->nr), b->nr, b->par.gl);
+        } catch (...) {
+            b->sxyz = s0;  // the slot keeps its shot
+            b->rxyz = r0;
+            throw;
+        }
+        b->t0[slot] = b->it;
+    });
+}
+
+int fwi_batch_release(fwi_batch *b, int slot)
+{
+    if (!b || slot < 0 || slot >= b->nshots) return fail(FWI_ERR_ARG, "bad argument");
+    return guarded([&] { b->eng->release_shot(slot); });
+}
+
+int fwi_batch_slot_time(const fwi_batch *b, int slot, int *t0, int *remaining)
+{
+    if (!b || slot < 0 || slot >= b->nshots) return fail(FWI_ERR_ARG, "bad argument");
+    if (t0) *t0 = b->t0[slot];
+    // the last sample (local nt-1) is read by the step run at t0 + nt - 1
+    if (remaining) *remaining = std::max(0, b->t0[slot] + b->pb.nt - b->it);
+    return FWI_OK;
+}
+
+int fwi_batch_slot_traces(fwi_batch *b, int slot, float *data)
+{
+    if (!b || !data || slot < 0 || slot >= b->nshots) return fail(FWI_ERR_ARG, "bad argument");
+    return guarded([&] {
+        if (!b->eng->continuous()) throw FwiError(FWI_ERR_STATE, "slot traces need a batch with shot slots");
+        if (b->it < b->t0[slot] + b->pb.nt) throw FwiError(FWI_ERR_STATE, "the slot's time axis has not been run to the end");
+        std::vector<float> rcv((size_t)b->nrcomp * b->nr * b->pb.nt);
+        if (b->par.gl > 0) b->eng->copy_strain(slot, 1, rcv.data());  // strain along the fibres, on the device
+        else b->eng->copy_shot_traces(slot, rcv.data());
+        batch_shot_output(*b, rcv.data(), data);
     });
 }
 
@@ -520,27 +688,16 @@ int fwi_batch_traces(fwi_batch *b, float *data)
 {
     if (!b || !data) return fail(FWI_ERR_ARG, "null argument");
     return guarded([&] {
+        if (b->eng->continuous()) throw FwiError(FWI_ERR_STATE, "a batch with shot slots returns traces per slot");
         if (b->it != b->pb.nt - 1) throw FwiError(FWI_ERR_STATE, "the time axis has not been run to the end");
         b->eng->extract_last();
         const int nt = b->pb.nt;
         const int ntr = b->nrcomp * b->nr;
         std::vector<float> rcv((size_t)b->nshots * ntr * nt);
-        b->eng->copy_traces(rcv.data());
-        const bool sinc = b->par.resampling_linear == 0;
-        const float alpha = b->pb.dt / b->dt_data;
-        for (int s = 0; s < b->nshots; s++) {
-            float *r = rcv.data() + (size_t)s * ntr * nt;
-            std::vector<float> v;
-            if (b->par.seismotype == 1) {
-                v.resize((size_t)ntr * nt);
-                apply_dt(false, r, v.data(), ntr, nt, b->pb.dt);
-                r = v.data();
-            }
-            for (size_t i = 0; i < (size_t)ntr * nt; i++) r[i] *= alpha;
-            float *d = data + (size_t)s * ntr * b->nt_data;
-            std::fill(d, d + (size_t)ntr * b->nt_data, 0.f);
-            resample_adjoint(sinc, b->par.sinc_half_length, d, b->nt_data, b->dt_data, r, nt, b->pb.dt, ntr);
-        }
+        if (b->par.gl > 0) b->eng->copy_strain(0, b->nshots, rcv.data());  // strain along the fibres, on the device
+        else b->eng->copy_traces(rcv.data());
+        for (int s = 0; s < b->nshots; s++)
+            batch_shot_output(*b, rcv.data() + (size_t)s * ntr * nt, data + (size_t)s * ntr * b->nt_data);
     });
 }
 
@@ -598,9 +755,6 @@ int fwi_objective_create(fwi_objective **out, int device, const fwi_grid *grid, 
         return fail(FWI_ERR_ARG, "The model must contain 2, 3, or 6 parameters");
     if (grid->nx < 12 || grid->ny < 12 || grid->nz < 12) return fail(FWI_ERR_ARG, "each grid axis needs at least 12 points");
     if (nt_data < 2 || !(dt_data > 0)) return fail(FWI_ERR_ARG, "the wavelet needs at least 2 samples and dt > 0");
-    if (par->gl > 0 && nmodels != 2)
-        return fail(FWI_ERR_UNSUPPORTED, "DAS receivers (gl > 0) are taken by the operator path (fwi_op_*); "
-                                         "batches and the objective take point receivers");
     return guarded([&] {
         std::unique_ptr<fwi_objective> o(new fwi_objective());
         o->device = device;
@@ -613,7 +767,15 @@ int fwi_objective_create(fwi_objective **out, int device, const fwi_grid *grid, 
         o->nshots = nshots;
         o->nr = nr;
         o->nscomp = nmodels == 2 ? 1 : (o->par.mt ? 6 : 3);
-        o->nrcomp = nmodels == 2 ? 1 : 3;
+        if (nmodels == 2) o->par.gl = 0.f;  // analyzeGeometry, we_op.cpp:11-14
+        o->nrcomp = nmodels == 2 ? 1 : (o->par.gl > 0 ? 1 : 3);  // DAS: strain along each fibre
+        if (o->par.gl > 0)
+            for (int s = 0; s < nshots; s++)
+                for (const Loc5 &l : shot_fibres(rxyz, s, nr))
+                    if (!dipole_inside(l, o->par.gl, grid->nx, grid->ny, grid->nz, grid->dx, grid->dy, grid->dz,
+                                       grid->ox, grid->oy, grid->oz))
+                        throw FwiError(FWI_ERR_ARG, "a DAS channel has its gauge length falling outside subsurface "
+                                                    "model boundaries");
         o->batch = batch < 1 ? nshots : std::min(batch, nshots);
         o->wavelet = expand_wavelet(wavelet, wavelet_ncomp, nt_data, nmodels, o->par);
         o->sxyz.assign(sxyz, sxyz + 3 * nshots);
@@ -621,22 +783,33 @@ int fwi_objective_create(fwi_objective **out, int device, const fwi_grid *grid, 
         const size_t nd = (size_t)nshots * o->nrcomp * nr * nt_data;
         o->observed.assign(observed, observed + nd);
         if (!finite_all(observed, (int64_t)nd)) throw FwiError(FWI_ERR_NAN, "observed data contain non-finite values");
-        double dn = 1.0;
-        if (normalize) {
-            double ss = 0;
-            for (size_t i = 0; i < nd; i++) ss += (double)observed[i] * observed[i];
-            dn = ss * dt_data;
-            if (dn < 1e-16) dn = 1.0;
-        }
-        o->dnorm = dn;
+        o->normalize = normalize;
+        o->dnorm = data_norm(*o);
         *out = o.release();
     });
 }
 
-int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, float *grad, float *residual)
+int fwi_objective_set_shots(fwi_objective *o, const float *sxyz, const float *rxyz, const float *observed)
 {
-    if (!o || !model || !f || !grad) return fail(FWI_ERR_ARG, "null argument");
+    if (!o || !sxyz || !rxyz || !observed) return fail(FWI_ERR_ARG, "null argument");
     return guarded([&] {
+        const size_t nd = o->observed.size();
+        if (!finite_all(observed, (int64_t)nd)) throw FwiError(FWI_ERR_NAN, "observed data contain non-finite values");
+        o->sxyz.assign(sxyz, sxyz + o->sxyz.size());
+        o->rxyz.assign(rxyz, rxyz + o->rxyz.size());
+        o->observed.assign(observed, observed + nd);
+        o->dnorm = data_norm(*o);
+    });
+}
+
+// The objective of all shots (f, grad: summed over the shots, residual
+// optional) or, with gs, one objective per shot: fs [nshots] and gs
+// [nshots][nm][nxyz], each normalised by its own data.
+static void objective_eval(fwi_objective *o, const float *model, double *f, float *grad, float *residual, double *fs,
+                           float *gs)
+{
+    {
+        const bool per_shot = gs != nullptr;
         const fwi_grid &g = o->grid;
         const int64_t n = (int64_t)g.nx * g.ny * g.nz;
         const int nm = std::min(3, o->nmodels);
@@ -664,13 +837,16 @@ int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, floa
             o->nmodels == 2 ? std::max(par.free_surface_stiffness, 1.0f) : par.free_surface_stiffness;
         const int nt = p.nt, ntd = o->nt_data;
         const int ncr = p.ncomp();
-        const int ntr = ncr * o->nr;
+        const int ntr = o->nrcomp * o->nr;  // data traces of a shot
+        const int ntr_raw = ncr * o->nr;    // extracted rows of a shot (DAS: the dipoles' three components)
+        const bool das = par.gl > 0;
         const bool sinc = par.resampling_linear == 0;
         const float alpha = p.dt / o->dt_data;
         // wavelet at the propagation sampling (same for every shot)
         std::vector<float> w1((size_t)o->nscomp * nt);
         resample_forward(sinc, par.sinc_half_length, o->wavelet.data(), ntd, o->dt_data, w1.data(), nt, p.dt, o->nscomp);
-        std::vector<double> gsum((size_t)nm * n, 0.0);
+        std::vector<double> gsum(per_shot ? 0 : (size_t)nm * n, 0.0);
+        std::vector<double> fshot(o->nshots, 0.0);
         double fsum = 0.0;
         o->device_bytes = 0;
         // FWI_OBJ_TIMING=1: per-batch phase times on stderr (host clock)
@@ -698,6 +874,7 @@ int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, floa
             eng->set_storage(par.snapshot_storage);
             eng->set_snapshot_budget((int64_t)((double)par.snapshot_budget_gb * 1e9));
             eng->set_checkpointing(par.checkpoint_slots, par.checkpoint_precision);
+            eng->set_per_shot_gradient(per_shot);
             eng->set_model(m.data());
             // tables of the batch (shot b of the batch at wavefield offset b)
             InjTable inj, adj;
@@ -715,8 +892,19 @@ int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, floa
                 const float *rs = &o->rxyz[(size_t)5 * o->nr * sh];
                 for (int r = 0; r < o->nr; r++) rl[r] = Loc{rs[5 * r], rs[5 * r + 1], rs[5 * r + 2]};
                 PointOp pr = make_delta(p.nx, p.ny, p.nz, p.dx, p.dy, p.dz, g.ox, g.oy, g.oz, rl, false);
-                InjTable ta2 = injection_table(pr, p.nx, p.ny, p.nz, ncr);
-                ExtTable e = extraction_table(pr, p.nx, p.ny, p.nz);
+                InjTable ta2;
+                ExtTable e;
+                if (das) {
+                    // the channels' dipoles (dipole_m3, injector.cpp:313-493; we_op.cpp:1015)
+                    const Dipole dp = make_dipole(p.nx, p.ny, p.nz, p.dx, p.dy, p.dz, g.ox, g.oy, g.oz,
+                                                  shot_fibres(o->rxyz.data(), sh, o->nr), par.gl);
+                    ta2 = dipole_injection_table(dp, p.nx, p.ny, p.nz, ncr);
+                    e = dipole_extraction_table(dp, p.nx, p.ny, p.nz);
+                } else {
+                    ta2 = injection_table(pr, p.nx, p.ny, p.nz, ncr);
+                    e = extraction_table(pr, p.nx, p.ny, p.nz);
+                }
+                ext.ntap = e.ntap;
                 for (int c = 0; c < ncr; c++) {
                     for (size_t k = 0; k < t.gidx[c].size(); k++) {
                         inj.gidx[c].push_back(t.gidx[c][k] + b * n);
@@ -725,27 +913,40 @@ int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, floa
                     }
                     for (size_t k = 0; k < ta2.gidx[c].size(); k++) {
                         adj.gidx[c].push_back(ta2.gidx[c][k] + b * n);
-                        adj.trace[c].push_back(ta2.trace[c][k] + b * ntr);
+                        adj.trace[c].push_back(ta2.trace[c][k] + b * ntr_raw);
                         adj.w[c].push_back(ta2.w[c][k]);
                     }
                 }
                 for (auto gi : e.gidx) ext.gidx.push_back(gi + b * n);
                 ext.w.insert(ext.w.end(), e.w.begin(), e.w.end());
             }
+            if (das) eng->set_das(das_weights(o->rxyz.data(), s0, B, o->nr), o->nr, par.gl);
             const auto t1 = now();
             if (on_device) {
                 eng->forward(inj, B * o->nscomp, src.data(), ext, nullptr, true);
+                // DAS: strain along the fibres, on the device (we_op.cpp:929)
+                const float *strain = das ? eng->strain_traces(0, B) : nullptr;
                 const auto t2 = now();
                 const size_t ntrb = (size_t)B * ntr;
                 nvtxRangePushA("fwi3d residual");
+                std::vector<double> pt(ntrb);
                 fsum += o->dres.run(*eng, (size_t)s0 * ntr * ntd, (int)ntrb, par.seismotype, alpha,
-                                    residual ? residual + (size_t)s0 * ntr * ntd : nullptr);
+                                    residual ? residual + (size_t)s0 * ntr * ntd : nullptr, pt.data(), strain);
                 nvtxRangePop();
-                std::vector<float> gb((size_t)nm * n);
+                for (int b = 0; b < B; b++)
+                    for (int tr = 0; tr < ntr; tr++) fshot[s0 + b] += pt[(size_t)b * ntr + tr];
+                std::vector<float> gb((size_t)(per_shot ? B : 1) * nm * n);
                 const auto t3 = now();
-                eng->adjoint_dev(adj, (int)ntrb, o->dres.adjoint_sources(), gb.data());
+                if (das) {
+                    // strain sources back to the dipoles' three components (we_op.cpp:1015)
+                    eng->adjoint_dev(adj, B * ntr_raw, eng->strain_adjoint(o->dres.adjoint_sources()), gb.data());
+                } else {
+                    eng->adjoint_dev(adj, (int)ntrb, o->dres.adjoint_sources(), gb.data());
+                }
                 const auto t4 = now();
-                for (size_t i = 0; i < gb.size(); i++) gsum[i] += gb[i];
+                if (per_shot) std::copy(gb.begin(), gb.end(), gs + (size_t)s0 * nm * n);
+                else
+                    for (size_t i = 0; i < gb.size(); i++) gsum[i] += gb[i];
                 if (timing)
                     std::fprintf(stderr,
                                  "objective batch %d: prep %.3f s, forward %.3f s, device residual %.3f s, adjoint %.3f s\n",
@@ -754,17 +955,26 @@ int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, floa
                 o->pb = p;
                 continue;
             }
-            std::vector<float> rcv((size_t)B * ntr * nt);
+            std::vector<float> rcv((size_t)B * ntr_raw * nt);
             eng->forward(inj, B * o->nscomp, src.data(), ext, rcv.data(), true);
             const auto t2 = now();
             if (!finite_all(rcv.data(), (int64_t)rcv.size())) throw FwiError(FWI_ERR_NAN, "non-finite values in the traces");
             const auto tr0 = now();
             double t_ra = 0, t_rf = 0;
-            std::vector<float> asrc((size_t)B * ntr * nt);
+            std::vector<float> asrc((size_t)B * ntr_raw * nt);
             std::vector<float> syn((size_t)ntr * ntd), tmp;
             for (int b = 0; b < B; b++) {
                 const int sh = s0 + b;
-                float *r = rcv.data() + (size_t)b * ntr * nt;
+                float *r = rcv.data() + (size_t)b * ntr_raw * nt;
+                if (das) {
+                    // strain along the fibres into component 0 (we_op.cpp:929)
+                    std::vector<float> dip(o->nr), az(o->nr);
+                    for (int q = 0; q < o->nr; q++) {
+                        dip[q] = o->rxyz[((size_t)sh * o->nr + q) * 5 + 3];
+                        az[q] = o->rxyz[((size_t)sh * o->nr + q) * 5 + 4];
+                    }
+                    dipole_to_strain(false, r, dip.data(), az.data(), o->nr, nt, par.gl);
+                }
                 if (par.seismotype == 1) {
                     tmp.resize((size_t)ntr * nt);
                     apply_dt(false, r, tmp.data(), ntr, nt, p.dt);
@@ -785,10 +995,11 @@ int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, floa
                     ss -= 0.5 * (a0 * a0 + a1 * a1);
                 }
                 fsum += ss;
+                fshot[sh] = ss;
                 if (residual) std::memcpy(residual + (size_t)sh * ntr * ntd, syn.data(), sizeof(float) * syn.size());
                 // adjoint sources: Ht(r) (optimization.cpp:118), then jacobianT's data path (we_op.cpp:994-1003)
                 apply_ht(false, syn.data(), syn.data(), ntr, ntd, o->dt_data);
-                float *as = asrc.data() + (size_t)b * ntr * nt;
+                float *as = asrc.data() + (size_t)b * ntr_raw * nt;
                 const auto tf0 = now();
                 resample_forward(sinc, par.sinc_half_length, syn.data(), ntd, o->dt_data, as, nt, p.dt, ntr);
                 t_rf += secs(tf0, now());
@@ -800,12 +1011,23 @@ int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, floa
                     apply_dt(true, as, tmp.data(), ntr, nt, p.dt);
                     std::memcpy(as, tmp.data(), sizeof(float) * tmp.size());
                 }
+                if (das) {
+                    // strain sources back to the dipoles' three components (we_op.cpp:1015)
+                    std::vector<float> dip(o->nr), az(o->nr);
+                    for (int q = 0; q < o->nr; q++) {
+                        dip[q] = o->rxyz[((size_t)sh * o->nr + q) * 5 + 3];
+                        az[q] = o->rxyz[((size_t)sh * o->nr + q) * 5 + 4];
+                    }
+                    dipole_to_strain(true, as, dip.data(), az.data(), o->nr, nt, par.gl);
+                }
             }
-            std::vector<float> gb((size_t)nm * n);
+            std::vector<float> gb((size_t)(per_shot ? B : 1) * nm * n);
             const auto t3 = now();
-            eng->adjoint(adj, B * ntr, asrc.data(), gb.data());
+            eng->adjoint(adj, B * ntr_raw, asrc.data(), gb.data());
             const auto t4 = now();
-            for (size_t i = 0; i < gb.size(); i++) gsum[i] += gb[i];
+            if (per_shot) std::copy(gb.begin(), gb.end(), gs + (size_t)s0 * nm * n);
+            else
+                for (size_t i = 0; i < gb.size(); i++) gsum[i] += gb[i];
             if (timing)
                 std::fprintf(stderr,
                              "objective batch %d: prep %.3f s, forward %.3f s, residual %.3f s (check %.3f, "
@@ -816,14 +1038,40 @@ int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, floa
             o->pb = p;
         }
         // H quadrature, chain rule to (vp, vs, rho), 1/dnorm (we_op.cpp:1027-1067, optimization.cpp:194)
+        if (f) *f = 0.5 * o->dt_data * fsum / o->dnorm;
+        if (per_shot) {
+            for (int sh = 0; sh < o->nshots; sh++) {
+                float *gsh = gs + (size_t)sh * nm * n;
+                for (int q = 0; q < nm; q++) apply_h3(gsh + q * n, p.nx, p.ny, p.nz, p.dx, p.dy, p.dz);
+                gradient_to_velocity(gsh, m.data(), o->nmodels, n);
+                const double dn = data_norm(*o, sh);
+                const float sc = (float)(1.0 / dn);
+                for (int64_t i = 0; i < nm * n; i++) gsh[i] *= sc;
+                fs[sh] = 0.5 * o->dt_data * fshot[sh] / dn;
+            }
+            if (!finite_all(gs, (int64_t)o->nshots * nm * n))
+                throw FwiError(FWI_ERR_NAN, "non-finite values in the gradient");
+            return;
+        }
         for (int64_t i = 0; i < nm * n; i++) grad[i] = (float)gsum[i];
         for (int q = 0; q < nm; q++) apply_h3(grad + q * n, p.nx, p.ny, p.nz, p.dx, p.dy, p.dz);
         gradient_to_velocity(grad, m.data(), o->nmodels, n);
         const float sc = (float)(1.0 / o->dnorm);
         for (int64_t i = 0; i < nm * n; i++) grad[i] *= sc;
-        *f = 0.5 * o->dt_data * fsum / o->dnorm;
         if (!finite_all(grad, nm * n)) throw FwiError(FWI_ERR_NAN, "non-finite values in the gradient");
-    });
+    }
+}
+
+int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, float *grad, float *residual)
+{
+    if (!o || !model || !f || !grad) return fail(FWI_ERR_ARG, "null argument");
+    return guarded([&] { objective_eval(o, model, f, grad, residual, nullptr, nullptr); });
+}
+
+int fwi_objective_evaluate_shots(fwi_objective *o, const float *model, double *f, float *grad)
+{
+    if (!o || !model || !f || !grad) return fail(FWI_ERR_ARG, "null argument");
+    return guarded([&] { objective_eval(o, model, nullptr, nullptr, nullptr, f, grad); });
 }
 
 int64_t fwi_objective_device_bytes(const fwi_objective *o) { return o ? o->device_bytes : 0; }

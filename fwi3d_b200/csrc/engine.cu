@@ -120,7 +120,7 @@ dim3 grid_of(const Dims &g, int nshots, int ny_launch = -1)
 __global__ void k_acoustic_step(StepArgs a)
 {
     int ix, iy, iz, s;
-    if (!point_of(a.g, a.nyb, a.y0, a.y1, ix, iy, iz, s)) return;
+    if (!point_of(a.g, a.nyb, a.y0, a.y1, ix, iy, iz, s) || shot_idle(a, s)) return;
     const StepArgs b = shot_args(a, s);
     b.next[0][b.g.idx(ix, iy, iz)] = acoustic_point(b, ix, iy, iz);
 }
@@ -137,7 +137,7 @@ template <int PH>
 __global__ void k_elastic_step(StepArgs a)
 {
     int ix, iy, iz, s;
-    if (!point_of(a.g, a.nyb, a.y0, a.y1, ix, iy, iz, s)) return;
+    if (!point_of(a.g, a.nyb, a.y0, a.y1, ix, iy, iz, s) || shot_idle(a, s)) return;
     const StepArgs b = shot_args(a, s);
     const int64_t i = b.g.idx(ix, iy, iz);
     const float v0 = elastic_point<PH>(b, 0, ix, iy, iz);
@@ -213,6 +213,7 @@ __global__ void __launch_bounds__(fz::NT, MINB)
     c.rows.p = c.sm->rows;
     const int tid = threadIdx.x + fz::TZ * threadIdx.y;
     c.shot = blockIdx.z / nchunks;
+    if (shot_idle(a, c.shot)) return;
     const int ch = blockIdx.z - c.shot * nchunks;
     c.so = c.shot * a.sst;
     tile_range(blockIdx.x, a.g.nz, fz::TZ, c.z0, c.zend);
@@ -254,6 +255,7 @@ __global__ void __launch_bounds__(fz::NT, 2)
     c.rows.p = c.sm->rows;
     const int tid = threadIdx.x + fz::TZ * threadIdx.y;
     c.shot = blockIdx.z / nchunks;
+    if (shot_idle(a, c.shot)) return;
     const int ch = blockIdx.z - c.shot * nchunks;
     c.so = c.shot * a.sst;
     tile_range(blockIdx.x + (MODE == 1 ? bz0 : 0), a.g.nz, fz::TZ, c.z0, c.zend);
@@ -284,6 +286,7 @@ __global__ void __launch_bounds__(fa::NT, 2) k_acoustic_fused(const __grid_const
     c.sm = &sm;
     const int tid = threadIdx.x + fa::TZ * threadIdx.y;
     const int shot = blockIdx.z / nchunks;
+    if (shot_idle(a, shot)) return;
     const int ch = blockIdx.z - shot * nchunks;
     c.so = shot * a.sst;
     tile_range(blockIdx.x, a.g.nz, fa::TZ, c.z0, c.zend);
@@ -320,6 +323,7 @@ __global__ void __launch_bounds__(f3::NT, 1) k_elastic_march(const __grid_consta
     c.rows.p = c.sm->rows;  // filled below; first read after the first phase's barrier
     const int tid = threadIdx.x + f3::TZ * threadIdx.y;
     const int shot = blockIdx.z / nchunks;
+    if (shot_idle(a, shot)) return;
     const int ch = blockIdx.z - shot * nchunks;
     c.so = shot * a.sst;
     tile_range(blockIdx.x, a.g.nz, f3::TZ, c.z0, c.zend);
@@ -393,7 +397,7 @@ __global__ void k_elastic_face_sat(const __grid_constant__ StepArgs a, int npts)
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= npts) return;
     int ix, iy, iz;
-    if (!face_point(a.g, a.y0, a.y1, k, ix, iy, iz)) return;
+    if (!face_point(a.g, a.y0, a.y1, k, ix, iy, iz) || shot_idle(a, blockIdx.y)) return;
     const int64_t so = (int64_t)blockIdx.y * a.sst;
     const int64_t i = a.g.idx(ix, iy, iz);
     float sat[3];
@@ -426,7 +430,7 @@ static int face_points(const Problem &pb, int y0, int y1)
 // (acoustic).  Equivalent to the reference's injection into the operator sum
 // before the update (we_op.cpp:691-693): update, scaling and taper are linear in it.
 __global__ void k_inject(StepArgs a, int c, const int64_t *gidx, const int *trace, const float *w, int n,
-                         const float *src, int nt, int it, const int *itp)
+                         const float *src, int nt, int it, const int *itp, const int *t0)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -435,6 +439,10 @@ __global__ void k_inject(StepArgs a, int c, const int64_t *gidx, const int *trac
     const int64_t gi = gidx[k];
     const int64_t sh = gi / nxyz;
     const int64_t i = gi - sh * nxyz;
+    if (t0) {
+        it -= t0[sh];  // shot slots: the shot's own time index
+        if (it < 0 || it >= nt) return;
+    }
     const float sv = w[k] * src[(int64_t)trace[k] * nt + it];
     const int iz = (int)(i % a.g.nz);
     const int ix = (int)((i / a.g.nz) % a.g.nx);
@@ -448,20 +456,22 @@ __global__ void k_inject(StepArgs a, int c, const int64_t *gidx, const int *trac
 
 // Initial condition prev = inject(src[:,0]) then scaled (we_op.cpp:611-619, 1635-1636).
 __global__ void k_inject0(float *prev, int64_t sst, int64_t nxyz, const int64_t *gidx, const int *trace,
-                          const float *w, int n, const float *src, int nt)
+                          const float *w, int n, const float *src, int nt, int only)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const int64_t gi = gidx[k];
     const int64_t sh = gi / nxyz;
+    if (only >= 0 && sh != only) return;
     atomicAdd(&prev[sh * sst + (gi - sh * nxyz)], w[k] * src[(int64_t)trace[k] * nt]);
 }
 
-__global__ void k_scale0(float *prev, int64_t sst, const float *coef, int64_t n, int nshots, float dt, int acoustic)
+__global__ void k_scale0(float *prev, int64_t sst, const float *coef, int64_t n, int nshots, float dt, int acoustic,
+                         int only)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    for (int s = 0; s < nshots; s++) {
+    for (int s = only >= 0 ? only : 0; s < (only >= 0 ? only + 1 : nshots); s++) {
         float *p = prev + s * sst + i;
         const float v = *p;
         if (v == 0.f) continue;
@@ -472,13 +482,17 @@ __global__ void k_scale0(float *prev, int64_t sst, const float *coef, int64_t n,
 
 // Receivers: rcv[s][c][r][it] = sum_k w_k u_c(g_k) (injector.cpp:118-140).
 __global__ void k_extract(const float *u, int64_t sst, int64_t nxyz, int ncomp, const int64_t *gidx, const float *w,
-                          int nrec, int nr, float *rcv, int nt, int it, int ntap, const int *itp)
+                          int nrec, int nr, float *rcv, int nt, int it, int ntap, const int *itp, const int *t0)
 {
     const int row = blockIdx.x * blockDim.x + threadIdx.x;
     const int c = blockIdx.y;
     if (row >= nrec) return;
     if (itp) it += *itp;
     const int sh = row / nr, r = row - sh * nr;
+    if (t0) {
+        it -= t0[sh];  // shot slots: the shot's own time index
+        if (it < 0 || it >= nt) return;
+    }
     const float *uc = u + sh * sst + c * nxyz;
     const int64_t b = (int64_t)ntap * row;
     float acc = 0.f;
@@ -555,8 +569,10 @@ __global__ void k_tick(int *itp, int by) { *itp += by; }
 // Imaging of every shot of a batch at once: the increments of the shots
 // (fields at offsets s * sst) are summed in FP64 per point, then added to the
 // gradient once.
+// gst > 0: one gradient per shot, shot s's at offset s * gst (its increments
+// are not summed with the other shots').
 template <int PH>
-__global__ void k_image_batch(ImageArgs a, int nshots, int64_t sst)
+__global__ void k_image_batch(ImageArgs a, int nshots, int64_t sst, int64_t gst)
 {
     int ix, iy, iz, s;
     if (!point_of(a.g, (a.g.ny + BY - 1) / BY, ix, iy, iz, s)) return;
@@ -577,7 +593,15 @@ __global__ void k_image_batch(ImageArgs a, int nshots, int64_t sst)
             g1 += i1;
             g2 += i2;
         }
+        if (gst) {
+            const int64_t o = sh * gst + i;
+            a.grad[0][o] += g0;
+            a.grad[1][o] += g1;
+            if (PH != ACOUSTIC) a.grad[2][o] += g2;
+            g0 = g1 = g2 = 0.0;
+        }
     }
+    if (gst) return;
     a.grad[0][i] += g0;
     a.grad[1][i] += g1;
     if (PH != ACOUSTIC) a.grad[2][i] += g2;
@@ -769,7 +793,8 @@ int64_t Engine::device_bytes() const
 {
     return model_.bytes + w2c_.bytes + fields_.bytes + aux_.bytes + snaps_.bytes + grad_.bytes + sdiv_.bytes + taper_.bytes +
            src_dev_.bytes + rcv_dev_.bytes + snapq_.bytes + snaps_scale_.bytes + enc_.bytes + amax_.bytes +
-           snapz_.bytes + rv_store_.bytes + rv_scale_.bytes + rec_fields_.bytes;
+           snapz_.bytes + rv_store_.bytes + rv_scale_.bytes + rec_fields_.bytes + grad_f32_.bytes + adj_src_buf_.bytes +
+           das_w_.bytes + das_rcv_.bytes + das_src_.bytes;
 }
 
 float *Engine::level(int l) const
@@ -904,7 +929,7 @@ StepArgs make_step_args(const Problem &pb, const float *m, const float *const sd
 }
 }  // namespace
 
-void Engine::init_prev(const DevInj &inj, const float *src_dev, float *prev)
+void Engine::init_prev(const DevInj &inj, const float *src_dev, float *prev, int only_shot)
 {
     cudaStream_t s = (cudaStream_t)stream_;
     const int64_t n = pb_.nxyz();
@@ -914,10 +939,10 @@ void Engine::init_prev(const DevInj &inj, const float *src_dev, float *prev)
         if (inj.n[c] == 0) continue;
         k_inject0<<<(inj.n[c] + 255) / 256, 256, 0, s>>>(prev + c * n, sst, n, inj.gidx[c].as<int64_t>(),
                                                           inj.trace[c].as<int>(), inj.w[c].as<float>(), inj.n[c],
-                                                          src_dev, pb_.nt);
+                                                          src_dev, pb_.nt, only_shot);
         const float *coef = model_.as<float>() + (pb_.nmodels == 2 ? 0 : 2 * n);
         k_scale0<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(prev + c * n, sst, coef, n, pb_.nshots, pb_.dt,
-                                                               pb_.nmodels == 2);
+                                                               pb_.nmodels == 2, only_shot);
     }
     CK(cudaGetLastError());
 }
@@ -937,6 +962,7 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
     for (int ax = 0; ax < 3; ax++)
         for (int f = 0; f < 3; f++) a.w2c[ax][f] = w2c_ptr_[ax][f];
     a.taper_prev = taper_prev ? 1 : 0;
+    a.active = continuous_ ? shot_active_.as<int>() : nullptr;
     const dim3 blk(BZ, BX, BY);
     // per-point launch over planes [y0, y1)
     auto range = [&](StepArgs &st, int y0, int y1) {
@@ -1149,7 +1175,8 @@ void Engine::inject(const DevInj &inj, const float *src_dev, int it, float *next
     for (int c = 0; c < nc; c++) {
         if (inj.n[c] == 0) continue;
         k_inject<<<(inj.n[c] + 127) / 128, 128, 0, s>>>(a, c, inj.gidx[c].as<int64_t>(), inj.trace[c].as<int>(),
-                                                         inj.w[c].as<float>(), inj.n[c], src_dev, pb_.nt, it, itp_);
+                                                         inj.w[c].as<float>(), inj.n[c], src_dev, pb_.nt, it, itp_,
+                                                         continuous_ ? shot_t0_.as<int>() : nullptr);
     }
     CK(cudaGetLastError());
 }
@@ -1162,7 +1189,8 @@ void Engine::extract(const DevExt &ext, const float *curr, float *rcv_dev, int i
     const int64_t n = pb_.nxyz();
     const dim3 grd((ext.nrec + 127) / 128, nc);
     k_extract<<<grd, 128, 0, s>>>(curr, (int64_t)nc * n, n, nc, ext.gidx.as<int64_t>(), ext.w.as<float>(), ext.nrec,
-                                  ext.nr, rcv_dev, pb_.nt, it, ext.ntap, itp_);
+                                  ext.nr, rcv_dev, pb_.nt, it, ext.ntap, itp_,
+                                  continuous_ ? shot_t0_.as<int>() : nullptr);
     CK(cudaGetLastError());
 }
 
@@ -1274,6 +1302,13 @@ void Engine::reset()
     rot_ = 0;
     fields_.zero(s);
     if (rcv_dev_.p) rcv_dev_.zero(s);
+    if (continuous_) {
+        // every slot restarts at step 0, active
+        shot_t0_.zero(s);
+        const std::vector<int> ones(pb_.nshots, 1);
+        CK(cudaMemcpyAsync(shot_active_.p, ones.data(), shot_active_.bytes, cudaMemcpyHostToDevice, s));
+        CK(cudaStreamSynchronize(s));
+    }
     init_prev(inj_, src_dev_.as<float>(), level(0));
     // capture the replayed steps here (nothing runs), so that the first run
     // does not pay for the capture and instantiation
@@ -1292,7 +1327,8 @@ void Engine::run_step(int it, bool taper_prev)
 uint64_t Engine::graph_key() const
 {
     const void *ptrs[] = {fields_.p, model_.p, src_dev_.p, rcv_dev_.p, inj_.gidx[0].p, inj_.gidx[1].p, inj_.gidx[2].p,
-                          inj_.trace[0].p, inj_.w[0].p, ext_.gidx.p, ext_.w.p, sdiv_.p, taper_.p, w2c_.p};
+                          inj_.trace[0].p, inj_.w[0].p, ext_.gidx.p, ext_.w.p, sdiv_.p, taper_.p, w2c_.p,
+                          continuous_ ? shot_t0_.p : nullptr, continuous_ ? shot_active_.p : nullptr};
     uint64_t h = 1469598103934665603ull;
     auto mix = [&](uint64_t v) { h = (h ^ v) * 1099511628211ull; };
     for (const void *p : ptrs) mix((uint64_t)(uintptr_t)p);
@@ -1346,7 +1382,8 @@ bool Engine::capture_graph()
 
 void Engine::run(int it0, int nsteps)
 {
-    const int end = std::min(it0 + nsteps, pb_.nt - 1);
+    // shot slots run past nt: each shot's sources and receivers stop at its own end
+    const int end = continuous_ ? it0 + nsteps : std::min(it0 + nsteps, pb_.nt - 1);
     int it = it0;
     // CUDA graph replay in rotation-aligned blocks of three steps when the
     // run is long enough; step kernels take their per-step arguments from the
@@ -1374,6 +1411,165 @@ void Engine::run(int it0, int nsteps)
 }
 
 void Engine::extract_last() { extract(ext_, level(1), rcv_dev_.as<float>(), pb_.nt - 1); }
+
+void Engine::set_continuous()
+{
+    if (continuous_) return;
+    CK(cudaSetDevice(device_));
+    shot_t0_.alloc(sizeof(int) * pb_.nshots);
+    shot_t0_.zero(stream_);
+    const std::vector<int> ones(pb_.nshots, 1);
+    shot_active_.alloc(sizeof(int) * pb_.nshots);
+    CK(cudaMemcpy(shot_active_.p, ones.data(), shot_active_.bytes, cudaMemcpyHostToDevice));
+    continuous_ = true;
+}
+
+void Engine::release_shot(int slot)
+{
+    if (slot < 0 || slot >= pb_.nshots) throw FwiError(FWI_ERR_ARG, "slot out of range");
+    if (!continuous_) throw FwiError(FWI_ERR_STATE, "slots are not enabled");
+    const int zero = 0;
+    CK(cudaMemcpyAsync(shot_active_.as<int>() + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, (cudaStream_t)stream_));
+    sync();
+}
+
+// Tables of every shot into the existing device buffers (a reallocation
+// when a count changed; the next run recaptures its graph then).
+void Engine::upload_tables(const InjTable &inj, const ExtTable &ext)
+{
+    cudaStream_t s = (cudaStream_t)stream_;
+    for (int c = 0; c < 3; c++) {
+        const int n = (int)inj.gidx[c].size();
+        if (n != inj_.n[c]) {
+            inj_.n[c] = n;
+            inj_.gidx[c].alloc(sizeof(int64_t) * n);
+            inj_.trace[c].alloc(sizeof(int) * n);
+            inj_.w[c].alloc(sizeof(float) * n);
+        }
+        if (n) {
+            CK(cudaMemcpyAsync(inj_.gidx[c].p, inj.gidx[c].data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(inj_.trace[c].p, inj.trace[c].data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(inj_.w[c].p, inj.w[c].data(), sizeof(float) * n, cudaMemcpyHostToDevice, s));
+        }
+    }
+    if (ext.nrec != ext_.nrec || ext.ntap != ext_.ntap)
+        throw FwiError(FWI_ERR_ARG, "a slot keeps the batch's receiver count");
+    CK(cudaMemcpyAsync(ext_.gidx.p, ext.gidx.data(), ext_.gidx.bytes, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ext_.w.p, ext.w.data(), ext_.w.bytes, cudaMemcpyHostToDevice, s));
+    // the host tables may go out of scope after return
+    sync();
+}
+
+void Engine::join_shot(int slot, const InjTable &inj, const ExtTable &ext, int t0)
+{
+    if (slot < 0 || slot >= pb_.nshots) throw FwiError(FWI_ERR_ARG, "slot out of range");
+    CK(cudaSetDevice(device_));
+    set_continuous();
+    const int64_t n = pb_.nxyz();
+    const Dims g{pb_.nx, pb_.ny, pb_.nz};
+    StepArgs a = make_step_args(pb_, model_.as<float>(), sdiv_ptr_, taper_ptr_, scale_);
+    for (int c = 0; c < 3; c++)
+        for (int64_t gi : inj.gidx[c]) {
+            if (gi / n != slot) continue;
+            const int64_t i = gi % n;
+            const int iz = (int)(i % g.nz), ix = (int)((i / g.nz) % g.nx), iy = (int)(i / ((int64_t)g.nz * g.nx));
+            if (in_taper(a, ix, iy, iz))
+                throw FwiError(FWI_ERR_UNSUPPORTED, "a source point of the joining shot lies in a taper zone");
+        }
+    upload_tables(inj, ext);
+    cudaStream_t s = (cudaStream_t)stream_;
+    const int64_t sst = (int64_t)pb_.ncomp() * n;
+    for (int l = 0; l < 3; l++) CK(cudaMemsetAsync(level(l) + slot * sst, 0, sizeof(float) * sst, s));
+    const size_t rows = (size_t)pb_.ncomp() * ext_.nr * pb_.nt;
+    CK(cudaMemsetAsync(rcv_dev_.as<float>() + slot * rows, 0, sizeof(float) * rows, s));
+    init_prev(inj_, src_dev_.as<float>(), level(0), slot);
+    CK(cudaMemcpyAsync(shot_t0_.as<int>() + slot, &t0, sizeof(int), cudaMemcpyHostToDevice, s));
+    const int one = 1;
+    CK(cudaMemcpyAsync(shot_active_.as<int>() + slot, &one, sizeof(int), cudaMemcpyHostToDevice, s));
+    sync();
+}
+
+// Strain along the fibre (dipole_to_strain forward, misc.cpp:11-42):
+// (w0 u0 + w1 u1 + w2 u2) / gl per sample, in the host formulation's order
+// and rounding.  grid: (samples of a shot / 256, shots), raw [.][3][nr][nt].
+__global__ void k_das_strain(const float *raw, float *out, const float *w, int nr, int nt, float gl, int s0)
+{
+    const int64_t cs = (int64_t)nr * nt;
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= cs) return;
+    const int sh = s0 + blockIdx.y;
+    const float *wr = w + ((int64_t)sh * nr + k / nt) * 3;
+    const float *p = raw + (int64_t)sh * 3 * cs + k;
+    const float v = __fadd_rn(__fadd_rn(__fmul_rn(wr[0], p[0]), __fmul_rn(wr[1], p[cs])), __fmul_rn(wr[2], p[2 * cs]));
+    out[(int64_t)blockIdx.y * cs + k] = __fdiv_rn(v, gl);
+}
+
+// Its adjoint: u2 = w2 s / gl, u1 = w1 s / gl, u0 = s (w0 / gl), as the host
+// formulation rounds them.  src [nsh][nr][nt] -> out [nsh][3][nr][nt].
+__global__ void k_das_spread(const float *src, float *out, const float *w, int nr, int nt, float gl)
+{
+    const int64_t cs = (int64_t)nr * nt;
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= cs) return;
+    const int sh = blockIdx.y;
+    const float *wr = w + ((int64_t)sh * nr + k / nt) * 3;
+    const float s = src[(int64_t)sh * cs + k];
+    float *o = out + (int64_t)sh * 3 * cs + k;
+    o[2 * cs] = __fdiv_rn(__fmul_rn(wr[2], s), gl);
+    o[cs] = __fdiv_rn(__fmul_rn(wr[1], s), gl);
+    o[0] = __fmul_rn(s, __fdiv_rn(wr[0], gl));
+}
+
+void Engine::set_das(const std::vector<float> &w, int nr, float gl)
+{
+    CK(cudaSetDevice(device_));
+    if ((int64_t)w.size() != (int64_t)pb_.nshots * nr * 3) throw FwiError(FWI_ERR_ARG, "DAS weights of every shot's channels");
+    das_nr_ = nr;
+    das_gl_ = gl;
+    das_w_.alloc(sizeof(float) * w.size());
+    CK(cudaMemcpyAsync(das_w_.p, w.data(), das_w_.bytes, cudaMemcpyHostToDevice, (cudaStream_t)stream_));
+    sync();  // w may go out of scope
+}
+
+const float *Engine::strain_traces(int s0, int nsh)
+{
+    if (das_gl_ <= 0.f) throw FwiError(FWI_ERR_STATE, "no DAS channels set");
+    const int64_t cs = (int64_t)das_nr_ * pb_.nt;
+    das_rcv_.alloc(sizeof(float) * nsh * cs);
+    const dim3 grd((unsigned)((cs + 255) / 256), nsh);
+    k_das_strain<<<grd, 256, 0, (cudaStream_t)stream_>>>(rcv_dev_.as<float>(), das_rcv_.as<float>(), das_w_.as<float>(),
+                                                         das_nr_, pb_.nt, das_gl_, s0);
+    CK(cudaGetLastError());
+    return das_rcv_.as<float>();
+}
+
+const float *Engine::strain_adjoint(const float *src_dev)
+{
+    if (das_gl_ <= 0.f) throw FwiError(FWI_ERR_STATE, "no DAS channels set");
+    const int64_t cs = (int64_t)das_nr_ * pb_.nt;
+    das_src_.alloc(sizeof(float) * pb_.nshots * 3 * cs);
+    const dim3 grd((unsigned)((cs + 255) / 256), pb_.nshots);
+    k_das_spread<<<grd, 256, 0, (cudaStream_t)stream_>>>(src_dev, das_src_.as<float>(), das_w_.as<float>(), das_nr_,
+                                                         pb_.nt, das_gl_);
+    CK(cudaGetLastError());
+    return das_src_.as<float>();
+}
+
+void Engine::copy_strain(int s0, int nsh, float *rcv)
+{
+    const float *d = strain_traces(s0, nsh);
+    CK(cudaMemcpyAsync(rcv, d, sizeof(float) * nsh * das_nr_ * pb_.nt, cudaMemcpyDeviceToHost, (cudaStream_t)stream_));
+    sync();
+}
+
+void Engine::copy_shot_traces(int slot, float *rcv)
+{
+    if (slot < 0 || slot >= pb_.nshots) throw FwiError(FWI_ERR_ARG, "slot out of range");
+    const size_t rows = (size_t)pb_.ncomp() * ext_.nr * pb_.nt;
+    CK(cudaMemcpyAsync(rcv, rcv_dev_.as<float>() + slot * rows, sizeof(float) * rows, cudaMemcpyDeviceToHost,
+                       (cudaStream_t)stream_));
+    sync();
+}
 
 void Engine::copy_traces(float *rcv)
 {
@@ -2037,7 +2233,8 @@ void DeviceResidual::set_axes(int hl, int ntd, float dtd, int nt, float dt)
     dt_ = dt;
 }
 
-double DeviceResidual::run(Engine &eng, size_t obs_offset, int ntraces, int seismotype, float alpha, float *residual)
+double DeviceResidual::run(Engine &eng, size_t obs_offset, int ntraces, int seismotype, float alpha, float *residual,
+                           double *per_trace, const float *traces)
 {
     if (ntraces <= 0) return 0.0;
     cudaStream_t st = (cudaStream_t)eng.stream();
@@ -2048,7 +2245,7 @@ double DeviceResidual::run(Engine &eng, size_t obs_offset, int ntraces, int seis
     if (!bad_.p) bad_.alloc(sizeof(int));
     CK(cudaMemsetAsync(bad_.p, 0, sizeof(int), st));
     ResidualArgs a{};
-    a.rcv = eng.traces_dev();
+    a.rcv = traces ? traces : eng.traces_dev();  // DAS: the strain traces
     a.obs = obs_.as<float>() + obs_offset;
     a.asrc = asrc_.as<float>();
     a.resid = residual ? resid_.as<float>() : nullptr;
@@ -2084,6 +2281,7 @@ double DeviceResidual::run(Engine &eng, size_t obs_offset, int ntraces, int seis
     if (bad) throw FwiError(FWI_ERR_NAN, "non-finite values in the traces");
     double sum = 0.0;
     for (int k = 0; k < ntraces; k++) sum += part[k];
+    if (per_trace) std::copy(part.begin(), part.end(), per_trace);
     return sum;
 }
 
@@ -2121,9 +2319,10 @@ void Engine::image(int itl, const float *curr, const float *prevl)
         a.grad[c] = grad_.as<double>() + (int64_t)(c < (pb_.nmodels == 2 ? 2 : 3) ? c : 0) * n;
     }
     const int64_t sst = (int64_t)nc * n;
-    if (pb_.nmodels == 2) k_image_batch<ACOUSTIC><<<grd, blk, 0, s>>>(a, pb_.nshots, sst);
-    else if (pb_.nmodels == 3) k_image_batch<ELASTIC><<<grd, blk, 0, s>>>(a, pb_.nshots, sst);
-    else k_image_batch<VTI><<<grd, blk, 0, s>>>(a, pb_.nshots, sst);
+    const int64_t gst = per_shot_grad_ ? (int64_t)std::min(3, pb_.nmodels) * n : 0;
+    if (pb_.nmodels == 2) k_image_batch<ACOUSTIC><<<grd, blk, 0, s>>>(a, pb_.nshots, sst, gst);
+    else if (pb_.nmodels == 3) k_image_batch<ELASTIC><<<grd, blk, 0, s>>>(a, pb_.nshots, sst, gst);
+    else k_image_batch<VTI><<<grd, blk, 0, s>>>(a, pb_.nshots, sst, gst);
     CK(cudaGetLastError());
 }
 
@@ -2145,16 +2344,20 @@ void Engine::adjoint_impl(const InjTable &inj, int ntrace, const float *adj_src,
     cudaStream_t s = (cudaStream_t)stream_;
     const int64_t n = pb_.nxyz();
     const int nm = std::min(3, pb_.nmodels);
-    DevInj dinj;
+    // adjoint source tables, host adjoint sources and the FP32 gradient live
+    // in members of the engine: a repeated evaluation (same counts) reuses
+    // them instead of a cudaMalloc / cudaFree pair, which would synchronise
+    // the device under other sessions' work
+    DevInj &dinj = adj_inj_;
     upload_inj(inj, ntrace, dinj);
-    DevBuf asrc_own;
     const float *asrc_p = adj_src_dev;
     if (!asrc_p) {
-        asrc_own.alloc(sizeof(float) * (size_t)ntrace * pb_.nt);
-        CK(cudaMemcpyAsync(asrc_own.p, adj_src, asrc_own.bytes, cudaMemcpyHostToDevice, s));
-        asrc_p = asrc_own.as<float>();
+        adj_src_buf_.alloc(sizeof(float) * (size_t)ntrace * pb_.nt);
+        CK(cudaMemcpyAsync(adj_src_buf_.p, adj_src, adj_src_buf_.bytes, cudaMemcpyHostToDevice, s));
+        asrc_p = adj_src_buf_.as<float>();
     }
-    grad_.alloc(sizeof(double) * nm * n);
+    const int64_t ng = (per_shot_grad_ ? pb_.nshots : 1) * nm * n;  // one gradient, or one per shot
+    grad_.alloc(sizeof(double) * ng);
     grad_.zero(s);
     rot_ = 0;
     fields_.zero(s);
@@ -2167,8 +2370,9 @@ void Engine::adjoint_impl(const InjTable &inj, int ntrace, const float *adj_src,
         rot_ = (rot_ + 1) % 3;
     }
     image(0, level(1), level(0));
-    DevBuf gf(sizeof(float) * nm * n);
-    k_d2f<<<(unsigned)((nm * n + 255) / 256), 256, 0, s>>>(grad_.as<double>(), gf.as<float>(), nm * n);
+    DevBuf &gf = grad_f32_;
+    gf.alloc(sizeof(float) * ng);
+    k_d2f<<<(unsigned)((ng + 255) / 256), 256, 0, s>>>(grad_.as<double>(), gf.as<float>(), ng);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(grad, gf.p, gf.bytes, cudaMemcpyDeviceToHost, s));
     sync();

@@ -113,6 +113,36 @@ public:
     void copy_traces(float *rcv);         // [nshots][nrcomp][nr][nt] raw traces (host)
     int launches_per_step() const;
 
+    // Shot slots: in continuous mode every shot of the batch carries its own
+    // start step t0 (all 0 when the mode begins); its sources and receivers
+    // run on its local time it - t0, and a run is no longer bounded by nt.
+    // join_shot replaces the geometry of one slot (tables of all shots,
+    // gidx offset by shot as in set_sources/set_receivers, the same source
+    // traces) and restarts it at step t0: its three wavefield levels and its
+    // traces are zeroed and its initial condition applied.  Throws when one
+    // of its source points lies in a taper zone, where the first step of a
+    // restarted shot would taper its initial state (the reference tapers
+    // prev only after the first step).  An idle slot (release_shot) is
+    // advanced by no kernel until a shot joins it.
+    void set_continuous();
+    bool continuous() const { return continuous_; }
+    void join_shot(int slot, const InjTable &inj, const ExtTable &ext, int t0);
+    void release_shot(int slot);
+    void copy_shot_traces(int slot, float *rcv);  // [nrcomp][nr][nt] raw traces of one slot (host)
+
+    // DAS (fibre) receivers: the strain along each fibre from the three
+    // components of its dipole rows (dipole_to_strain, misc.cpp:11-42), on
+    // the device.  w: [nshots][nr][3] projection weights (cos dip cos az,
+    // cos dip sin az, sin dip, as floats), gl the gauge length.
+    void set_das(const std::vector<float> &w, int nr, float gl);
+    // strain [nsh][nr][nt] of shots [s0, s0+nsh) of the raw traces
+    // [nshots][3][nr][nt] (device; kept until the next call)
+    const float *strain_traces(int s0, int nsh);
+    // its adjoint: strain sources [nshots][nr][nt] to dipole sources
+    // [nshots][3][nr][nt] (device; kept until the next call)
+    const float *strain_adjoint(const float *src_dev);
+    void copy_strain(int s0, int nsh, float *rcv);  // strain_traces to the host
+
     // --- operator / gradient path (one shot or a batch of shots) -------------
     // Snapshot storage of the forward wavefield for the imaging condition.
     enum Storage { STORE_FP32 = 0, STORE_FP16P = 1 };
@@ -135,7 +165,9 @@ public:
     // all shots (as set_sources/set_receivers); rcv [nshots][ncomp][nr][nt].
     void forward(const InjTable &inj, int ntrace, const float *src, const ExtTable &ext, float *rcv, bool store);
     // adjoint + imaging of every shot of the batch; grad out: [min(3,nm)][nxyz]
-    // float, summed over the shots in FP64 (before H quadrature and chain rule)
+    // float, summed over the shots in FP64 (before H quadrature and chain
+    // rule), or with per-shot gradients [nshots][min(3,nm)][nxyz]
+    void set_per_shot_gradient(bool on) { per_shot_grad_ = on; }
     void adjoint(const InjTable &inj, int ntrace, const float *adj_src, float *grad);
     // the same with the adjoint sources [ntrace][nt] already on the device
     // (stream-ordered after the engine's earlier work)
@@ -168,7 +200,8 @@ public:
 
 private:
     void upload_inj(const InjTable &t, int ntrace, DevInj &d);
-    void init_prev(const DevInj &inj, const float *src_dev, float *prev);
+    void init_prev(const DevInj &inj, const float *src_dev, float *prev, int only_shot = -1);
+    void upload_tables(const InjTable &inj, const ExtTable &ext);
     void step(float *prev, float *curr, float *next, bool taper_prev);
     void inject(const DevInj &inj, const float *src_dev, int it, float *next);
     void extract(const DevExt &ext, const float *curr, float *rcv_dev, int it);
@@ -184,6 +217,12 @@ private:
     // one stream
     void *side_ = nullptr, *ev_fork_ = nullptr, *ev_join_ = nullptr;
     bool conc_ = true;
+    bool continuous_ = false;     // shot slots with their own start steps (shot_t0_)
+    bool per_shot_grad_ = false;  // the adjoint keeps one gradient per shot
+    DevBuf shot_t0_, shot_active_;
+    DevBuf das_w_, das_rcv_, das_src_;  // DAS projection weights, strain traces, dipole sources
+    int das_nr_ = 0;
+    float das_gl_ = 0.f;
     DevBuf model_;                 // [nm][nxyz]
     DevBuf w2c_;                   // closure weights of the D2var coefficients per axis (StepArgs::w2c)
     const float *w2c_ptr_[3][3] = {};
@@ -259,6 +298,8 @@ private:
     int64_t kpts_ = 0;
     void kmark(bool begin, const char *name, int64_t pts);
     DevInj inj_;
+    DevInj adj_inj_;                  // adjoint source tables (reused between adjoints)
+    DevBuf adj_src_buf_, grad_f32_;   // host adjoint sources on the device, FP32 gradient
     DevExt ext_;
 };
 
@@ -282,7 +323,8 @@ public:
     // traces from obs_offset on; returns the FP64 misfit sum (before 0.5 dt /
     // dnorm), leaves the adjoint sources on the device and, when residual is
     // not null, copies the residual [ntraces][ntd] there.  Synchronises eng's stream.
-    double run(Engine &eng, size_t obs_offset, int ntraces, int seismotype, float alpha, float *residual);
+    double run(Engine &eng, size_t obs_offset, int ntraces, int seismotype, float alpha, float *residual,
+               double *per_trace = nullptr, const float *traces = nullptr);
     const float *adjoint_sources() const { return asrc_.as<float>(); }
 
 private:

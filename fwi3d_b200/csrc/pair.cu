@@ -92,6 +92,7 @@ __global__ void __launch_bounds__(pz::NT, 2)
     c.rows.p = c.sm->rows;
     const int tid = threadIdx.x;
     c.shot = blockIdx.z / nchunks;
+    if (shot_idle(a, c.shot)) return;
     const int ch = blockIdx.z - c.shot * nchunks;
     c.so = c.shot * a.sst;
     tile_range(blockIdx.x + (MODE == 1 ? bz0 : 0), a.g.nz, fz::TZ, c.z0, c.zend);

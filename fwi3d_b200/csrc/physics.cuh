@@ -60,7 +60,13 @@ struct StepArgs {
     // coefficient f = 0 mu, 1 c66, 2 c11b = 2 (1 + 2 eps) mu (VTI); line index
     // y*nz + z (x lines), x*nz + z (y lines), y*nx + x (z lines)
     const float *w2c[3][3];
+    // shot slots: active[s] == 0 marks an idle slot, whose fields no kernel
+    // advances (null: every shot active)
+    const int *active;
 };
+
+// An idle shot slot: its CTAs or threads return at once.
+FWI_HD bool shot_idle(const StepArgs &a, int s) { return a.active && !a.active[s]; }
 
 // Pointers of shot s.
 FWI_HD StepArgs shot_args(const StepArgs &a, int s)

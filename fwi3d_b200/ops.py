@@ -224,7 +224,7 @@ def forward_batch(sv, device: int = 0) -> np.ndarray:
     ncomp = 1 if w.ndim == 1 else w.shape[0]
     sx = np.ascontiguousarray(np.asarray(sv.par.sxyz, dtype=np.float32)[:, :3])
     rx = np.ascontiguousarray(np.asarray(sv.par.rxyz, dtype=np.float32).reshape(ns, nr, 5))
-    nrcomp = 1 if sv.nmodels == 2 else 3
+    nrcomp = 1 if sv.nmodels == 2 or sv.par.gl > 0 else 3  # DAS: strain along each fibre
     out = np.zeros((ns, nrcomp, nr, w.shape[-1]), dtype=np.float32)
     model = np.ascontiguousarray(sv.model, dtype=np.float32)
     cp = to_cparam(sv.par)
@@ -254,7 +254,7 @@ class FwiObjective:
         w = np.ascontiguousarray(sv.wavelet, dtype=np.float32)
         ncomp = 1 if w.ndim == 1 else w.shape[0]
         self.nt_data = w.shape[-1]
-        self.nrcomp = 1 if sv.nmodels == 2 else 3
+        self.nrcomp = 1 if sv.nmodels == 2 or sv.par.gl > 0 else 3  # DAS: strain along each fibre
         obs = np.ascontiguousarray(observed, dtype=np.float32)
         if obs.size != self.ns * self.nrcomp * self.nr * self.nt_data:
             raise _lib.FwiError(_lib.FWI_ERR_ARG, f"observed data of shape {obs.shape} do not match the survey")
@@ -280,6 +280,32 @@ class FwiObjective:
         _lib.check(_lib.load().fwi_objective_evaluate(self._h, _lib.fptr(m), C.byref(f), _lib.fptr(g),
                                                       _lib.fptr(r) if r is not None else None))
         return (f.value, g, r) if want_residual else (f.value, g)
+
+    def evaluate_shots(self, model: np.ndarray):
+        """One objective per shot from the same batched launches: misfits
+        [ns] (FP64) and gradients [ns][nm][...], each shot normalised by its
+        own data (independent gradient requests on one model)."""
+        m = np.ascontiguousarray(model, dtype=np.float32)
+        if m.size != int(np.prod(self.shape)):
+            raise _lib.FwiError(_lib.FWI_ERR_ARG, f"model of shape {m.shape}, expected {self.shape}")
+        g = np.zeros((self.ns, self.nm) + tuple(self.shape[1:]), dtype=np.float32)
+        f = np.zeros(self.ns, dtype=np.float64)
+        _lib.check(_lib.load().fwi_objective_evaluate_shots(self._h, _lib.fptr(m),
+                                                            f.ctypes.data_as(C.POINTER(C.c_double)), _lib.fptr(g)))
+        return f, g
+
+    def set_shots(self, sv, observed: np.ndarray) -> None:
+        """New shots (same counts) for the next evaluations, which reuse the
+        objective's device buffers."""
+        if len(sv.par.sxyz) != self.ns or any(len(r) != self.nr for r in sv.par.rxyz):
+            raise _lib.FwiError(_lib.FWI_ERR_ARG, "set_shots keeps the shot and receiver counts")
+        obs = np.ascontiguousarray(observed, dtype=np.float32)
+        if obs.size != self.ns * self.nrcomp * self.nr * self.nt_data:
+            raise _lib.FwiError(_lib.FWI_ERR_ARG, f"observed data of shape {obs.shape} do not match the survey")
+        sx = np.ascontiguousarray(np.asarray(sv.par.sxyz, dtype=np.float32)[:, :3])
+        rx = np.ascontiguousarray(np.asarray(sv.par.rxyz, dtype=np.float32).reshape(self.ns, self.nr, 5))
+        _lib.check(_lib.load().fwi_objective_set_shots(self._h, _lib.fptr(sx), _lib.fptr(rx), _lib.fptr(obs)))
+        self.sv = sv
 
     def device_bytes(self) -> int:
         return int(_lib.load().fwi_objective_device_bytes(self._h))

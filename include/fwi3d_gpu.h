@@ -136,6 +136,24 @@ int fwi_batch_sync(fwi_batch *b);
 int fwi_batch_stream(fwi_batch *b, void **stream);
 /* Data [nshots][nrcomp][nr][nt_data] after the full time axis was run. */
 int fwi_batch_traces(fwi_batch *b, float *data);
+/* Shot slots (serving; no counterpart in the reference, whose modeling runs
+ * one survey at a time).  fwi_batch_enable_slots, right after a reset, turns
+ * the session's shots into slots with their own start steps (all 0 then).
+ * fwi_batch_join restarts `slot` with a new shot (sxyz [3], rxyz [nr][5]) at
+ * the session's current step while the other slots run on; a run is then no
+ * longer bounded by nt, every slot's sources and receivers follow its own
+ * time axis, and its data come from fwi_batch_slot_traces once
+ * fwi_batch_slot_time reports 0 steps remaining (fwi_batch_traces refuses).
+ * fwi_batch_release makes a slot idle: no kernel advances it until the next
+ * join (a session opened with spare slots releases them; a slot whose data
+ * were read is released).  A shot whose source lies in a taper zone cannot
+ * join (FWI_ERR_UNSUPPORTED): its first step would taper its initial state,
+ * which a shot started at time 0 does not see; it needs a session of its own. */
+int fwi_batch_enable_slots(fwi_batch *b);
+int fwi_batch_join(fwi_batch *b, int slot, const float *sxyz, const float *rxyz);
+int fwi_batch_release(fwi_batch *b, int slot);
+int fwi_batch_slot_time(const fwi_batch *b, int slot, int *t0, int *remaining);
+int fwi_batch_slot_traces(fwi_batch *b, int slot, float *data);
 int fwi_batch_get_info(const fwi_batch *b, fwi_op_info *info, int *launches_per_step);
 /* Diagnostics (no counterpart in the reference): time each launch of the
  * step's main kernel with a pair of CUDA events on the session stream, for up
@@ -191,6 +209,16 @@ int fwi_objective_create(fwi_objective **o, int device, const fwi_grid *grid, in
                          const float *sxyz, int nr, const float *rxyz, const float *observed, int normalize,
                          int batch);
 int fwi_objective_evaluate(fwi_objective *o, const float *model, double *f, float *grad, float *residual);
+/* Serving (no counterpart in the reference).  fwi_objective_evaluate_shots:
+ * one objective per shot -- f [nshots], grad [nshots][min(3,nmodels)][nxyz],
+ * each normalised by its own shot's data -- from the same batched launches
+ * (independent gradient requests on one model in one evaluation).
+ * fwi_objective_set_shots: new shots for the same counts (sxyz [nshots][3],
+ * rxyz [nshots][nr][5], observed data); the evaluations after it reuse the
+ * objective's device buffers (wavefields, snapshot or checkpoint stores,
+ * residual state), so a server allocates no device memory per request. */
+int fwi_objective_evaluate_shots(fwi_objective *o, const float *model, double *f, float *grad);
+int fwi_objective_set_shots(fwi_objective *o, const float *sxyz, const float *rxyz, const float *observed);
 /* Device bytes of the last evaluation (wavefields, snapshots, model, tables). */
 int64_t fwi_objective_device_bytes(const fwi_objective *o);
 void fwi_objective_destroy(fwi_objective *o);

@@ -299,3 +299,44 @@ def test_graph_replay_matches_plain_launches(monkeypatch):
         out["b" + g] = tr
     assert np.array_equal(out["op1"], out["op0"])
     assert np.array_equal(out["b1"], out["b0"])
+
+
+def test_das_batch_equals_operator():
+    """DAS channels on the batch path (two shots in one launch, strain formed
+    on the device) against the operator path shot by shot."""
+    sv = _das(n=28, steps=120)
+    n = 28
+    sv.par.sxyz = [[0.5 * n * sv.dx, 0.4 * n * sv.dx, 0.3 * n * sv.dx], [0.4 * n * sv.dx, 0.55 * n * sv.dx, 0.25 * n * sv.dx]]
+    sv.par.rxyz = [sv.par.rxyz[0], sv.par.rxyz[0]]
+    sv.par.ns = 2
+    d = ops.forward_batch(sv)
+    assert d.shape[1] == 1
+    for s in range(2):
+        ref = ops.from_survey(sv, s).forward(False, sv.model)
+        assert rel(d[s], ref) < 1e-6, s
+
+
+def test_das_objective_matches_reference(oracle_fp32):
+    """The device FWI objective with DAS channels (strain on the device, its
+    adjoint spread back to the dipoles) against nlls_fwi of the reference's
+    FP32 build; the host residual path (FWI_HOST_RESIDUAL=1) gives the same."""
+    import os
+
+    sv = _das(n=26, steps=120)
+    sv.par.sub = 1
+    tol, _, _ = _das_tol(oracle_fp32, sv)
+    true = synth.Survey(sv.name, sv.nmodels, sv.nx, sv.ny, sv.nz, sv.dx, sv.dy, sv.dz, sv.model * np.float32(1.02),
+                        sv.wavelet, sv.dt_data, sv.par.copy())
+    obs = oracle_fp32.modeling(true, precision="fp32")[0][None].astype(np.float32)
+    ref = oracle_fp32.fwi(sv, obs, solver="none")
+    f, g = ops.FwiObjective(sv, obs, normalize=True, batch=1).evaluate(sv.model)
+    assert abs(f - ref["f"][0]) / ref["f"][0] < 10 * tol
+    for k in range(3):
+        assert rel(g[k], ref["grad"][k]) < 1e-4 + 10 * tol, k
+    os.environ["FWI_HOST_RESIDUAL"] = "1"
+    try:
+        fh, gh = ops.FwiObjective(sv, obs, normalize=True, batch=1).evaluate(sv.model)
+    finally:
+        del os.environ["FWI_HOST_RESIDUAL"]
+    assert fh == pytest.approx(f, rel=1e-6)
+    assert rel(gh, g) < 1e-6
