@@ -94,3 +94,51 @@ def test_scaled_16bit_checkpoints_vs_fp64_oracle(oracle_fp32, precision):
         print(f"precision {precision} grad[{k}]: vs fp64 {e:.3e} (FP32 full storage {e32:.3e})")
         errs.append(e)
     assert max(errs) < BOUND[precision]
+
+
+def _vti_case(n=26, steps=160):
+    sv = synth.vti_layered(nx=n, ny=n + 2, nz=n - 2, nsteps=steps, taper=5, rec_stride=3, nshots=1, dt=0.0005)
+    sv.par.sxyz = [[0.5 * n * sv.dx, 0.45 * n * sv.dx, 0.3 * n * sv.dx]]
+    sv.par.sub = 1
+    return sv
+
+
+def test_vti_fp32_checkpoints_equal_full_storage():
+    sv = _vti_case()
+    rng = np.random.default_rng(1)
+    op = ops.from_survey(sv)
+    d = op.forward(False, sv.model)
+    adj = (rng.standard_normal(d.shape) * np.abs(d).max()).astype(np.float32)
+    g_full = op.jacobianT(False, None, sv.model, adj)
+    sv.par.checkpoint_slots = 7
+    opc = ops.from_survey(sv)
+    opc.forward(False, sv.model)
+    g_ck = opc.jacobianT(False, None, sv.model, adj)
+    for k in range(3):
+        assert rel(g_ck[k], g_full[k]) < 1e-6, k
+
+
+@pytest.mark.parametrize("precision", [1, 2])
+def test_vti_scaled_16bit_checkpoints_vs_fp64_oracle(oracle_fp32, precision):
+    """The VTI gradient with 16-bit restart states (the configuration's FP16
+    per-snapshot-scaled checkpoints) against the reference's FP64 build; the
+    distance is printed and bounded as for the isotropic case."""
+    sv = _vti_case()
+    rng = np.random.default_rng(0)
+    ref, _ = oracle_fp32.modeling(sv, precision="fp32")
+    adj = (rng.standard_normal(ref.shape) * np.abs(ref).max()).astype(np.float32)
+    _, g64, _ = oracle_fp32.forward_jacobianT(sv, adj, precision="fp64")
+    op = ops.from_survey(sv)
+    op.forward(False, sv.model)
+    g32 = op.jacobianT(False, None, sv.model, adj)
+    sv.par.checkpoint_slots = 6
+    sv.par.checkpoint_precision = precision
+    op16 = ops.from_survey(sv)
+    op16.forward(False, sv.model)
+    g16 = op16.jacobianT(False, None, sv.model, adj)
+    errs = []
+    for k in range(3):
+        e, e32 = rel(g16[k], g64[k]), rel(g32[k], g64[k])
+        print(f"VTI precision {precision} grad[{k}]: vs fp64 {e:.3e} (FP32 full storage {e32:.3e})")
+        errs.append(e)
+    assert max(errs) < BOUND[precision]
