@@ -53,9 +53,10 @@ int guarded(F &&f)
 
 bool finite_all(const float *p, int64_t n)
 {
-    for (int64_t i = 0; i < n; i++)
-        if (!std::isfinite(p[i])) return false;
-    return true;
+    int bad = 0;
+#pragma omp parallel for reduction(| : bad) schedule(static)
+    for (int64_t i = 0; i < n; i++) bad |= !std::isfinite(p[i]);
+    return !bad;
 }
 }  // namespace
 
@@ -150,9 +151,30 @@ struct fwi_batch {
     std::unique_ptr<Engine> eng;
     std::vector<float> sxyz, rxyz;  // geometry of every slot: [nshots][3], [nshots][nr][5]
     std::vector<int> t0;            // start step of every slot (shot slots)
+    DeviceResidual out;             // modeling output on the device (sinc resampling)
 };
 
 namespace {
+// FWI_BATCH_TIMING=1: host-clock times of the phases of a batch call on
+// stderr (the device work of a phase is synchronised only where the phase
+// ends in a synchronisation anyway).
+struct PhaseClock {
+    bool on = false;
+    std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+    PhaseClock()
+    {
+        const char *e = std::getenv("FWI_BATCH_TIMING");
+        on = e && e[0] == '1';
+    }
+    void mark(const char *what)
+    {
+        if (!on) return;
+        const auto n = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "fwi batch: %-28s %8.3f s\n", what, std::chrono::duration<double>(n - t).count());
+        t = n;
+    }
+};
+
 // DAS channel s*nr + r of a [nshots][nr][5] receiver array: its fibre, and
 // the projection weights of dipole_to_strain (misc.cpp:11-42) as that
 // routine forms them in float.
@@ -234,6 +256,23 @@ void batch_shot_output(const fwi_batch &b, float *r, float *d)
     std::fill(d, d + (size_t)ntr * b.nt_data, 0.f);
     resample_adjoint(b.par.resampling_linear == 0, b.par.sinc_half_length, d, b.nt_data, b.dt_data, r, nt, b.pb.dt,
                      ntr);
+}
+
+// Data of shots [s0, s0+nsh) to data [nsh][nrcomp][nr][nt_data] on the device
+// (sinc resampling and traces that fit the kernel's shared memory), false
+// where the host path must take them.
+bool batch_device_output(fwi_batch &b, int s0, int nsh, float *data)
+{
+    const int nt = b.pb.nt;
+    const char *he = std::getenv("FWI_HOST_OUTPUT");  // =1: the host path (the same values bit for bit)
+    if ((he && he[0] == '1') || b.par.resampling_linear != 0 || std::max(nt, b.nt_data) > kResidualMaxSamples)
+        return false;
+    const int ntr = b.nrcomp * b.nr;
+    const float *src = b.par.gl > 0 ? b.eng->strain_traces(s0, nsh)
+                                    : b.eng->traces_dev() + (size_t)s0 * b.pb.ncomp() * b.nr * nt;
+    b.out.set_axes(b.par.sinc_half_length, b.nt_data, b.dt_data, nt, b.pb.dt);
+    b.out.data(*b.eng, src, nsh * ntr, b.par.seismotype, b.pb.dt / b.dt_data, data);
+    return true;
 }
 }  // namespace
 
@@ -537,6 +576,7 @@ int fwi_batch_create(fwi_batch **out, int device, const fwi_grid *grid, int nmod
         const int64_t n = (int64_t)grid->nx * grid->ny * grid->nz;
         if (!finite_all(model, nmodels * n)) throw FwiError(FWI_ERR_NAN, "model contains non-finite values");
         std::vector<float> m(model, model + nmodels * n);
+        PhaseClock clk;
         TimeAxis ta = analyze_model(m, nmodels, grid->nx, grid->ny, grid->nz, grid->dx, grid->dy, grid->dz, nt_data,
                                     dt_data, b->par);
         convert_model(m, nmodels, n);
@@ -557,8 +597,11 @@ int fwi_batch_create(fwi_batch **out, int device, const fwi_grid *grid, int nmod
         p.free_surface_stiffness =
             nmodels == 2 ? std::max(b->par.free_surface_stiffness, 1.0f) : b->par.free_surface_stiffness;
         p.nshots = nshots;
+        clk.mark("model analysis + convert");
         b->eng.reset(new Engine(device, p));
+        clk.mark("engine (device buffers)");
         b->eng->set_model(m.data());
+        clk.mark("set_model (tables)");
         // sources: the same wavelet for every shot, resampled once
         std::vector<float> w = expand_wavelet(wavelet, wavelet_ncomp, nt_data, nmodels, b->par);
         std::vector<float> w1((size_t)b->nscomp * p.nt);
@@ -571,11 +614,14 @@ int fwi_batch_create(fwi_batch **out, int device, const fwi_grid *grid, int nmod
         b->t0.assign(nshots, 0);
         InjTable all;
         ExtTable ext;
+        clk.mark("wavelet");
         batch_tables(*b, all, ext);
+        clk.mark("geometry tables (host)");
         b->eng->set_sources(all, nshots * b->nscomp, src.data());
         b->eng->set_receivers(ext, nr);
         if (b->par.gl > 0) b->eng->set_das(das_weights(rxyz, 0, nshots, nr), nr, b->par.gl);
         b->eng->sync();
+        clk.mark("tables upload");
         *out = b.release();
     });
 }
@@ -664,6 +710,7 @@ int fwi_batch_slot_traces(fwi_batch *b, int slot, float *data)
     return guarded([&] {
         if (!b->eng->continuous()) throw FwiError(FWI_ERR_STATE, "slot traces need a batch with shot slots");
         if (b->it < b->t0[slot] + b->pb.nt) throw FwiError(FWI_ERR_STATE, "the slot's time axis has not been run to the end");
+        if (batch_device_output(*b, slot, 1, data)) return;
         std::vector<float> rcv((size_t)b->nrcomp * b->nr * b->pb.nt);
         if (b->par.gl > 0) b->eng->copy_strain(slot, 1, rcv.data());  // strain along the fibres, on the device
         else b->eng->copy_shot_traces(slot, rcv.data());
@@ -691,6 +738,7 @@ int fwi_batch_traces(fwi_batch *b, float *data)
         if (b->eng->continuous()) throw FwiError(FWI_ERR_STATE, "a batch with shot slots returns traces per slot");
         if (b->it != b->pb.nt - 1) throw FwiError(FWI_ERR_STATE, "the time axis has not been run to the end");
         b->eng->extract_last();
+        if (batch_device_output(*b, 0, b->nshots, data)) return;
         const int nt = b->pb.nt;
         const int ntr = b->nrcomp * b->nr;
         std::vector<float> rcv((size_t)b->nshots * ntr * nt);
@@ -725,10 +773,16 @@ int fwi_forward_batch(int device, const fwi_grid *grid, int nmodels, const fwi_p
     int rc = fwi_batch_create(&b, device, grid, nmodels, par, model, wavelet, wavelet_ncomp, nt_data, dt_data, nshots,
                               sxyz, nr, rxyz);
     if (rc != FWI_OK) return rc;
+    PhaseClock clk;
     rc = fwi_batch_reset(b);
+    clk.mark("reset (+ graph capture)");
     if (rc == FWI_OK) rc = fwi_batch_run(b, b->pb.nt - 1);
+    if (rc == FWI_OK) rc = fwi_batch_sync(b);
+    clk.mark("time steps");
     if (rc == FWI_OK) rc = fwi_batch_traces(b, data);
+    clk.mark("traces (copy + host)");
     fwi_batch_destroy(b);
+    clk.mark("destroy");
     return rc;
 }
 

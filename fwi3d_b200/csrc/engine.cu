@@ -2106,6 +2106,38 @@ __device__ void rs_dt(bool adj, const float *in, float *out, int nt, float dt)
     }
 }
 
+// Modeling output of one trace (blockIdx.x): Dt for velocity data, times
+// alpha, adjoint resampling to the data axis (the first half of k_residual,
+// without the observed data).
+__global__ void k_trace_data(ResidualArgs a)
+{
+    extern __shared__ float rs_sm[];
+    const int nt = a.nt, ntd = a.ntd;
+    float *r = rs_sm, *tmp = rs_sm + nt;
+    const int64_t tr = blockIdx.x;
+    const float *src = a.rcv + tr * nt;
+    for (int it = threadIdx.x; it < nt; it += blockDim.x) r[it] = src[it];
+    __syncthreads();
+    if (a.seismotype == 1) {
+        rs_dt(false, r, tmp, nt, a.dt);
+        __syncthreads();
+        for (int it = threadIdx.x; it < nt; it += blockDim.x) r[it] = tmp[it];
+        __syncthreads();
+    }
+    for (int it = threadIdx.x; it < nt; it += blockDim.x) r[it] = __fmul_rn(r[it], a.alpha);
+    __syncthreads();
+    for (int j = threadIdx.x; j < ntd; j += blockDim.x) {
+        float d = 0.f;
+        for (int itd = a.jlo[j]; itd < a.jhi[j]; itd++) {
+            const int k = j - a.first[itd];
+            if (k < 0 || k >= a.count[itd]) continue;
+            const int q = a.off[itd] + k;
+            d = rs_tap(d, r[itd], a.s[q], a.win[q]);
+        }
+        a.resid[tr * ntd + j] = d;
+    }
+}
+
 __global__ void k_residual(ResidualArgs a)
 {
     extern __shared__ float rs_sm[];
@@ -2231,6 +2263,39 @@ void DeviceResidual::set_axes(int hl, int ntd, float dtd, int nt, float dt)
     dtd_ = dtd;
     nt_ = nt;
     dt_ = dt;
+}
+
+void DeviceResidual::data(Engine &eng, const float *traces, int ntraces, int seismotype, float alpha, float *out)
+{
+    if (ntraces <= 0) return;
+    cudaStream_t st = (cudaStream_t)eng.stream();
+    const size_t nt = (size_t)nt_, ntd = (size_t)ntd_;
+    if (resid_.bytes < sizeof(float) * ntraces * ntd) resid_.alloc(sizeof(float) * ntraces * ntd);
+    ResidualArgs a{};
+    a.rcv = traces;
+    a.resid = resid_.as<float>();
+    a.first = first_.as<int>();
+    a.count = count_.as<int>();
+    a.off = off_.as<int>();
+    a.s = s_.as<float>();
+    a.win = win_.as<double>();
+    a.jlo = jlo_.as<int>();
+    a.jhi = jhi_.as<int>();
+    a.nt = nt_;
+    a.ntd = ntd_;
+    a.seismotype = seismotype;
+    a.alpha = alpha;
+    a.dt = dt_;
+    a.dtd = dtd_;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        CK(cudaFuncSetAttribute(k_trace_data, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(sizeof(float) * 2 * kResidualMaxSamples)));
+    });
+    k_trace_data<<<ntraces, 128, sizeof(float) * 2 * nt, st>>>(a);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, resid_.p, sizeof(float) * ntraces * ntd, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
 }
 
 double DeviceResidual::run(Engine &eng, size_t obs_offset, int ntraces, int seismotype, float alpha, float *residual,

@@ -326,6 +326,12 @@ public:
     double run(Engine &eng, size_t obs_offset, int ntraces, int seismotype, float alpha, float *residual,
                double *per_trace = nullptr, const float *traces = nullptr);
     const float *adjoint_sources() const { return asrc_.as<float>(); }
+    // Data of ntraces raw traces [ntraces][nt] on the device (modeling output,
+    // we_op.cpp:929-941): Dt for velocity data, times alpha, adjoint
+    // resampling to the data axis, into out [ntraces][ntd] on the host; the
+    // host formulation's operations in its order (same values bit for bit).
+    // Synchronises eng's stream.
+    void data(Engine &eng, const float *traces, int ntraces, int seismotype, float alpha, float *out);
 
 private:
     int device_ = -1, nt_ = -1, ntd_ = -1, hl_ = -1;

@@ -25,20 +25,25 @@ inline float hcoef(int n, int i)
     return 1.f;
 }
 
+// Element-wise loops and min / max reductions over the model, in parallel
+// (min and max are exact, so the results do not depend on the split).
 inline float fmin_range(const float *p, int64_t n)
 {
     float v = p[0];
+#pragma omp parallel for reduction(min : v) schedule(static)
     for (int64_t i = 1; i < n; i++) v = std::min(v, p[i]);
     return v;
 }
 inline float fmax_range(const float *p, int64_t n)
 {
     float v = p[0];
+#pragma omp parallel for reduction(max : v) schedule(static)
     for (int64_t i = 1; i < n; i++) v = std::max(v, p[i]);
     return v;
 }
 inline void clip_range(float *p, int64_t n, float lo, float hi)
 {
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < n; i++) p[i] = std::max(lo, std::min(hi, p[i]));
 }
 }  // namespace
@@ -72,16 +77,18 @@ TimeAxis analyze_model(std::vector<float> &model, int nmodels, int nx, int ny, i
                 clip_range(m + 5 * n, n, p.gammamin, p.gammamax);
             }
             // vs <= vp/sqrt(2) (we_op.cpp:331-341)
+#pragma omp parallel for schedule(static)
             for (int64_t i = 0; i < n; i++)
                 if ((double)m[i] < std::sqrt(2.0) * (double)m[n + i]) m[n + i] = (float)((double)m[i] / std::sqrt(2.0001));
         }
         ta.vmax = fmax_range(m, n);
         ta.vmin = fmin_range(m + n, n);
         if (nmodels == 6) {
-            float t = 0.f;
-            for (int64_t i = 0; i < n; i++) {
+            float t = (float)((double)m[0] * std::sqrt((double)(1 + 2 * m[4 * n])));
+#pragma omp parallel for reduction(max : t) schedule(static)
+            for (int64_t i = 1; i < n; i++) {
                 const float v = (float)((double)m[i] * std::sqrt((double)(1 + 2 * m[4 * n + i])));
-                t = i == 0 ? v : std::max(t, v);
+                t = std::max(t, v);
             }
             ta.vmax = std::max(t, ta.vmax);
         }
@@ -120,6 +127,7 @@ void convert_model(std::vector<float> &model, int nmodels, int64_t n)
     float *p0 = m, *p1 = m + n, *p2 = m + 2 * n;
     if (nmodels == 2) {
         // we_op.cpp:1539-1545
+#pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < n; i++) {
             p0[i] = p1[i] * p0[i] * p0[i];
             p1[i] = (float)(1.0 / p1[i]);
@@ -127,6 +135,7 @@ void convert_model(std::vector<float> &model, int nmodels, int64_t n)
         return;
     }
     float *p3 = m + 3 * n, *p5 = m + 5 * n;
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < n; i++) {
         p0[i] = p2[i] * (p0[i] * p0[i] - 2 * p1[i] * p1[i]);  // lambda
         p1[i] = p2[i] * p1[i] * p1[i];                          // mu

@@ -340,3 +340,21 @@ def test_das_objective_matches_reference(oracle_fp32):
         del os.environ["FWI_HOST_RESIDUAL"]
     assert fh == pytest.approx(f, rel=1e-6)
     assert rel(gh, g) < 1e-6
+
+
+@pytest.mark.parametrize("case", ["elastic_velocity", "acoustic", "das"])
+def test_device_trace_output_equals_host(case, monkeypatch):
+    """Batch traces post-processed on the device (Dt for velocity data,
+    dt/dt_data, sinc resampling to the data axis) equal the host formulation
+    (FWI_HOST_OUTPUT=1) bit for bit, for a whole batch and for shot slots."""
+    if case == "acoustic":
+        sv = synth.acoustic_linear(n=30, nsteps=90, taper=4, rec_stride=3)
+    elif case == "das":
+        sv = _das(n=28, steps=90)
+    else:
+        sv = _elastic(n=28, steps=90)
+        sv.par.seismotype = 1
+    dev = ops.forward_batch(sv)
+    monkeypatch.setenv("FWI_HOST_OUTPUT", "1")
+    host = ops.forward_batch(sv)
+    assert np.array_equal(dev, host)
