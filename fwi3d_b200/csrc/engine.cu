@@ -569,16 +569,68 @@ __global__ void k_tick(int *itp, int by) { *itp += by; }
 // Imaging of every shot of a batch at once: the increments of the shots
 // (fields at offsets s * sst) are summed in FP64 per point, then added to the
 // gradient once.
+// Point k of the 4-point shell of the grid (every point within 4 of a face):
+// the z rows 0..3 and nz-4..nz-1 whole, then the x rows 0..3 and nx-4..nx-1
+// of the other z rows, then the y planes 0..3 and ny-4..ny-1 of the rest.
+__device__ __forceinline__ bool shell_point(const Dims &g, int64_t k, int &ix, int &iy, int &iz)
+{
+    const int64_t nzs = (int64_t)8 * g.nx * g.ny;  // z rows of the shell
+    if (k < nzs) {
+        const int r = (int)(k % 8);
+        iz = r < 4 ? r : g.nz - 8 + r;
+        const int64_t q = k / 8;
+        ix = (int)(q % g.nx);
+        iy = (int)(q / g.nx);
+        return true;
+    }
+    k -= nzs;
+    const int mz = g.nz - 8;
+    const int64_t nxs = (int64_t)8 * mz * g.ny;
+    if (k < nxs) {
+        iz = 4 + (int)(k % mz);
+        const int64_t q = k / mz;
+        const int r = (int)(q % 8);
+        ix = r < 4 ? r : g.nx - 8 + r;
+        iy = (int)(q / 8);
+        return true;
+    }
+    k -= nxs;
+    const int mx = g.nx - 8;
+    if (k < (int64_t)8 * mz * mx) {
+        iz = 4 + (int)(k % mz);
+        const int64_t q = k / mz;
+        ix = 4 + (int)(q % mx);
+        const int r = (int)(q / mx);
+        iy = r < 4 ? r : g.ny - 8 + r;
+        return true;
+    }
+    return false;
+}
+
 // gst > 0: one gradient per shot, shot s's at offset s * gst (its increments
-// are not summed with the other shots').
-template <int PH>
+// are not summed with the other shots').  PART 0: every point; 1: the box of
+// points at least 4 from every face, whose derivatives are interior rows
+// only, so no warp diverges into the closure rows (z rows selected in place,
+// which keeps the lanes' 128-byte alignment); 2: the 4-point shell, one
+// thread per shell point (shell_point, 1-D grid).
+template <int PH, int PART = 0>
 __global__ void k_image_batch(ImageArgs a, int nshots, int64_t sst, int64_t gst)
 {
     int ix, iy, iz, s;
-    if (!point_of(a.g, (a.g.ny + BY - 1) / BY, ix, iy, iz, s)) return;
+    if (PART == 1) {
+        const Dims b{a.g.nx - 8, a.g.ny - 8, a.g.nz};
+        if (!point_of(b, (b.ny + BY - 1) / BY, ix, iy, iz, s) || iz < 4 || iz >= a.g.nz - 4) return;
+        ix += 4;
+        iy += 4;
+    } else if (PART == 2) {
+        if (!shell_point(a.g, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ix, iy, iz)) return;
+    } else if (!point_of(a.g, (a.g.ny + BY - 1) / BY, ix, iy, iz, s)) {
+        return;
+    }
     const int64_t i = a.g.idx(ix, iy, iz);
     double g0 = 0.0, g1 = 0.0, g2 = 0.0;
-    const bool in = ix >= 4 && ix < a.g.nx - 4 && iy >= 4 && iy < a.g.ny - 4 && iz >= 4 && iz < a.g.nz - 4;
+    const bool in = PART == 1 || (PART == 0 && ix >= 4 && ix < a.g.nx - 4 && iy >= 4 && iy < a.g.ny - 4 &&
+                                  iz >= 4 && iz < a.g.nz - 4);
     for (int sh = 0; sh < nshots; sh++) {
         if (PH == ACOUSTIC) {
             double k, b;
@@ -668,6 +720,8 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     cudaStream_t s;
     CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     stream_ = s;
+    const char *isp = std::getenv("FWI_IMAGE_SPLIT");
+    image_split_ = !(isp && isp[0] == '0');
     const char *cc = std::getenv("FWI_CONCURRENT");
     conc_ = !(cc && cc[0] == '0');
     if (conc_) {
@@ -2385,9 +2439,25 @@ void Engine::image(int itl, const float *curr, const float *prevl)
     }
     const int64_t sst = (int64_t)nc * n;
     const int64_t gst = per_shot_grad_ ? (int64_t)std::min(3, pb_.nmodels) * n : 0;
-    if (pb_.nmodels == 2) k_image_batch<ACOUSTIC><<<grd, blk, 0, s>>>(a, pb_.nshots, sst, gst);
-    else if (pb_.nmodels == 3) k_image_batch<ELASTIC><<<grd, blk, 0, s>>>(a, pb_.nshots, sst, gst);
-    else k_image_batch<VTI><<<grd, blk, 0, s>>>(a, pb_.nshots, sst, gst);
+    if (image_split_ && pb_.nmodels != 2 && pb_.nx > 8 && pb_.ny > 8 && pb_.nz > 8) {
+        // interior box and shell apart: the box's warps take the interior rows only
+        const dim3 gbox = grid_of(Dims{pb_.nx - 8, pb_.ny - 8, pb_.nz}, 1);
+        const int64_t nsh = n - (int64_t)(pb_.nx - 8) * (pb_.ny - 8) * (pb_.nz - 8);
+        const unsigned gsh = (unsigned)((nsh + 255) / 256);
+        if (pb_.nmodels == 3) {
+            k_image_batch<ELASTIC, 1><<<gbox, blk, 0, s>>>(a, pb_.nshots, sst, gst);
+            k_image_batch<ELASTIC, 2><<<gsh, 256, 0, s>>>(a, pb_.nshots, sst, gst);
+        } else {
+            k_image_batch<VTI, 1><<<gbox, blk, 0, s>>>(a, pb_.nshots, sst, gst);
+            k_image_batch<VTI, 2><<<gsh, 256, 0, s>>>(a, pb_.nshots, sst, gst);
+        }
+    } else if (pb_.nmodels == 2) {
+        k_image_batch<ACOUSTIC><<<grd, blk, 0, s>>>(a, pb_.nshots, sst, gst);
+    } else if (pb_.nmodels == 3) {
+        k_image_batch<ELASTIC><<<grd, blk, 0, s>>>(a, pb_.nshots, sst, gst);
+    } else {
+        k_image_batch<VTI><<<grd, blk, 0, s>>>(a, pb_.nshots, sst, gst);
+    }
     CK(cudaGetLastError());
 }
 

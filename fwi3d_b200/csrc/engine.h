@@ -219,6 +219,7 @@ private:
     bool conc_ = true;
     bool continuous_ = false;     // shot slots with their own start steps (shot_t0_)
     bool per_shot_grad_ = false;  // the adjoint keeps one gradient per shot
+    bool image_split_ = true;     // imaging in an interior-box and a shell launch (FWI_IMAGE_SPLIT=0: one)
     DevBuf shot_t0_, shot_active_;
     DevBuf das_w_, das_rcv_, das_src_;  // DAS projection weights, strain traces, dipole sources
     int das_nr_ = 0;
