@@ -727,7 +727,17 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     if (conc_) {
         cudaStream_t s2;
         cudaEvent_t e0, e1;
-        CK(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+        // the side stream (edge tiles, y-wall slabs: the longest CTAs of a
+        // step) at the device's highest priority, so that its blocks are
+        // dispatched ahead of the interior tiles' (FWI_SIDE_PRIORITY=0: default priority)
+        const char *sp = std::getenv("FWI_SIDE_PRIORITY");
+        if (!(sp && sp[0] == '0')) {
+            int lo = 0, hi = 0;
+            CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+            CK(cudaStreamCreateWithPriority(&s2, cudaStreamNonBlocking, hi));
+        } else {
+            CK(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+        }
         side_ = s2;
         CK(cudaEventCreateWithFlags(&e0, cudaEventDisableTiming));
         ev_fork_ = e0;
@@ -781,6 +791,12 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     // (measured at 256^3 x 8: 1 12.88, 2 11.05, 4 10.11, 8 9.85, 16 9.84 ms per step)
     const char *fw = std::getenv("FWI_FUSED_WAVES");
     fused_waves_ = fw ? std::max(1, std::atoi(fw)) : 8;
+    // the paired kernel's launches aim at about four waves: with the edge
+    // tiles and slabs on a second stream beside the interior tiles, longer y
+    // chunks (less prologue per plane) beat shorter tails (256^3 x 8: 5.95 ms
+    // per step at 4 waves, 6.08 at 8, 6.24 at 16)
+    const char *pw = std::getenv("FWI_PAIR_WAVES");
+    pair_waves_ = pw ? std::max(1, std::atoi(pw)) : 4;
     // isotropic interior tiles: two z-adjacent points per thread in packed
     // FP32 pairs (FWI_PAIR=0: one point per thread)
     const char *pe = std::getenv("FWI_PAIR");
@@ -1146,8 +1162,8 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
         const size_t sm = sizeof(FusedSmem);
         // y chunks per tile column: about fused_waves_ waves of resident CTAs,
         // at least 16 planes per chunk
-        auto chunks = [&](int64_t tiles, int minb) {
-            const int64_t target = (int64_t)sm_count_ * minb * fused_waves_;
+        auto chunks = [&](int64_t tiles, int minb, int waves = 0) {
+            const int64_t target = (int64_t)sm_count_ * minb * (waves > 0 ? waves : fused_waves_);
             const int64_t c = (target + tiles - 1) / tiles;
             return (int)std::max<int64_t>(1, std::min<int64_t>(c, (f.y1 - f.y0) / 16));
         };
@@ -1163,7 +1179,7 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
             // paired kernel: edge tiles (all of them when no tile is interior), then interior tiles
             const int64_t ti = (int64_t)(zh - zl) * (xh - xl) * pb_.nshots;
             const int64_t te = (int64_t)kz * kx * pb_.nshots - ti;
-            const int ne = chunks(te, 2), ni = chunks(std::max<int64_t>(ti, 1), 2);
+            const int ne = chunks(te, 2, pair_waves_), ni = chunks(std::max<int64_t>(ti, 1), 2, pair_waves_);
             const bool even = pb_.nz % 2 == 0;
             if (te > 0 && pair_edge_ == 2) {
                 // tiles touching an x face only, a z face only, both: y chunks per launch
@@ -1172,7 +1188,7 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
                 const int64_t tiles[3] = {tm3, tm4, tm5};
                 for (int mode = 3; mode <= 5; mode++) {
                     if (tiles[mode - 3] == 0) continue;
-                    const int nm = chunks(tiles[mode - 3] * pb_.nshots, 2);
+                    const int nm = chunks(tiles[mode - 3] * pb_.nshots, 2, pair_waves_);
                     pair_launch(even, mode, dim3(kz, kx, nm * pb_.nshots), sm, se, f, nm, tm, 0, 0);
                 }
             } else if (te > 0) {

@@ -288,6 +288,7 @@ private:
     int pair_edge_ = 2;            // its edge tiles: 0 one-point kernel, 1 x-face-only tiles paired, 2 all paired
     bool fused_split_ = true;      // interior and edge tiles of the fused kernel in separate launches
     int fused_waves_ = 8;          // y chunks per tile column: about this many waves of resident CTAs
+    int pair_waves_ = 4;           // the same for the paired kernel's launches
     bool fused_split_active() const;
     bool tma_ = false;             // fused kernel copies planes with bulk-tensor copies
     DevBuf tma_err_;               // int: a fused-kernel wait for a plane copy gave up
