@@ -799,6 +799,14 @@ Engine::Engine(int device, const Problem &pb) : device_(device), pb_(pb)
     // tiles and slabs on a second stream beside the interior tiles, longer y
     // chunks (less prologue per plane) beat shorter tails (256^3 x 8: 5.95 ms
     // per step at 4 waves, 6.08 at 8, 6.24 at 16)
+    // edge-tile modes on the second stream (FWI_SIDE_MODES, digits of 3..5):
+    // the z-face and corner tiles beside the slabs, the x-face tiles after
+    // the interior tiles balance the two streams best (256^3 x 8: 5.84 ms per
+    // step; all three on the second stream 5.93, mode 4 alone 5.89)
+    const char *smo = std::getenv("FWI_SIDE_MODES");
+    side_modes_ = 0;
+    for (const char *c = smo ? smo : "45"; *c; c++)
+        if (*c >= '3' && *c <= '5') side_modes_ |= 1 << (*c - '0');
     const char *pw = std::getenv("FWI_PAIR_WAVES");
     pair_waves_ = pw ? std::max(1, std::atoi(pw)) : 4;
     // isotropic interior tiles: two z-adjacent points per thread in packed
@@ -1185,22 +1193,26 @@ void Engine::step(float *prev, float *curr, float *next, bool taper_prev)
             const int64_t te = (int64_t)kz * kx * pb_.nshots - ti;
             const int ne = chunks(te, 2, pair_waves_), ni = chunks(std::max<int64_t>(ti, 1), 2, pair_waves_);
             const bool even = pb_.nz % 2 == 0;
-            if (te > 0 && pair_edge_ == 2) {
-                // tiles touching an x face only, a z face only, both: y chunks per launch
-                const int64_t nzi = zh - zl, nxi = xh - xl;
-                const int64_t tm3 = (kx - nxi) * nzi, tm4 = nxi * (kz - nzi), tm5 = (kx - nxi) * (kz - nzi);
-                const int64_t tiles[3] = {tm3, tm4, tm5};
+            // tiles touching an x face only (mode 3), a z face only (4), both (5): y chunks per launch;
+            // the modes of side_modes_ on the second stream, the others after the interior tiles
+            const int64_t nzi = zh - zl, nxi = xh - xl;
+            const int64_t tiles[3] = {(kx - nxi) * nzi, nxi * (kz - nzi), (kx - nxi) * (kz - nzi)};
+            auto edges = [&](bool side, cudaStream_t st) {
                 for (int mode = 3; mode <= 5; mode++) {
-                    if (tiles[mode - 3] == 0) continue;
+                    if (tiles[mode - 3] == 0 || (((side_modes_ >> mode) & 1) != 0) != side) continue;
                     const int nm = chunks(tiles[mode - 3] * pb_.nshots, 2, pair_waves_);
-                    pair_launch(even, mode, dim3(kz, kx, nm * pb_.nshots), sm, se, f, nm, tm, 0, 0);
+                    pair_launch(even, mode, dim3(kz, kx, nm * pb_.nshots), sm, st, f, nm, tm, 0, 0);
                 }
+            };
+            if (te > 0 && pair_edge_ == 2) {
+                edges(true, se);
             } else if (te > 0) {
                 // tiles with a z face: the one-point-per-thread kernel; with x faces only: the paired one
                 k_elastic_fused_part<2><<<dim3(kz, kx, ne * pb_.nshots), fblk, sm, s>>>(f, ne, tm, pair_edge_, 0);
                 if (pair_edge_ == 1) pair_launch(even, 3, dim3(kz, kx, ne * pb_.nshots), sm, s, f, ne, tm, 0, 0);
             }
             if (ti > 0) pair_launch(even, 1, dim3(zh - zl, xh - xl, ni * pb_.nshots), sm, s, f, ni, tm, zl, xl);
+            if (te > 0 && pair_edge_ == 2) edges(false, s);
             if (conc) {
                 CK(cudaEventRecord((cudaEvent_t)ev_join_, se));
                 CK(cudaStreamWaitEvent(s, (cudaEvent_t)ev_join_, 0));
