@@ -289,6 +289,7 @@ private:
     bool fused_split_ = true;      // interior and edge tiles of the fused kernel in separate launches
     int fused_waves_ = 8;          // y chunks per tile column: about this many waves of resident CTAs
     int pair_waves_ = 4;           // the same for the paired kernel's launches
+    bool slabs_last_ = true;       // the y-wall slabs after the side stream's edge tiles (FWI_SLABS_LAST=0: first)
     int side_modes_ = 0x30;        // bit m: edge mode m of the paired kernel on the second stream
     bool fused_split_active() const;
     bool tma_ = false;             // fused kernel copies planes with bulk-tensor copies
