@@ -30,7 +30,7 @@ EXPORTS = [
     "fwi_batch_sync", "fwi_batch_stream", "fwi_batch_traces", "fwi_batch_get_info", "fwi_batch_destroy",
     "fwi_last_error", "fwi_version", "fwi_elastic_step_static", "fwi_batch_time_main_kernel",
     "fwi_batch_main_kernel_time", "fwi_objective_create", "fwi_objective_evaluate", "fwi_objective_device_bytes",
-    "fwi_objective_destroy", "fwi_batch_enable_slots", "fwi_batch_join", "fwi_batch_release",
+    "fwi_objective_destroy", "fwi_batch_enable_slots", "fwi_batch_ready", "fwi_batch_join", "fwi_batch_release",
     "fwi_batch_slot_time", "fwi_batch_slot_traces", "fwi_objective_evaluate_shots", "fwi_objective_set_shots",
 ]
 
@@ -111,6 +111,8 @@ def load() -> C.CDLL:
     lib.fwi_batch_stream.restype = C.c_int
     lib.fwi_batch_traces.argtypes = [vp, fp]
     lib.fwi_batch_traces.restype = C.c_int
+    lib.fwi_batch_ready.argtypes = [vp, C.POINTER(C.c_int)]
+    lib.fwi_batch_ready.restype = C.c_int
     lib.fwi_batch_enable_slots.argtypes = [vp]
     lib.fwi_batch_enable_slots.restype = C.c_int
     lib.fwi_batch_join.argtypes = [vp, C.c_int, fp, fp]

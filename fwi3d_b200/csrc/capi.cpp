@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/fwi3d_gpu.h"
+#include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 
 #include "engine.h"
@@ -722,6 +723,21 @@ int fwi_batch_sync(fwi_batch *b)
 {
     if (!b) return fail(FWI_ERR_ARG, "null batch");
     return guarded([&] { b->eng->sync(); });
+}
+
+int fwi_batch_ready(fwi_batch *b, int *ready)
+{
+    if (!b || !ready) return fail(FWI_ERR_ARG, "null argument");
+    return guarded([&] {
+        const cudaError_t e = cudaStreamQuery((cudaStream_t)b->eng->stream());
+        if (e == cudaErrorNotReady) {
+            *ready = 0;
+            return;
+        }
+        if (e != cudaSuccess) throw FwiError(FWI_ERR_CUDA, cudaGetErrorString(e));
+        b->eng->sync();  // idle: surfaces the kernels' error flags
+        *ready = 1;
+    });
 }
 
 int fwi_batch_stream(fwi_batch *b, void **stream)

@@ -13,10 +13,12 @@ resident until the request completes:
   arrives while a session of its key runs takes a free slot (a spare one, or
   one whose shot has completed) at the next scheduling round and starts
   there, while the other slots run on; idle slots cost memory, not compute;
-* sessions advance up to `chunk` time steps per scheduling round (to the
-  next slot completion), each on its own CUDA stream, so work of different
-  sessions overlaps on the device and requests that arrive meanwhile are
-  admitted at the next round, while the others are running;
+* a session gets up to `chunk` time steps at a time (to its next slot
+  completion) on its own CUDA stream, and its next steps as soon as those
+  have finished: the dispatcher polls the sessions instead of waiting for
+  all of them, so a small session is not held to the pace of a large one,
+  work of different sessions overlaps on the device, and requests that
+  arrive meanwhile are admitted while the others run;
 * gradient requests of one key (same model, time axis, receiver count) are
   evaluated together, one objective per shot from the same batched launches
   (fwi_objective_evaluate_shots), on worker threads with their own streams;
@@ -176,6 +178,12 @@ class GpuExecutor:
 
     def wait(self, s) -> None:
         _lib.check(self.lib.fwi_batch_sync(s["h"]))
+
+    def ready(self, s) -> bool:
+        """The session's enqueued steps have finished (without waiting)."""
+        r = C.c_int()
+        _lib.check(self.lib.fwi_batch_ready(s["h"], C.byref(r)))
+        return bool(r.value)
 
     def remaining(self, s, slot: int) -> int:
         left = C.c_int()
@@ -344,7 +352,7 @@ class Server:
                     joined = False
                     if not r.own_session:
                         for se in sessions:
-                            if se["key"] != key:
+                            if se["key"] != key or se.get("busy"):
                                 continue
                             for k, q in enumerate(se["slots"]):
                                 if q is None:
@@ -380,24 +388,38 @@ class Server:
                     sessions.append({"x": x, "key": key, "slots": list(group) + [None] * (cap - len(group)),
                                      "bytes": b})
                     used += b
-                # advance every session to its next slot completion, at most one
-                # chunk (asynchronous launches on each session's own stream)
+                # every idle session gets its steps to its next slot completion,
+                # at most one chunk (asynchronous launches on its own stream)
                 for se in sessions:
+                    if se.get("busy"):
+                        continue
                     act = [k for k, q in enumerate(se["slots"]) if q is not None]
                     if not act:
                         continue  # kept for a pending shot of its key, which joins next round
                     k = min([self.chunk] + [self.ex.remaining(se["x"], j) for j in act])
                     if k > 0:
                         self.ex.advance(se["x"], k)
+                        se["busy"] = True
                     for j in act:
                         se["slots"][j].updates += k * se["x"]["points"]
+                # poll: sessions whose steps have finished turn idle
+                ready = getattr(self.ex, "ready", None)
+                progressed = False
                 for se in sessions:
-                    self.ex.wait(se["x"])
-                # completions; a session without shots closes unless a pending
-                # shot of its key will take a slot at the next admission
+                    if se.get("busy") and (ready is None or ready(se["x"])):
+                        if ready is None:
+                            self.ex.wait(se["x"])
+                        se["busy"] = False
+                        progressed = True
+                # completions of the idle sessions; a session without shots
+                # closes unless a pending shot of its key will take a slot at
+                # the next admission
                 arrivals()
                 keep = []
                 for se in sessions:
+                    if se.get("busy"):
+                        keep.append(se)
+                        continue
                     for j, q in enumerate(se["slots"]):
                         if q is not None and self.ex.remaining(se["x"], j) == 0:
                             q.result = self.ex.finish_slot(se["x"], j)
@@ -428,7 +450,9 @@ class Server:
                     else:
                         gkeep.append((fut, group, b))
                 grads = gkeep
-                if not sessions and done < len(requests):
+                if sessions and not progressed and all(se.get("busy") for se in sessions):
+                    sleep(0.0005)  # every session's steps still running
+                elif not sessions and done < len(requests):
                     if grads:
                         sleep(0.002)  # gradients on the workers, nothing to advance here
                     elif future and not pending:
@@ -436,6 +460,8 @@ class Server:
         finally:
             pool.shutdown(wait=True)
             for se in sessions:
+                if se.get("busy"):
+                    self.ex.wait(se["x"])
                 self.ex.close(se["x"])
             if hasattr(self.ex, "drop_cache"):
                 self.ex.drop_cache()

@@ -132,6 +132,11 @@ int fwi_batch_reset(fwi_batch *b);
 /* Enqueue nsteps time steps on the session's stream (asynchronous). */
 int fwi_batch_run(fwi_batch *b, int nsteps);
 int fwi_batch_sync(fwi_batch *b);
+/* *ready = 1 when the session's enqueued work has finished (then as
+ * fwi_batch_sync, without waiting), else 0: a dispatcher polls its sessions
+ * and gives each its next steps as soon as it is idle.  Serving; no
+ * counterpart in the reference. */
+int fwi_batch_ready(fwi_batch *b, int *ready);
 /* The cudaStream_t the session launches on (for event timing). */
 int fwi_batch_stream(fwi_batch *b, void **stream);
 /* Data [nshots][nrcomp][nr][nt_data] after the full time axis was run. */

@@ -206,3 +206,45 @@ def test_session_bytes_grow_with_shots_and_gradient():
     sv = synth.elastic_layered(n=24, nsteps=50, taper=4, rec_stride=6, nshots=1)
     assert serving.session_bytes(sv, 2) > serving.session_bytes(sv, 1)
     assert serving.session_bytes(sv, 1, gradient=True) > serving.session_bytes(sv, 1)
+
+
+class PollingExecutor(FakeExecutor):
+    """A session of model "big" reports its steps finished only on every
+    third poll; the others at once."""
+
+    def __init__(self, clock):
+        super().__init__(clock)
+        self.polls = {}
+        self.advances = {}
+        self.order = []
+
+    def open_batch(self, reqs, model, slots=None):
+        s = super().open_batch(reqs, model, slots)
+        s["model"] = reqs[0].model_id
+        return s
+
+    def advance(self, s, n):
+        self.advances[s["model"]] = self.advances.get(s["model"], 0) + 1
+        self.order.append(s["model"])
+        self.polls[id(s)] = 0
+        return super().advance(s, n)
+
+    def ready(self, s):
+        self.polls[id(s)] = self.polls.get(id(s), 0) + 1
+        return s["model"] != "big" or self.polls[id(s)] >= 3
+
+
+def test_idle_sessions_advance_while_a_slow_one_runs():
+    clk = FakeClock()
+    ex = PollingExecutor(clk)
+    big = _req(0, model_id="big", steps=300)
+    small = _req(1, model_id="small", steps=300)
+    srv = serving.Server({"big": None, "small": None}, executor=ex, chunk=20, max_batch=1)
+    srv.run([big, small], clock=clk, sleep=clk.sleep)
+    assert big.done is not None and small.done is not None
+    assert small.done < big.done
+    # the small session took its next chunk whenever it was idle, not once per
+    # slow round: between two chunks of the big session it ran several
+    runs = "".join("b" if m == "big" else "s" for m in ex.order)
+    assert "bsss" in runs and ex.advances["small"] == ex.advances["big"]
+    assert all(np.all(r.result == r.rid) for r in (big, small))
